@@ -1,0 +1,203 @@
+/*
+ * akmc.h -- C ABI of libakmc_b200.so, the B200 (sm_100a) vacancy-hop engine.
+ *
+ * Drop-in boundary for the GPU backend of MISA-AKMC (panzhija/MISA-AKMC-GPU).
+ * The reference's ABVIModel (models/abvi/kmc.cpp) drives its backend through
+ * the free functions of gpu/gpu_simulate.h:31-66 on the types of
+ * gpu/DeviceVacRatesSolver.h:7-25.  Each of those entry points has a
+ * counterpart below (cited at the declaration); the fused entry points
+ * (akmc_run_rounds, akmc_run) run the whole sector schedule of
+ * src/algorithms/sl/sublattice.inl:24-190 on the device.
+ *
+ * Plain C types only.  Every call returns an akmc_status and never exits the
+ * process (the reference exits on any HIP error, gpu/gpuError.hip:5-37).
+ * A context is used by one host thread at a time.
+ */
+#ifndef AKMC_H
+#define AKMC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define AKMC_API __attribute__((visibility("default")))
+#else
+#define AKMC_API
+#endif
+
+typedef enum akmc_status {
+  AKMC_OK = 0,
+  AKMC_EINVAL = -1,     /* bad argument or configuration */
+  AKMC_ENOMEM = -2,     /* device or host allocation failed, or over the memory budget */
+  AKMC_ECUDA = -3,      /* CUDA runtime error (message in akmc_last_error) */
+  AKMC_ETIMEOUT = -4,   /* a bounded device wait gave up */
+  AKMC_EBUSY = -5,      /* resource in use (server full, call in flight) */
+  AKMC_ESTATE = -6,     /* call out of order (e.g. run before prepare) */
+  AKMC_EOVERFLOW = -7,  /* a per-sector vacancy list or the event log overflowed */
+  AKMC_ERANGE = -8,     /* a density left the F table or a round exceeded its hop cap */
+  AKMC_ENOTFOUND = -9   /* unknown job id */
+} akmc_status;
+
+enum { AKMC_MODEL_PAIRBOND = 0, AKMC_MODEL_EAM = 1 };
+enum { AKMC_FP64 = 0, AKMC_FP32C = 1 };
+enum { AKMC_RNG_XOSHIRO = 0 };
+
+/* Occupancy codes (src/lattice/lattice_types.h:20-36). */
+enum { AKMC_V = 0, AKMC_FE = 1, AKMC_CU = 2, AKMC_NI = 4, AKMC_MN = 8 };
+
+/* Maximum vacancies in the active sector of one domain block. */
+#define AKMC_MAX_SECTOR_VACANCIES 64
+
+/*
+ * EAM model on the rigid BCC lattice: pair and density functions at the five
+ * shells within the cutoff (species order Fe, Cu, Ni, Mn) and the embedding
+ * function F(rho) at rho = k * 2^-7, k = 0..4999.  The density f is used in
+ * 2^-24 fixed point, so the per-site density cache is an exact int32 sum.
+ */
+typedef struct akmc_eam_tables {
+  int32_t n_shells;
+  int32_t reserved;
+  double f_shell[4][5];
+  double phi_shell[4][4][5];
+  double F[5000];
+} akmc_eam_tables;
+
+/* One AKMC job: a periodic box decomposed into domain blocks, each block with
+ * the 8 sectors of the synchronous sublattice. */
+typedef struct akmc_job_config {
+  int64_t box[3];           /* cells per dimension (config.yaml box.size) */
+  int32_t blocks[3];        /* domain blocks per dimension; 1,1,1 = single domain */
+  int32_t energy_model;     /* AKMC_MODEL_* */
+  int32_t precision;        /* AKMC_FP64 / AKMC_FP32C (EAM only) */
+  int32_t rng;              /* AKMC_RNG_XOSHIRO */
+  double lattice_const;     /* Angstrom (box.lattice_const) */
+  double cutoff_radius;     /* Angstrom (box.cutoff_radius) */
+  double attempt_freq;      /* 1/s (simulation.attempt_freq) */
+  double temperature;       /* K (simulation.temperature) */
+  double sector_window;     /* s; the reference hard-codes 3e-7 (src/simulation.h:73-74) */
+  uint64_t seed;            /* xoshiro256** streams of event selection and time, per block */
+  int64_t hop_budget;       /* job ends after the round reaching it; <= 0: none */
+  int64_t max_rounds;       /* job ends after this many sector rounds; <= 0: none */
+  const akmc_eam_tables* eam; /* EAM model (copied at akmc_add_job); NULL for pair-bond */
+} akmc_job_config;
+
+/* One performed hop; the layout of dev_event (gpu/DeviceVacRatesSolver.h:20-25)
+ * extended with the selection draw, the total rate and the residence time. */
+typedef struct akmc_event {
+  int64_t round;
+  int64_t hop;        /* hop index within its block */
+  int64_t from_site;  /* vacancy site before the hop (dev_event.from_id) */
+  int64_t to_site;    /* vacancy site after the hop (dev_event.to_id) */
+  int32_t block;      /* domain block within the job */
+  int32_t species;    /* code of the atom that moved (dev_event.to_type) */
+  double u;
+  double total;
+  double dt;
+  int32_t n_act;      /* vacancies in the sector when the hop was selected */
+  int32_t n_dirty;    /* vacancies whose rates the hop invalidated */
+  int32_t job;
+  int32_t reserved;
+} akmc_event;
+
+typedef struct akmc_job_state {
+  int64_t round;
+  int64_t hops;
+  int32_t done;
+  int32_t n_blocks;
+  int64_t n_sites;
+  int64_t n_vacancies;
+} akmc_job_state;
+
+typedef struct akmc_context_config {
+  int32_t device;              /* CUDA device ordinal */
+  int32_t graph_rounds;        /* sector rounds per captured CUDA graph (0: 32) */
+  void* stream;                /* cudaStream_t to run on; NULL: the context creates one */
+  int64_t event_log_capacity;  /* 0: no event log */
+  int64_t hop_cap_per_round;   /* per block and round; 0: 1e7 */
+} akmc_context_config;
+
+typedef struct akmc_ctx akmc_ctx;
+
+AKMC_API const char* akmc_status_string(akmc_status s);
+AKMC_API akmc_status akmc_last_error(akmc_ctx* ctx, char* buf, int32_t len);
+
+/* initialize_gpu (gpu/gpu_simulate.h:47, gpu_simulate.hip:1764-1769): selects
+ * device process_rank % device_count.  Unlike the reference it does not reset
+ * the device. */
+AKMC_API akmc_status akmc_initialize_gpu(int32_t process_rank, int32_t* device);
+
+AKMC_API akmc_status akmc_create(const akmc_context_config* cfg, akmc_ctx** out);
+AKMC_API akmc_status akmc_destroy(akmc_ctx* ctx);
+
+/* Registers a job.  occ holds the occupancy codes of the 2*nx*ny*nz sites,
+ * site id = x + 2nx (y + ny z) with x doubled (LatListMeta::getLId,
+ * src/lattice/lattice_list_meta.h:103-106); every AKMC_V site is a vacancy.
+ * The library copies the array; the caller keeps ownership (the reference's
+ * firstSectLocalToGpu frees its caller's array, gpu_simulate.hip:1207). */
+AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
+                                  int32_t* job_id);
+
+/* gpu_prepare (gpu/gpu_simulate.h:51, gpu_simulate.hip:1771-1831): allocates the
+ * device state of every registered job, uploads the lattices and builds the
+ * density caches. */
+AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx);
+
+/* Runs n sector rounds of every unfinished job on the device (the loop body of
+ * SubLattice::startTimeLoop, sublattice.inl:64-177, for all domain blocks at
+ * once).  Asynchronous on the context stream; errors surface at akmc_sync. */
+AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds);
+/* Runs until every job is done (hop budget or max_rounds) or max_rounds pass. */
+AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds);
+AKMC_API akmc_status akmc_sync(akmc_ctx* ctx);
+AKMC_API void* akmc_stream(akmc_ctx* ctx);
+
+/* gpu_final (gpu/gpu_simulate.h:49, gpu_simulate.hip:1833-1872): waits for the
+ * device and reports any deferred error. */
+AKMC_API akmc_status akmc_gpu_final(akmc_ctx* ctx);
+
+AKMC_API akmc_status akmc_get_job_state(akmc_ctx* ctx, int32_t job, akmc_job_state* st);
+AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out, int64_t n_sites);
+AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int64_t n_sites);
+/* evo[nblocks][8]: per-sector evolution time (SectorMeta, sublattice.h:17-33); hops[nblocks]. */
+AKMC_API akmc_status akmc_get_block_clocks(akmc_ctx* ctx, int32_t job, double* evo, int64_t* hops, int32_t n_blocks);
+/* Copies the event log (all jobs, device order) and empties it. */
+AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t capacity, int64_t* n_out);
+/* Device-side counters: [0] hops, [1] rate evaluations, [2] rounds run, [3] blocks processed. */
+AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out4);
+
+/*
+ * Per-hop entry points for a single-domain job, with the host driving the
+ * sector loop, the RNG and the clock exactly as ABVIModel + SubLattice do.
+ */
+/* calculate_GPU / first_calculate_GPU (gpu_simulate.h:33-35, gpu_simulate.hip:1211-1716):
+ * rates of every vacancy in sector sector_id; returns their ordered sum. */
+AKMC_API akmc_status akmc_calculate(akmc_ctx* ctx, int32_t job, int32_t sector_id, double* total);
+/* selectAndPerformEventGPU (gpu_simulate.h:37-41, gpu_simulate.hip:1388-1449):
+ * selects the first event whose cumulative rate exceeds u * total in z-y-x
+ * order and performs it.  ev->from_site < 0 when no event is selected. */
+AKMC_API akmc_status akmc_select_and_perform(akmc_ctx* ctx, int32_t job, int32_t sector_id, double u,
+                                             akmc_event* ev);
+
+/* Helpers. */
+/* Synthetic Johnson-form EAM for Fe, Cu, Ni, Mn from a seed (xoshiro stream tag 5). */
+AKMC_API akmc_status akmc_eam_johnson(uint64_t seed, double lattice_const, double cutoff_radius,
+                                      akmc_eam_tables* out);
+/* Random alloy and vacancies (creation::createRandom, src/creation.cpp:96-164) with
+ * xoshiro256** streams: one draw per site in site-id order, then vacancies. */
+AKMC_API akmc_status akmc_create_lattice(const int64_t box[3], const int32_t type_codes[4], const int64_t ratio[4],
+                                         int64_t n_vacancies, uint64_t seed, uint8_t* occ, int64_t n_sites);
+/* Isolated-Cu count (profiles/m_event_hook.cpp:17-55) and Cu cluster-size histogram (1nn). */
+AKMC_API akmc_status akmc_cluster_stats(const uint8_t* occ, const int64_t box[3], int64_t* isolated_cu, int64_t* hist,
+                                        int64_t hist_len);
+
+/* Device checks of the shared arithmetic: port_exp/port_log of x[i] on the GPU. */
+AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AKMC_H */

@@ -1,0 +1,734 @@
+// akmc_api.cu -- the C ABI of include/akmc.h over the kernels of akmc_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "akmc_device.h"
+#include "akmc_model.h"
+
+using namespace akmc;
+
+namespace {
+
+struct HostJob {
+  akmc_job_config cfg{};
+  bool has_eam = false;
+  akmc_eam_tables eam{};
+  std::vector<uint8_t> occ;
+  int64_t nsites = 0;
+  int64_t nvac = 0;
+  int32_t block0 = 0, nblocks = 0;
+  int32_t vac0 = 0;
+  int32_t pot = 0;
+  std::vector<int32_t> split[3];
+  uint8_t* d_occ = nullptr;
+  int32_t* d_rho = nullptr;
+};
+
+struct DevPot {
+  Potential P;
+  double* d_coef = nullptr;
+  FCell32* d_f32 = nullptr;
+  std::vector<double> coef;
+  std::vector<FCell32> f32;
+  bool has_eam = false;
+  akmc_eam_tables src{};
+};
+
+const char* cuda_name(int e) { return cudaGetErrorString(static_cast<cudaError_t>(e)); }
+
+}  // namespace
+
+struct akmc_ctx {
+  akmc_context_config cfg{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  std::vector<HostJob> jobs;
+  std::vector<DevPot> pots;
+  bool prepared = false;
+  int32_t nblocks = 0, nvac = 0;
+  // device state
+  JobDev* d_jobs = nullptr;
+  BlockDev* d_blocks = nullptr;
+  int32_t* d_vac_site = nullptr;
+  int32_t* d_vac_job = nullptr;
+  int32_t* d_blk_list = nullptr;
+  int32_t* d_active = nullptr;
+  int32_t* d_n_active = nullptr;
+  Potential* d_pots = nullptr;
+  Geometry* d_geo = nullptr;
+  akmc_event* d_log = nullptr;
+  unsigned long long* d_log_count = nullptr;
+  unsigned int* d_status = nullptr;
+  unsigned long long* d_counters = nullptr;
+  double* d_api_total = nullptr;
+  akmc_event* d_api_event = nullptr;
+  size_t smem = 0;
+  int hop_grid = 0;
+  RoundArgs args{};
+  cudaGraphExec_t graph = nullptr;
+  cudaGraph_t graph_def = nullptr;
+  int graph_rounds = 0;
+  int32_t* d_vac_count = nullptr;
+  // kernel timing mode: rounds launched one by one with events around the hop kernel
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;
+  double hop_ms = 0.0;
+  int64_t hop_launches = 0;
+};
+
+namespace {
+
+akmc_status fail(akmc_ctx* c, akmc_status s, const std::string& msg) {
+  if (c) c->err = msg;
+  return s;
+}
+#define CK(call)                                                                                       \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess) return fail(ctx, AKMC_ECUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+  return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+}
+
+akmc_status check_status(akmc_ctx* ctx) {
+  unsigned int st = 0;
+  CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (!st) return AKMC_OK;
+  CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
+  if (st & kErrVacOverflow) return fail(ctx, AKMC_EOVERFLOW, "more than AKMC_MAX_SECTOR_VACANCIES vacancies in one sector");
+  if (st & kErrRhoRange) return fail(ctx, AKMC_ERANGE, "a density left the F table");
+  if (st & kErrHopCap) return fail(ctx, AKMC_ERANGE, "a block exceeded the hop cap of one round");
+  if (st & kErrLogOverflow) return fail(ctx, AKMC_EOVERFLOW, "event log full");
+  return fail(ctx, AKMC_ESTATE, "device reported status " + std::to_string(st));
+}
+
+void free_device(akmc_ctx* ctx) {
+  for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
+  ctx->ev.clear();
+  cudaFree(ctx->d_vac_count);
+  ctx->d_vac_count = nullptr;
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  if (ctx->graph_def) cudaGraphDestroy(ctx->graph_def);
+  ctx->graph = nullptr;
+  ctx->graph_def = nullptr;
+  for (auto& j : ctx->jobs) {
+    cudaFree(j.d_occ);
+    cudaFree(j.d_rho);
+    j.d_occ = nullptr;
+    j.d_rho = nullptr;
+  }
+  for (auto& p : ctx->pots) {
+    cudaFree(p.d_coef);
+    cudaFree(p.d_f32);
+    p.d_coef = nullptr;
+    p.d_f32 = nullptr;
+  }
+  void* ptrs[] = {ctx->d_jobs, ctx->d_blocks, ctx->d_vac_site, ctx->d_vac_job, ctx->d_blk_list, ctx->d_active,
+                  ctx->d_n_active, ctx->d_pots, ctx->d_geo, ctx->d_log, ctx->d_log_count, ctx->d_status,
+                  ctx->d_counters, ctx->d_api_total, ctx->d_api_event};
+  for (void* p : ptrs) cudaFree(p);
+  ctx->d_jobs = nullptr;
+  ctx->d_blocks = nullptr;
+  ctx->d_vac_site = ctx->d_vac_job = ctx->d_blk_list = ctx->d_active = ctx->d_n_active = nullptr;
+  ctx->d_pots = nullptr;
+  ctx->d_geo = nullptr;
+  ctx->d_log = nullptr;
+  ctx->d_log_count = nullptr;
+  ctx->d_status = nullptr;
+  ctx->d_counters = nullptr;
+  ctx->d_api_total = nullptr;
+  ctx->d_api_event = nullptr;
+  ctx->prepared = false;
+}
+
+int region_sites(const HostJob& j) {
+  int64_t mx = 1;
+  for (int d = 0; d < 3; ++d) {
+    int wmax = 0;
+    for (size_t k = 0; k + 1 < j.split[d].size(); ++k) {
+      const int w = j.split[d][k + 1] - j.split[d][k];
+      wmax = std::max(wmax, w - w / 2);
+    }
+    mx *= (wmax + 4) * (d == 0 ? 2 : 1);
+  }
+  return static_cast<int>(mx);
+}
+
+}  // namespace
+
+extern "C" {
+
+AKMC_API const char* akmc_status_string(akmc_status s) {
+  switch (s) {
+    case AKMC_OK: return "ok";
+    case AKMC_EINVAL: return "invalid argument";
+    case AKMC_ENOMEM: return "out of memory";
+    case AKMC_ECUDA: return "CUDA error";
+    case AKMC_ETIMEOUT: return "timed out";
+    case AKMC_EBUSY: return "busy";
+    case AKMC_ESTATE: return "invalid state";
+    case AKMC_EOVERFLOW: return "overflow";
+    case AKMC_ERANGE: return "out of range";
+    case AKMC_ENOTFOUND: return "not found";
+  }
+  return "unknown";
+}
+
+AKMC_API akmc_status akmc_last_error(akmc_ctx* ctx, char* buf, int32_t len) {
+  if (!ctx || !buf || len <= 0) return AKMC_EINVAL;
+  std::snprintf(buf, static_cast<size_t>(len), "%s", ctx->err.c_str());
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_initialize_gpu(int32_t process_rank, int32_t* device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return AKMC_ECUDA;
+  const int d = (process_rank < 0 ? 0 : process_rank) % n;
+  if (cudaSetDevice(d) != cudaSuccess) return AKMC_ECUDA;
+  if (device) *device = d;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_create(const akmc_context_config* cfg, akmc_ctx** out) {
+  if (!out) return AKMC_EINVAL;
+  *out = nullptr;
+  akmc_ctx* ctx = new (std::nothrow) akmc_ctx();
+  if (!ctx) return AKMC_ENOMEM;
+  if (cfg) ctx->cfg = *cfg;
+  if (ctx->cfg.graph_rounds <= 0) ctx->cfg.graph_rounds = 32;
+  if (ctx->cfg.hop_cap_per_round <= 0) ctx->cfg.hop_cap_per_round = 10000000;
+  if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) {
+    delete ctx;
+    return AKMC_ECUDA;
+  }
+  if (ctx->cfg.stream) {
+    ctx->stream = static_cast<cudaStream_t>(ctx->cfg.stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return AKMC_ECUDA;
+    }
+    ctx->own_stream = true;
+  }
+  *out = ctx;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_destroy(akmc_ctx* ctx) {
+  if (!ctx) return AKMC_EINVAL;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_device(ctx);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return AKMC_OK;
+}
+
+AKMC_API void* akmc_stream(akmc_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
+                                  int32_t* job_id) {
+  if (!ctx || !cfg || !occ) return AKMC_EINVAL;
+  if (ctx->prepared) return fail(ctx, AKMC_ESTATE, "jobs must be added before akmc_prepare");
+  HostJob j;
+  j.cfg = *cfg;
+  j.cfg.eam = nullptr;
+  for (int d = 0; d < 3; ++d) {
+    if (cfg->box[d] < 8 || cfg->box[d] > (1 << 20)) return fail(ctx, AKMC_EINVAL, "box edge must be in [8, 2^20] cells");
+    const int p = cfg->blocks[d] > 0 ? cfg->blocks[d] : 1;
+    block_split(cfg->box[d], p, j.split[d]);
+    for (int k = 0; k < p; ++k)
+      if (j.split[d][k + 1] - j.split[d][k] < 8)
+        return fail(ctx, AKMC_EINVAL, "domain block edges must be >= 8 cells (sector halos may not overlap)");
+  }
+  j.nsites = 2 * cfg->box[0] * cfg->box[1] * cfg->box[2];
+  if (j.nsites != n_sites) return fail(ctx, AKMC_EINVAL, "n_sites != 2*nx*ny*nz");
+  if (j.nsites >= (int64_t(1) << 31)) return fail(ctx, AKMC_EINVAL, "more than 2^31 sites in one job");
+  if (cfg->energy_model != AKMC_MODEL_PAIRBOND && cfg->energy_model != AKMC_MODEL_EAM)
+    return fail(ctx, AKMC_EINVAL, "unknown energy model");
+  if (cfg->precision != AKMC_FP64 && cfg->precision != AKMC_FP32C) return fail(ctx, AKMC_EINVAL, "unknown precision");
+  if (cfg->rng != AKMC_RNG_XOSHIRO) return fail(ctx, AKMC_EINVAL, "unsupported rng");
+  if (!(cfg->temperature > 0) || !(cfg->attempt_freq > 0) || !(cfg->sector_window > 0))
+    return fail(ctx, AKMC_EINVAL, "temperature, attempt_freq and sector_window must be > 0");
+  if (cfg->energy_model == AKMC_MODEL_EAM) {
+    if (!cfg->eam) return fail(ctx, AKMC_EINVAL, "EAM job without tables");
+    j.has_eam = true;
+    j.eam = *cfg->eam;
+  }
+  j.occ.assign(occ, occ + n_sites);
+  for (int64_t s = 0; s < n_sites; ++s) {
+    if (occ[s] == kV) ++j.nvac;
+    else if (!is_atom(occ[s])) return fail(ctx, AKMC_EINVAL, "invalid occupancy code at site " + std::to_string(s));
+  }
+  j.nblocks = (cfg->blocks[0] > 0 ? cfg->blocks[0] : 1) * (cfg->blocks[1] > 0 ? cfg->blocks[1] : 1) *
+              (cfg->blocks[2] > 0 ? cfg->blocks[2] : 1);
+  ctx->jobs.push_back(std::move(j));
+  if (job_id) *job_id = static_cast<int32_t>(ctx->jobs.size() - 1);
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
+  if (!ctx) return AKMC_EINVAL;
+  if (ctx->prepared) return AKMC_OK;
+  if (ctx->jobs.empty()) return fail(ctx, AKMC_ESTATE, "no jobs");
+  CK(cudaSetDevice(ctx->cfg.device));
+  // potentials: pair-bond tables in every entry; EAM tables deduplicated by content
+  ctx->pots.clear();
+  {
+    DevPot pb;
+    if (build_potential(nullptr, pb.P, pb.coef, pb.f32)) return fail(ctx, AKMC_EINVAL, "potential");
+    ctx->pots.push_back(std::move(pb));
+  }
+  int max_region = 0;
+  int32_t nb = 0, nv = 0;
+  for (auto& j : ctx->jobs) {
+    j.pot = 0;
+    if (j.has_eam) {
+      int found = -1;
+      for (size_t i = 1; i < ctx->pots.size(); ++i)
+        if (std::memcmp(&ctx->pots[i].src, &j.eam, sizeof(j.eam)) == 0) found = static_cast<int>(i);
+      if (found < 0) {
+        DevPot p;
+        p.has_eam = true;
+        p.src = j.eam;
+        const int rc = build_potential(&j.eam, p.P, p.coef, p.f32);
+        if (rc == -2) return fail(ctx, AKMC_ERANGE, "EAM densities can exceed the F table");
+        if (rc) return fail(ctx, AKMC_EINVAL, "invalid EAM tables");
+        ctx->pots.push_back(std::move(p));
+        found = static_cast<int>(ctx->pots.size() - 1);
+      }
+      j.pot = found;
+    }
+    j.block0 = nb;
+    j.vac0 = nv;
+    nb += j.nblocks;
+    nv += static_cast<int32_t>(j.nvac);
+    max_region = std::max(max_region, region_sites(j));
+  }
+  ctx->nblocks = nb;
+  ctx->nvac = nv;
+  ctx->smem = hop_smem_bytes(max_region);
+  int dev_smem = 0;
+  CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
+  if (ctx->smem > static_cast<size_t>(dev_smem))
+    return fail(ctx, AKMC_EINVAL, "sector region does not fit in shared memory; use more domain blocks");
+  {
+    const int e = configure_hop_smem(ctx->smem);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cuda_name(e));
+  }
+  int sms = 148;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device));
+  int smem_sm = 0;
+  CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
+  int per_sm = std::max(1, std::min(32, static_cast<int>(smem_sm / (ctx->smem + 1024))));
+  ctx->hop_grid = std::max(1, std::min(nb, sms * per_sm));
+
+  // geometry and potentials
+  Geometry geo;
+  int nsh = 5;
+  for (auto& j : ctx->jobs) nsh = std::min(nsh, shells_within(j.cfg.lattice_const, j.cfg.cutoff_radius));
+  for (auto& j : ctx->jobs)
+    if (j.has_eam && (j.eam.n_shells != 5 || shells_within(j.cfg.lattice_const, j.cfg.cutoff_radius) != 5 ||
+                      2.0 * j.cfg.lattice_const < j.cfg.cutoff_radius))
+      return fail(ctx, AKMC_EINVAL, "the EAM path needs exactly the 5 BCC shells inside the cutoff");
+  build_geometry(geo, 5);
+  CK(dalloc(&ctx->d_geo, 1));
+  CK(cudaMemcpyAsync(ctx->d_geo, &geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<Potential> hp;
+  for (auto& p : ctx->pots) {
+    CK(dalloc(&p.d_coef, p.coef.size()));
+    CK(dalloc(&p.d_f32, p.f32.size()));
+    CK(cudaMemcpyAsync(p.d_coef, p.coef.data(), p.coef.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.d_f32, p.f32.data(), p.f32.size() * sizeof(FCell32), cudaMemcpyHostToDevice, ctx->stream));
+    Potential P = p.P;
+    P.Fcoef = p.d_coef;
+    P.F32 = p.d_f32;
+    hp.push_back(P);
+  }
+  CK(dalloc(&ctx->d_pots, hp.size()));
+  CK(cudaMemcpyAsync(ctx->d_pots, hp.data(), hp.size() * sizeof(Potential), cudaMemcpyHostToDevice, ctx->stream));
+
+  // jobs, blocks, vacancies
+  std::vector<JobDev> hj(ctx->jobs.size());
+  std::vector<BlockDev> hb(static_cast<size_t>(nb));
+  std::vector<int32_t> vsite(static_cast<size_t>(nv)), vjob(static_cast<size_t>(nv));
+  for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
+    HostJob& j = ctx->jobs[ji];
+    CK(dalloc(&j.d_occ, static_cast<size_t>(j.nsites)));
+    CK(cudaMemcpyAsync(j.d_occ, j.occ.data(), static_cast<size_t>(j.nsites), cudaMemcpyHostToDevice, ctx->stream));
+    if (j.has_eam) CK(dalloc(&j.d_rho, static_cast<size_t>(j.nsites)));
+    JobDev& J = hj[ji];
+    std::memset(&J, 0, sizeof(J));
+    J.occ = j.d_occ;
+    J.rho = j.d_rho;
+    for (int d = 0; d < 3; ++d) {
+      J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
+      J.nb[d] = static_cast<int32_t>(j.split[d].size() - 1);
+    }
+    J.sx = 2 * J.n[0];
+    J.sy = J.n[1];
+    J.sz = J.n[2];
+    J.block0 = j.block0;
+    J.nblocks = j.nblocks;
+    J.model = j.cfg.energy_model;
+    J.precision = j.cfg.precision;
+    J.pot = j.pot;
+    J.hop_budget = j.cfg.hop_budget;
+    J.max_rounds = j.cfg.max_rounds;
+    J.nu = j.cfg.attempt_freq;
+    J.kT = kBoltzmann * j.cfg.temperature;
+    J.window = j.cfg.sector_window;
+    for (int b = 0; b < j.nblocks; ++b) {
+      BlockDev& B = hb[static_cast<size_t>(j.block0 + b)];
+      std::memset(&B, 0, sizeof(B));
+      B.job = static_cast<int32_t>(ji);
+      B.local_id = b;
+      const int bi[3] = {b % J.nb[0], (b / J.nb[0]) % J.nb[1], b / (J.nb[0] * J.nb[1])};
+      for (int d = 0; d < 3; ++d) {
+        B.c0[d] = j.split[d][static_cast<size_t>(bi[d])];
+        B.c1[d] = j.split[d][static_cast<size_t>(bi[d]) + 1];
+      }
+      xoshiro_seed(B.xs, j.cfg.seed, kTagSelect, static_cast<uint64_t>(b));
+      xoshiro_seed(B.xt, j.cfg.seed, kTagTime, static_cast<uint64_t>(b));
+    }
+    int32_t k = j.vac0;
+    for (int64_t s = 0; s < j.nsites; ++s)
+      if (j.occ[static_cast<size_t>(s)] == kV) {
+        vsite[static_cast<size_t>(k)] = static_cast<int32_t>(s);
+        vjob[static_cast<size_t>(k)] = static_cast<int32_t>(ji);
+        ++k;
+      }
+  }
+  CK(dalloc(&ctx->d_jobs, hj.size()));
+  CK(dalloc(&ctx->d_blocks, hb.size()));
+  CK(dalloc(&ctx->d_vac_site, vsite.size()));
+  CK(dalloc(&ctx->d_vac_job, vjob.size()));
+  CK(dalloc(&ctx->d_blk_list, static_cast<size_t>(nb) * kMaxV));
+  CK(dalloc(&ctx->d_active, static_cast<size_t>(nb)));
+  CK(dalloc(&ctx->d_n_active, 1));
+  CK(dalloc(&ctx->d_status, 1));
+  CK(dalloc(&ctx->d_counters, 8));
+  CK(dalloc(&ctx->d_vac_count, 1));
+  CK(dalloc(&ctx->d_log_count, 1));
+  CK(dalloc(&ctx->d_api_total, 1));
+  CK(dalloc(&ctx->d_api_event, 1));
+  if (ctx->cfg.event_log_capacity > 0) CK(dalloc(&ctx->d_log, static_cast<size_t>(ctx->cfg.event_log_capacity)));
+  CK(cudaMemcpyAsync(ctx->d_jobs, hj.data(), hj.size() * sizeof(JobDev), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
+  if (nv) {
+    CK(cudaMemcpyAsync(ctx->d_vac_site, vsite.data(), vsite.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_vac_job, vjob.data(), vjob.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CK(cudaMemsetAsync(ctx->d_n_active, 0, 4, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_counters, 0, 64, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_log_count, 0, 8, ctx->stream));
+  for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
+    HostJob& j = ctx->jobs[ji];
+    if (!j.has_eam) continue;
+    const int e = launch_init_rho(j.d_occ, j.d_rho, hj[ji].sx, hj[ji].sy, hj[ji].sz, ctx->d_pots + j.pot, ctx->d_geo,
+                                  ctx->d_status, ctx->stream);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("init rho: ") + cuda_name(e));
+  }
+  RoundArgs& a = ctx->args;
+  std::memset(&a, 0, sizeof(a));
+  a.jobs = ctx->d_jobs;
+  a.njobs = static_cast<int32_t>(ctx->jobs.size());
+  a.nblocks = nb;
+  a.blocks = ctx->d_blocks;
+  a.vac_site = ctx->d_vac_site;
+  a.vac_job = ctx->d_vac_job;
+  a.nvac = nv;
+  a.mode = kModeRound;
+  a.blk_list = ctx->d_blk_list;
+  a.active = ctx->d_active;
+  a.n_active = ctx->d_n_active;
+  a.pots = ctx->d_pots;
+  a.geo = ctx->d_geo;
+  a.log = ctx->d_log;
+  a.log_count = ctx->d_log_count;
+  a.log_cap = ctx->cfg.event_log_capacity;
+  a.status = ctx->d_status;
+  a.counters = ctx->d_counters;
+  a.hop_cap = ctx->cfg.hop_cap_per_round;
+  a.api_job = -1;
+  a.api_sector = -1;
+  a.api_total = ctx->d_api_total;
+  a.api_event = ctx->d_api_event;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->prepared = true;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (n_rounds <= 0) return AKMC_OK;
+  CK(cudaSetDevice(ctx->cfg.device));
+  RoundArgs a = ctx->args;
+  a.mode = kModeRound;
+  if (ctx->timing) {
+    // one launch sequence per round, events around every hop kernel
+    const size_t pool = 512;
+    while (ctx->ev.size() < 2 * pool) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      ctx->ev.push_back(e);
+    }
+    int64_t left = n_rounds;
+    while (left > 0) {
+      const int64_t n = std::min<int64_t>(left, static_cast<int64_t>(pool));
+      for (int64_t r = 0; r < n; ++r) {
+        const int e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, ctx->ev[2 * r], ctx->ev[2 * r + 1]);
+        if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+      }
+      CK(cudaStreamSynchronize(ctx->stream));
+      for (int64_t r = 0; r < n; ++r) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[2 * r], ctx->ev[2 * r + 1]));
+        ctx->hop_ms += ms;
+        ctx->hop_launches += 1;
+      }
+      left -= n;
+    }
+    return AKMC_OK;
+  }
+  const int chunk = ctx->cfg.graph_rounds;
+  if (n_rounds >= chunk && !ctx->graph) {
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int e = 0;
+    for (int r = 0; r < chunk && !e; ++r) e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, nullptr, nullptr);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    if (e || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(ctx, AKMC_ECUDA, std::string("graph capture: ") + cuda_name(e ? e : ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&ctx->graph, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(ctx, AKMC_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    ctx->graph_def = g;
+    ctx->graph_rounds = chunk;
+  }
+  int64_t left = n_rounds;
+  while (ctx->graph && left >= ctx->graph_rounds) {
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    left -= ctx->graph_rounds;
+  }
+  for (; left > 0; --left) {
+    const int e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, nullptr, nullptr);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+  }
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_sync(akmc_ctx* ctx) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return AKMC_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return check_status(ctx);
+}
+
+AKMC_API akmc_status akmc_gpu_final(akmc_ctx* ctx) { return akmc_sync(ctx); }
+
+AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  std::vector<JobDev> hj(ctx->jobs.size());
+  int64_t done_rounds = 0;
+  const int64_t step = std::max<int64_t>(ctx->cfg.graph_rounds, 1);
+  while (max_rounds <= 0 || done_rounds < max_rounds) {
+    const int64_t n = max_rounds > 0 ? std::min(step, max_rounds - done_rounds) : step;
+    akmc_status s = akmc_run_rounds(ctx, n);
+    if (s) return s;
+    done_rounds += n;
+    CK(cudaMemcpyAsync(hj.data(), ctx->d_jobs, hj.size() * sizeof(JobDev), cudaMemcpyDeviceToHost, ctx->stream));
+    s = akmc_sync(ctx);
+    if (s) return s;
+    bool all = true;
+    for (auto& J : hj) all = all && J.done;
+    if (all) break;
+  }
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_job_state(akmc_ctx* ctx, int32_t job, akmc_job_state* st) {
+  if (!ctx || !st) return AKMC_EINVAL;
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  std::memset(st, 0, sizeof(*st));
+  st->n_blocks = j.nblocks;
+  st->n_sites = j.nsites;
+  st->n_vacancies = j.nvac;
+  if (!ctx->prepared) return AKMC_OK;
+  JobDev J;
+  CK(cudaMemcpyAsync(&J, ctx->d_jobs + job, sizeof(J), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  st->round = J.round;
+  st->hops = J.hops;
+  st->done = J.done;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out, int64_t n_sites) {
+  if (!ctx || !out) return AKMC_EINVAL;
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  if (n_sites != j.nsites) return AKMC_EINVAL;
+  if (!ctx->prepared) {
+    std::memcpy(out, j.occ.data(), static_cast<size_t>(n_sites));
+    return AKMC_OK;
+  }
+  CK(cudaMemcpyAsync(out, j.d_occ, static_cast<size_t>(n_sites), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int64_t n_sites) {
+  if (!ctx || !out) return AKMC_EINVAL;
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  if (n_sites != j.nsites || !j.has_eam) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  CK(cudaMemcpyAsync(out, j.d_rho, static_cast<size_t>(n_sites) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_block_clocks(akmc_ctx* ctx, int32_t job, double* evo, int64_t* hops, int32_t n_blocks) {
+  if (!ctx || !evo || !hops) return AKMC_EINVAL;
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  if (n_blocks != j.nblocks) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  std::vector<BlockDev> hb(static_cast<size_t>(j.nblocks));
+  CK(cudaMemcpyAsync(hb.data(), ctx->d_blocks + j.block0, hb.size() * sizeof(BlockDev), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int b = 0; b < j.nblocks; ++b) {
+    for (int k = 0; k < 8; ++k) evo[b * 8 + k] = hb[static_cast<size_t>(b)].evo[k];
+    hops[b] = hb[static_cast<size_t>(b)].hops;
+  }
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t capacity, int64_t* n_out) {
+  if (!ctx || !n_out) return AKMC_EINVAL;
+  *n_out = 0;
+  if (!ctx->prepared || !ctx->d_log) return AKMC_OK;
+  unsigned long long n = 0;
+  CK(cudaMemcpyAsync(&n, ctx->d_log_count, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const int64_t avail = std::min<int64_t>(static_cast<int64_t>(n), ctx->cfg.event_log_capacity);
+  const int64_t m = std::min<int64_t>(avail, capacity);
+  if (m > 0 && out)
+    CK(cudaMemcpyAsync(out, ctx->d_log, static_cast<size_t>(m) * sizeof(akmc_event), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_log_count, 0, 8, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_out = m;
+  if (static_cast<int64_t>(n) > ctx->cfg.event_log_capacity) return fail(ctx, AKMC_EOVERFLOW, "event log overflowed");
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out4) {
+  if (!ctx || !out4) return AKMC_EINVAL;
+  if (!ctx->prepared) {
+    for (int i = 0; i < 4; ++i) out4[i] = 0;
+    return AKMC_OK;
+  }
+  unsigned long long c[4];
+  CK(cudaMemcpyAsync(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < 4; ++i) out4[i] = static_cast<int64_t>(c[i]);
+  return AKMC_OK;
+}
+
+static akmc_status api_step(akmc_ctx* ctx, int32_t job, int32_t sector_id, int32_t mode, double u) {
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (ctx->jobs[static_cast<size_t>(job)].nblocks != 1)
+    return fail(ctx, AKMC_EINVAL, "the per-hop entry points drive single-domain jobs");
+  if (sector_id < 0 || sector_id > 7) return fail(ctx, AKMC_EINVAL, "sector id in [0, 7]");
+  CK(cudaSetDevice(ctx->cfg.device));
+  RoundArgs a = ctx->args;
+  a.mode = mode;
+  a.api_job = job;
+  a.api_sector = sector_id;
+  a.api_u = u;
+  a.log_cap = 0;
+  const int e = launch_api(a, ctx->smem, ctx->stream);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_calculate(akmc_ctx* ctx, int32_t job, int32_t sector_id, double* total) {
+  if (!ctx || !total) return AKMC_EINVAL;
+  akmc_status s = api_step(ctx, job, sector_id, kModeCalc, 0.0);
+  if (s) return s;
+  CK(cudaMemcpyAsync(total, ctx->d_api_total, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return akmc_sync(ctx);
+}
+
+AKMC_API akmc_status akmc_select_and_perform(akmc_ctx* ctx, int32_t job, int32_t sector_id, double u,
+                                             akmc_event* ev) {
+  if (!ctx || !ev) return AKMC_EINVAL;
+  akmc_status s = api_step(ctx, job, sector_id, kModeSelectPerform, u);
+  if (s) return s;
+  CK(cudaMemcpyAsync(ev, ctx->d_api_event, sizeof(akmc_event), cudaMemcpyDeviceToHost, ctx->stream));
+  return akmc_sync(ctx);
+}
+
+AKMC_API akmc_status akmc_eam_johnson(uint64_t seed, double lattice_const, double cutoff_radius,
+                                      akmc_eam_tables* out) {
+  if (!out) return AKMC_EINVAL;
+  return eam_johnson(seed, lattice_const, cutoff_radius, out, nullptr) ? AKMC_EINVAL : AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_create_lattice(const int64_t box[3], const int32_t type_codes[4], const int64_t ratio[4],
+                                         int64_t n_vacancies, uint64_t seed, uint8_t* occ, int64_t n_sites) {
+  if (!box || !type_codes || !ratio || !occ) return AKMC_EINVAL;
+  return create_lattice(box, type_codes, ratio, n_vacancies, seed, occ, n_sites) ? AKMC_EINVAL : AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_cluster_stats(const uint8_t* occ, const int64_t box[3], int64_t* isolated_cu, int64_t* hist,
+                                        int64_t hist_len) {
+  if (!occ || !box || !isolated_cu || (!hist && hist_len > 0)) return AKMC_EINVAL;
+  return cluster_stats(occ, box, isolated_cu, hist, hist_len) ? AKMC_EINVAL : AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out) {
+  if (!ctx || !x || !exp_out || !log_out || n <= 0) return AKMC_EINVAL;
+  CK(cudaSetDevice(ctx->cfg.device));
+  double *dx = nullptr, *de = nullptr, *dl = nullptr;
+  CK(dalloc(&dx, static_cast<size_t>(n)));
+  CK(dalloc(&de, static_cast<size_t>(n)));
+  CK(dalloc(&dl, static_cast<size_t>(n)));
+  cudaMemcpyAsync(dx, x, static_cast<size_t>(n) * 8, cudaMemcpyHostToDevice, ctx->stream);
+  const int e = launch_device_math(dx, n, de, dl, ctx->stream);
+  cudaMemcpyAsync(exp_out, de, static_cast<size_t>(n) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(log_out, dl, static_cast<size_t>(n) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dx);
+  cudaFree(de);
+  cudaFree(dl);
+  if (e) return fail(ctx, AKMC_ECUDA, cuda_name(e));
+  if (se != cudaSuccess) return fail(ctx, AKMC_ECUDA, cudaGetErrorString(se));
+  return AKMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// akmc_device.h -- device-side state of the vacancy-hop engine (internal).
+#pragma once
+
+#include <stdint.h>
+
+#include "../../include/akmc.h"
+#include "akmc_common.cuh"
+
+namespace akmc {
+
+constexpr int kMaxV = AKMC_MAX_SECTOR_VACANCIES;  // vacancies per block and sector
+constexpr int kJumpN = 76;                        // |N(s) u N(t)| - 2 sites per jump
+constexpr int kRefreshN = 78;                     // density refresh sites per jump
+constexpr int kShellNb = 58;                      // neighbours within the 5-shell cutoff
+
+// Packed neighbour entry: int8 dX | int8 dy << 8 | int8 dz << 16 | (sh_s | sh_t << 4) << 24,
+// dX in doubled-x site units; shell codes 0 = outside the cutoff, 1..5 shells, 6 = the site itself.
+AK_HD int unpack_dx(int32_t w) { return static_cast<int8_t>(w & 0xff); }
+AK_HD int unpack_dy(int32_t w) { return static_cast<int8_t>((w >> 8) & 0xff); }
+AK_HD int unpack_dz(int32_t w) { return static_cast<int8_t>((w >> 16) & 0xff); }
+AK_HD int unpack_sh_s(int32_t w) { return (w >> 24) & 0xf; }
+AK_HD int unpack_sh_t(int32_t w) { return (w >> 28) & 0xf; }
+AK_HD int32_t pack_entry(int dx, int dy, int dz, int sh_s, int sh_t) {
+  return static_cast<int32_t>((static_cast<uint32_t>(dx) & 0xffu) | ((static_cast<uint32_t>(dy) & 0xffu) << 8) |
+                              ((static_cast<uint32_t>(dz) & 0xffu) << 16) |
+                              ((static_cast<uint32_t>(sh_s) | (static_cast<uint32_t>(sh_t) << 4)) << 24));
+}
+
+// Geometry tables (built on the host, one copy in global memory).
+struct Geometry {
+  int32_t nn1[2][8];                 // 1nn, LatListMeta::getIdBy1nnOffset order by x parity
+  int32_t nn2[6];                    // 2nn, PeriodLatticeList::get2nn2 order (mask 0x2F)
+  int32_t nbr[2][kShellNb];          // EAM shell neighbours (sh in sh_s)
+  int32_t jump[2][8][kJumpN];        // EAM dE site list of jump b, order (dz, dy, dX)
+  int32_t refresh[2][8][kRefreshN];  // density refresh list of jump b (incl. s and t)
+};
+
+// Per-potential tables.
+struct Potential {
+  int32_t fq[4][8];         // density contribution (Q.24) by species and shell code
+  double phi64[4][4][8];    // pair energy by (moving species, neighbour species, shell code)
+  float phi32[4][4][8];
+  double b1[5][5], b2[5][5];  // pair-bond 1nn / 2nn tables (V, Fe, Cu, Ni, Mn)
+  const double* Fcoef;      // kTabN x 4 doubles
+  const FCell32* F32;       // kTabN cells
+};
+
+struct JobDev {
+  uint8_t* occ;
+  int32_t* rho;
+  int32_t n[3];       // cells
+  int32_t sx, sy, sz; // sites per dimension (sx = 2 n[0])
+  int32_t nb[3];      // domain blocks per dimension
+  int32_t block0;     // first global block
+  int32_t nblocks;
+  int32_t model, precision, pot;
+  int32_t done;
+  int32_t pad;
+  int64_t round;
+  int64_t hops;
+  int64_t hop_budget, max_rounds;
+  double nu, kT, window;
+};
+
+struct BlockDev {
+  int32_t job, local_id;
+  int32_t c0[3], c1[3];  // block cells [c0, c1)
+  int64_t round;
+  int64_t hops;
+  double evo[8];         // per-sector evolution time
+  uint64_t xs[4], xt[4]; // selection / residence-time streams
+  int32_t cnt;           // vacancies bucketed into the active sector this round
+  int32_t done;          // the job finished at or before this block's last round
+};
+
+enum : uint32_t {
+  kErrVacOverflow = 1u,
+  kErrRhoRange = 2u,
+  kErrHopCap = 4u,
+  kErrLogOverflow = 8u,
+  kErrApiState = 16u,
+};
+
+enum : int32_t { kModeRound = 0, kModeCalc = 1, kModeSelectPerform = 2 };
+
+struct RoundArgs {
+  JobDev* jobs;
+  int32_t njobs;
+  int32_t nblocks;
+  BlockDev* blocks;
+  int32_t* vac_site;
+  int32_t* vac_job;
+  int32_t nvac;
+  int32_t mode;
+  int32_t* blk_list;  // nblocks * kMaxV
+  int32_t* active;    // nblocks
+  int32_t* n_active;
+  const Potential* pots;
+  const Geometry* geo;
+  akmc_event* log;
+  unsigned long long* log_count;
+  int64_t log_cap;
+  unsigned int* status;
+  unsigned long long* counters;  // hops, evaluations, rounds, blocks, n_act sum, staged sites, written sites, -
+  int64_t hop_cap;
+  // per-hop entry points
+  int32_t api_job, api_sector;
+  double api_u;
+  double* api_total;
+  akmc_event* api_event;
+};
+
+// Kernel launchers (akmc_kernels.cu).
+size_t hop_smem_bytes(int max_region_sites);
+int configure_hop_smem(size_t smem);
+// ev0/ev1 (cudaEvent_t or null) are recorded around the hop kernel.
+int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1);
+int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
+                             int32_t cap, int32_t* count, void* stream);
+int launch_api(const RoundArgs& a, size_t smem, void* stream);
+int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, const Potential* pot,
+                    const Geometry* geo, unsigned int* status, void* stream);
+int launch_device_math(const double* x, int64_t n, double* e, double* l, void* stream);
+
+}  // namespace akmc

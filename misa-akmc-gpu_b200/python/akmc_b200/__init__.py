@@ -1,0 +1,366 @@
+"""ctypes binding of libakmc_b200.so (include/akmc.h).
+
+The compute path is the CUDA library; this module only marshals arguments.
+There is no CPU fallback: loading fails with an error when the library has not
+been built, and every non-zero status raises AkmcError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(os.path.dirname(HERE))  # misa-akmc-gpu_b200/
+LIB_PATH = os.path.join(PKG, "lib", "libakmc_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "akmc.h")
+
+MODEL_PAIRBOND, MODEL_EAM = 0, 1
+FP64, FP32C = 0, 1
+RNG_XOSHIRO = 0
+V, FE, CU, NI, MN = 0, 1, 2, 4, 8
+MAX_SECTOR_VACANCIES = 64
+SECTOR_ORDER = (0, 7, 2, 5, 3, 4, 1, 6)
+
+STATUS = {
+    0: "AKMC_OK",
+    -1: "AKMC_EINVAL",
+    -2: "AKMC_ENOMEM",
+    -3: "AKMC_ECUDA",
+    -4: "AKMC_ETIMEOUT",
+    -5: "AKMC_EBUSY",
+    -6: "AKMC_ESTATE",
+    -7: "AKMC_EOVERFLOW",
+    -8: "AKMC_ERANGE",
+    -9: "AKMC_ENOTFOUND",
+}
+
+
+class AkmcError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("%s (%d): %s" % (STATUS.get(status, "?"), status, msg))
+
+
+class EamTables(C.Structure):
+    _fields_ = [
+        ("n_shells", C.c_int32),
+        ("reserved", C.c_int32),
+        ("f_shell", (C.c_double * 5) * 4),
+        ("phi_shell", ((C.c_double * 5) * 4) * 4),
+        ("F", C.c_double * 5000),
+    ]
+
+
+class JobConfig(C.Structure):
+    _fields_ = [
+        ("box", C.c_int64 * 3),
+        ("blocks", C.c_int32 * 3),
+        ("energy_model", C.c_int32),
+        ("precision", C.c_int32),
+        ("rng", C.c_int32),
+        ("lattice_const", C.c_double),
+        ("cutoff_radius", C.c_double),
+        ("attempt_freq", C.c_double),
+        ("temperature", C.c_double),
+        ("sector_window", C.c_double),
+        ("seed", C.c_uint64),
+        ("hop_budget", C.c_int64),
+        ("max_rounds", C.c_int64),
+        ("eam", C.POINTER(EamTables)),
+    ]
+
+
+class Event(C.Structure):
+    _fields_ = [
+        ("round", C.c_int64),
+        ("hop", C.c_int64),
+        ("from_site", C.c_int64),
+        ("to_site", C.c_int64),
+        ("block", C.c_int32),
+        ("species", C.c_int32),
+        ("u", C.c_double),
+        ("total", C.c_double),
+        ("dt", C.c_double),
+        ("n_act", C.c_int32),
+        ("n_dirty", C.c_int32),
+        ("job", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+EVENT_DTYPE = np.dtype(
+    [
+        ("round", "<i8"),
+        ("hop", "<i8"),
+        ("from_site", "<i8"),
+        ("to_site", "<i8"),
+        ("block", "<i4"),
+        ("species", "<i4"),
+        ("u", "<f8"),
+        ("total", "<f8"),
+        ("dt", "<f8"),
+        ("n_act", "<i4"),
+        ("n_dirty", "<i4"),
+        ("job", "<i4"),
+        ("reserved", "<i4"),
+    ]
+)
+assert EVENT_DTYPE.itemsize == C.sizeof(Event)
+
+
+class JobState(C.Structure):
+    _fields_ = [
+        ("round", C.c_int64),
+        ("hops", C.c_int64),
+        ("done", C.c_int32),
+        ("n_blocks", C.c_int32),
+        ("n_sites", C.c_int64),
+        ("n_vacancies", C.c_int64),
+    ]
+
+
+class ContextConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("graph_rounds", C.c_int32),
+        ("stream", C.c_void_p),
+        ("event_log_capacity", C.c_int64),
+        ("hop_cap_per_round", C.c_int64),
+    ]
+
+
+# every symbol include/akmc.h declares, with (restype, argtypes)
+_vp, _i32, _i64, _u64, _d = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_double
+SIGNATURES = {
+    "akmc_status_string": (C.c_char_p, [C.c_int]),
+    "akmc_last_error": (C.c_int, [_vp, C.c_char_p, _i32]),
+    "akmc_initialize_gpu": (C.c_int, [_i32, C.POINTER(_i32)]),
+    "akmc_create": (C.c_int, [C.POINTER(ContextConfig), C.POINTER(_vp)]),
+    "akmc_destroy": (C.c_int, [_vp]),
+    "akmc_add_job": (C.c_int, [_vp, C.POINTER(JobConfig), _vp, _i64, C.POINTER(_i32)]),
+    "akmc_prepare": (C.c_int, [_vp]),
+    "akmc_run_rounds": (C.c_int, [_vp, _i64]),
+    "akmc_run": (C.c_int, [_vp, _i64]),
+    "akmc_sync": (C.c_int, [_vp]),
+    "akmc_stream": (_vp, [_vp]),
+    "akmc_gpu_final": (C.c_int, [_vp]),
+    "akmc_get_job_state": (C.c_int, [_vp, _i32, C.POINTER(JobState)]),
+    "akmc_get_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
+    "akmc_get_rho": (C.c_int, [_vp, _i32, _vp, _i64]),
+    "akmc_get_block_clocks": (C.c_int, [_vp, _i32, _vp, _vp, _i32]),
+    "akmc_get_events": (C.c_int, [_vp, _vp, _i64, C.POINTER(_i64)]),
+    "akmc_get_counters": (C.c_int, [_vp, _vp]),
+    "akmc_calculate": (C.c_int, [_vp, _i32, _i32, C.POINTER(_d)]),
+    "akmc_select_and_perform": (C.c_int, [_vp, _i32, _i32, _d, C.POINTER(Event)]),
+    "akmc_eam_johnson": (C.c_int, [_u64, _d, _d, C.POINTER(EamTables)]),
+    "akmc_create_lattice": (C.c_int, [_vp, _vp, _vp, _i64, _u64, _vp, _i64]),
+    "akmc_cluster_stats": (C.c_int, [_vp, _vp, C.POINTER(_i64), _vp, _i64]),
+    "akmc_device_math": (C.c_int, [_vp, _vp, _i64, _vp, _vp]),
+}
+
+_lib = None
+
+
+def lib_path():
+    return LIB_PATH
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libakmc_b200.so not built (%s); run python misa-akmc-gpu_b200/build.py" % LIB_PATH
+            )
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc, ctx=None):
+    if rc != 0:
+        msg = ""
+        if ctx:
+            buf = C.create_string_buffer(512)
+            lib().akmc_last_error(ctx, buf, 512)
+            msg = buf.value.decode(errors="replace")
+        raise AkmcError(rc, msg)
+
+
+def eam_johnson(seed=42, lattice_const=2.855, cutoff=5.6):
+    t = EamTables()
+    _check(lib().akmc_eam_johnson(seed, lattice_const, cutoff, C.byref(t)))
+    return t
+
+
+def create_lattice(box, alloy, n_vacancies, seed):
+    box = np.asarray(box, np.int64)
+    codes = np.array([a[0] for a in alloy] + [FE] * (4 - len(alloy)), np.int32)
+    ratio = np.array([a[1] for a in alloy] + [0] * (4 - len(alloy)), np.int64)
+    occ = np.empty(int(2 * box[0] * box[1] * box[2]), np.uint8)
+    _check(lib().akmc_create_lattice(_ptr(box), _ptr(codes), _ptr(ratio), n_vacancies, seed, _ptr(occ), occ.size))
+    return occ
+
+
+def cluster_stats(occ, box, hist_len=64):
+    occ = np.ascontiguousarray(occ, np.uint8)
+    box = np.asarray(box, np.int64)
+    iso = C.c_int64(0)
+    hist = np.zeros(hist_len, np.int64)
+    _check(lib().akmc_cluster_stats(_ptr(occ), _ptr(box), C.byref(iso), _ptr(hist), hist_len))
+    return int(iso.value), hist
+
+
+def job_config(
+    box,
+    blocks=(1, 1, 1),
+    energy_model=MODEL_EAM,
+    precision=FP64,
+    lattice_const=2.855,
+    cutoff=5.6,
+    attempt_freq=6e12,
+    temperature=573.0,
+    window=3.0e-7,
+    seed=42,
+    hop_budget=0,
+    max_rounds=0,
+    eam=None,
+):
+    c = JobConfig()
+    c.box[:] = list(box)
+    c.blocks[:] = list(blocks)
+    c.energy_model = energy_model
+    c.precision = precision
+    c.rng = RNG_XOSHIRO
+    c.lattice_const = lattice_const
+    c.cutoff_radius = cutoff
+    c.attempt_freq = attempt_freq
+    c.temperature = temperature
+    c.sector_window = window
+    c.seed = seed
+    c.hop_budget = hop_budget
+    c.max_rounds = max_rounds
+    c._eam_ref = eam
+    c.eam = C.pointer(eam) if eam is not None else C.POINTER(EamTables)()
+    return c
+
+
+class Engine:
+    """One akmc_ctx: a set of jobs advanced together on one GPU."""
+
+    def __init__(self, device=0, stream=None, event_log_capacity=0, graph_rounds=32, hop_cap_per_round=0):
+        cfg = ContextConfig()
+        cfg.device = device
+        cfg.graph_rounds = graph_rounds
+        cfg.stream = stream
+        cfg.event_log_capacity = event_log_capacity
+        cfg.hop_cap_per_round = hop_cap_per_round
+        h = C.c_void_p()
+        _check(lib().akmc_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.jobs = []
+
+    def close(self):
+        if self.h:
+            lib().akmc_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        _check(rc, self.h)
+
+    def add_job(self, cfg, occ):
+        occ = np.ascontiguousarray(occ, np.uint8)
+        jid = C.c_int32(-1)
+        self._ck(lib().akmc_add_job(self.h, C.byref(cfg), _ptr(occ), occ.size, C.byref(jid)))
+        self.jobs.append((cfg, occ.size))
+        return jid.value
+
+    def prepare(self):
+        self._ck(lib().akmc_prepare(self.h))
+
+    def run_rounds(self, n):
+        self._ck(lib().akmc_run_rounds(self.h, n))
+
+    def run(self, max_rounds=0):
+        self._ck(lib().akmc_run(self.h, max_rounds))
+
+    def sync(self):
+        self._ck(lib().akmc_sync(self.h))
+
+    @property
+    def stream(self):
+        return lib().akmc_stream(self.h)
+
+    def job_state(self, job=0):
+        st = JobState()
+        self._ck(lib().akmc_get_job_state(self.h, job, C.byref(st)))
+        return dict(round=st.round, hops=st.hops, done=bool(st.done), n_blocks=st.n_blocks,
+                    n_sites=st.n_sites, n_vacancies=st.n_vacancies)
+
+    def occupancy(self, job=0):
+        n = self.jobs[job][1]
+        out = np.empty(n, np.uint8)
+        self._ck(lib().akmc_get_occupancy(self.h, job, _ptr(out), n))
+        return out
+
+    def rho(self, job=0):
+        n = self.jobs[job][1]
+        out = np.empty(n, np.int32)
+        self._ck(lib().akmc_get_rho(self.h, job, _ptr(out), n))
+        return out
+
+    def block_clocks(self, job=0):
+        nb = self.job_state(job)["n_blocks"]
+        evo = np.empty((nb, 8), np.float64)
+        hops = np.empty(nb, np.int64)
+        self._ck(lib().akmc_get_block_clocks(self.h, job, _ptr(evo), _ptr(hops), nb))
+        return evo, hops
+
+    def events(self, capacity=1 << 22):
+        out = np.empty(capacity, EVENT_DTYPE)
+        n = C.c_int64(0)
+        self._ck(lib().akmc_get_events(self.h, _ptr(out), capacity, C.byref(n)))
+        return out[: n.value].copy()
+
+    def counters(self):
+        out = np.zeros(4, np.int64)
+        self._ck(lib().akmc_get_counters(self.h, _ptr(out)))
+        return dict(hops=int(out[0]), evaluations=int(out[1]), rounds=int(out[2]), blocks=int(out[3]))
+
+    def calculate(self, job, sector_id):
+        t = C.c_double(0.0)
+        self._ck(lib().akmc_calculate(self.h, job, sector_id, C.byref(t)))
+        return t.value
+
+    def select_and_perform(self, job, sector_id, u):
+        ev = Event()
+        self._ck(lib().akmc_select_and_perform(self.h, job, sector_id, u, C.byref(ev)))
+        return ev
+
+    def device_math(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        e = np.empty_like(x)
+        l = np.empty_like(x)
+        self._ck(lib().akmc_device_math(self.h, _ptr(x), x.size, _ptr(e), _ptr(l)))
+        return e, l

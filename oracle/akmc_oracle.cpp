@@ -737,6 +737,7 @@ struct Job {
           if (from >= 0) break;
         }
         int64_t to = -1;
+        int64_t nd = 0;
         uint8_t X = 0;
         if (from >= 0) {
           // ABVIModel::perform (kmc.cpp:358-396)
@@ -755,7 +756,7 @@ struct Job {
             }
           }
           // device work model: vacancies of the sector within D cells of the hop
-          int64_t nd = 0;
+          nd = 0;
           for (const auto& v : vr) {
             const int64_t vs = (v.site == from) ? to : v.site;
             int64_t vX, vy, vz;
@@ -785,6 +786,7 @@ struct Job {
           e.total = total;
           e.dt = dt;
           e.n_act = static_cast<int32_t>(vr.size());
+          e.n_dirty = static_cast<int32_t>(nd);
           ev.push_back(e);
         }
       }

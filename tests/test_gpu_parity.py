@@ -1,0 +1,207 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Integer results (event sites, species, block, round, hop index, final
+occupancy, density cache) must be identical; the floating-point results of
+the same arithmetic (selection draw, total rate, residence time, per-sector
+clocks) must be identical bit for bit, because host and device execute the
+same IEEE operation sequence.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from helpers import CU_134, QUATERNARY, assert_same_events, device_job, oracle_job
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ak():
+    import os
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "misa-akmc-gpu_b200"))
+    import build
+
+    build.build()
+    import akmc_b200
+
+    return akmc_b200
+
+
+def run_pair(ak, rounds, jobs):
+    """jobs: list of dicts of oracle_job/device_job kwargs; returns (engine, oracles)."""
+    eng = ak.Engine(event_log_capacity=1 << 21)
+    oracles = []
+    for kw in jobs:
+        o = oracle_job(**kw)
+        dkw = {k: kw[k] for k in ("box", "blocks", "model", "precision", "seed", "temperature", "pot_seed", "window")
+               if k in kw}
+        device_job(eng, o, **dkw)
+        oracles.append(o)
+    eng.prepare()
+    for o in oracles:
+        o.run_rounds(rounds)
+    eng.run_rounds(rounds)
+    eng.sync()
+    return eng, oracles
+
+
+def check_job(eng, o, j, dev_events):
+    ev = dev_events[dev_events["job"] == j]
+    assert_same_events(ev, o.events())
+    assert np.array_equal(eng.occupancy(j), o.occupancy())
+    evo_d, hops_d = eng.block_clocks(j)
+    evo_o, hops_o = o.block_state()
+    assert np.array_equal(hops_d, hops_o)
+    assert np.array_equal(evo_d.view(np.uint64), evo_o.view(np.uint64))
+    st = eng.job_state(j)
+    assert st["hops"] == o.hops and st["round"] == o.round
+
+
+def test_device_exp_log_bit_exact(ak):
+    rng = np.random.default_rng(7)
+    x = np.concatenate([rng.uniform(-60, 0, 4000), rng.uniform(1e-300, 1, 4000), rng.uniform(-700, 700, 2000),
+                        [0.0, 1.0, 0.5, 2.0 ** -1074, 709.0, -745.0]])
+    with ak.Engine() as eng:
+        e, l = eng.device_math(x)
+    want_e = np.array([po.port_exp(v) for v in x])
+    want_l = np.array([po.port_log(v) if v > 0 else np.nan for v in x])
+    assert np.array_equal(e.view(np.uint64), want_e.view(np.uint64))
+    pos = x > 0
+    assert np.array_equal(l[pos].view(np.uint64), want_l[pos].view(np.uint64))
+
+
+@pytest.mark.parametrize("model,prec", [(po.MODEL_EAM, po.FP64), (po.MODEL_EAM, po.FP32C),
+                                        (po.MODEL_PAIRBOND, po.FP64)])
+def test_single_domain_20_cubed(ak, model, prec):
+    eng, (o,) = run_pair(ak, 400, [dict(box=(20, 20, 20), model=model, precision=prec)])
+    assert o.hops > 1000
+    check_job(eng, o, 0, eng.events())
+    if model == po.MODEL_EAM:
+        assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
+
+
+def test_domain_blocks_quaternary(ak):
+    kw = dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=60,
+              temperature=563.0, seed=7)
+    eng, (o,) = run_pair(ak, 160, [kw])
+    assert o.hops > 500
+    check_job(eng, o, 0, eng.events())
+    assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
+
+
+def test_uneven_blocks_and_odd_edges(ak):
+    kw = dict(box=(25, 17, 19), blocks=(3, 2, 1), model=po.MODEL_EAM, precision=po.FP32C, alloy=QUATERNARY,
+              n_vacancies=30, seed=11)
+    eng, (o,) = run_pair(ak, 120, [kw])
+    check_job(eng, o, 0, eng.events())
+    eng.close()
+
+
+def test_batched_jobs_of_different_shapes(ak):
+    jobs = [
+        dict(box=(20, 20, 20), model=po.MODEL_EAM, seed=1, temperature=573.0),
+        dict(box=(16, 24, 18), model=po.MODEL_PAIRBOND, seed=2, alloy=QUATERNARY, n_vacancies=9, temperature=500.0),
+        dict(box=(32, 16, 16), blocks=(2, 1, 1), model=po.MODEL_EAM, precision=po.FP32C, seed=3, n_vacancies=12,
+             temperature=650.0, pot_seed=5),
+    ]
+    eng, oracles = run_pair(ak, 96, jobs)
+    ev = eng.events()
+    for j, o in enumerate(oracles):
+        check_job(eng, o, j, ev)
+    eng.close()
+
+
+def test_hop_budget_stops_at_round_boundary(ak):
+    o = oracle_job(box=(20, 20, 20))
+    with ak.Engine(event_log_capacity=1 << 20) as eng:
+        device_job(eng, o, (20, 20, 20), hop_budget=2000)
+        eng.prepare()
+        o.run(2000, 100000)
+        eng.run(100000)
+        st = eng.job_state(0)
+        assert st["done"] and st["hops"] == o.hops and st["round"] == o.round
+        assert o.hops >= 2000
+        assert np.array_equal(eng.occupancy(0), o.occupancy())
+
+
+def test_job_without_vacancies_only_advances_clocks(ak):
+    o = oracle_job(box=(16, 16, 16), n_vacancies=0)
+    with ak.Engine() as eng:
+        device_job(eng, o, (16, 16, 16))
+        eng.prepare()
+        o.run_rounds(24)
+        eng.run_rounds(24)
+        evo_d, hops_d = eng.block_clocks(0)
+        evo_o, _ = o.block_state()
+        assert hops_d.sum() == 0
+        assert np.array_equal(evo_d.view(np.uint64), evo_o.view(np.uint64))
+
+
+def _host_driven_loop(eng, o_cfg_seed, window, rounds, job=0):
+    """SubLattice::startTimeLoop (sublattice.inl:61-140) driven from the host over
+    the per-hop entry points, with the host drawing the xoshiro streams."""
+    sel = iter(po.xoshiro_stream(o_cfg_seed, 3, 0, 1 << 20))
+    tim = iter(po.xoshiro_stream(o_cfg_seed, 4, 0, 1 << 20))
+    evo = [0.0] * 8
+    events = []
+    hops = 0
+    for rnd in range(rounds):
+        sector = ak_sector(rnd)
+        step = rnd // 8
+        thr = float(step + 1) * window - evo[sector]
+        t = 0.0
+        while t < thr:
+            total = eng.calculate(job, sector)
+            if total == 0.0 or abs(total) < np.finfo(float).eps:
+                t = thr
+                continue
+            u = float(int(next(sel)) >> 11) * 2.0 ** -53
+            ev = eng.select_and_perform(job, sector, u)
+            u2 = float((int(next(tim)) >> 11) + 1) * 2.0 ** -53
+            dt = -po.port_log(u2) / total
+            t += dt
+            if ev.from_site >= 0:
+                events.append((rnd, hops, ev.from_site, ev.to_site, ev.species, u, total, dt))
+                hops += 1
+        evo[sector] += t
+    return events, evo
+
+
+def ak_sector(rnd):
+    return (0, 7, 2, 5, 3, 4, 1, 6)[rnd % 8]
+
+
+@pytest.mark.parametrize("model", [po.MODEL_PAIRBOND, po.MODEL_EAM])
+def test_per_hop_entry_points_follow_the_reference_loop(ak, model):
+    o = oracle_job(box=(16, 16, 16), model=model, n_vacancies=6, seed=9)
+    with ak.Engine() as eng:
+        device_job(eng, o, (16, 16, 16), model=model, seed=9)
+        eng.prepare()
+        rounds = 24
+        events, evo = _host_driven_loop(eng, 9, 3e-7, rounds)
+        o.run_rounds(rounds)
+        oe = o.events()
+        assert len(events) == len(oe) and len(oe) > 20
+        for a, b in zip(events, oe):
+            assert a[0] == b["round"] and a[2] == b["from_site"] and a[3] == b["to_site"] and a[4] == b["species"]
+            assert a[5] == b["u"] and a[6] == b["total"] and a[7] == b["dt"]
+        evo_o, _ = o.block_state()
+        assert np.array_equal(np.array(evo).view(np.uint64), evo_o[0].view(np.uint64))
+        assert np.array_equal(eng.occupancy(0), o.occupancy())
+
+
+def test_sector_overflow_is_reported(ak):
+    # 200 vacancies in a 16^3 box: more than 64 in one sector
+    o = oracle_job(box=(16, 16, 16), n_vacancies=600, model=po.MODEL_PAIRBOND, alloy=((po.FE, 1),))
+    with ak.Engine() as eng:
+        device_job(eng, o, (16, 16, 16), model=po.MODEL_PAIRBOND)
+        eng.prepare()
+        eng.run_rounds(1)
+        with pytest.raises(ak.AkmcError) as ei:
+            eng.sync()
+        assert ei.value.status == -7
