@@ -1,0 +1,407 @@
+"""Benchmark of the vacancy-hop path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scale|scale32|batched|serial]
+                    [--rounds-per-step R] [--impl b200|reference]
+
+One step = R sector rounds of the synchronous sublattice (R/8 sublattice time
+steps of window 3e-7 s) over the workload's jobs.  `value` is whole-job vacancy
+hops per second with the lattices resident in HBM; `e2e` is the same metric
+through the public C ABI with the lattice uploaded from pinned host memory and
+read back every step.  N > 1 runs independent replicas (one per GPU, seed 42 +
+rank): the path has no exchange step between jobs.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "misa-akmc-gpu_b200"))
+sys.path.insert(0, os.path.join(ROOT, "misa-akmc-gpu_b200", "python"))
+
+METRIC = "vacancy hops/s on 1 B200: plain FP64 vs batched FP32-comp; p50/p99 job latency"
+FE, CU, NI, MN = 1, 2, 4, 8
+QUATERNARY = ((FE, 9766), (CU, 134), (NI, 70), (MN, 30))
+
+
+# ---------------------------------------------------------------------------
+# workloads
+def _xoshiro(seed, tag):
+    M = (1 << 64) - 1
+
+    def mix(z):
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        return z ^ (z >> 31)
+
+    h = mix(seed ^ ((tag * 0xD1B54A32D192ED03) & M))
+    h = mix(h ^ (0x632BE59BD9B4E019))
+    s = []
+    for _ in range(4):
+        h = (h + 0x9E3779B97F4A7C15) & M
+        s.append(mix(h))
+
+    def rotl(x, k):
+        return ((x << k) | (x >> (64 - k))) & M
+
+    def nxt():
+        r = rotl((s[1] * 5) & M, 7) * 9 & M
+        t = (s[1] << 17) & M
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = rotl(s[3], 45)
+        return (r >> 11) * 2.0 ** -53
+
+    return nxt
+
+
+def workload_jobs(name, rank=0):
+    """List of job dicts: box, blocks, alloy, n_vacancies, temperature, precision, seed."""
+    seed = 42 + rank
+    if name in ("scale", "scale32"):
+        n = 256
+        nv = int(round(2e-5 * 2 * n ** 3))
+        return [dict(box=(n, n, n), blocks=(16, 16, 16), alloy=QUATERNARY, n_vacancies=nv, temperature=563.0,
+                     precision=0 if name == "scale" else 1, seed=seed)]
+    if name == "serial":
+        return [dict(box=(20, 20, 20), blocks=(1, 1, 1), alloy=((FE, 9866), (CU, 134)), n_vacancies=20,
+                     temperature=573.0, precision=0, seed=seed)]
+    if name == "batched":
+        draw = _xoshiro(seed, 7)
+        jobs = []
+        for i in range(512):
+            edge = int(round(math.exp(math.log(16) + (math.log(48) - math.log(16)) * draw())))
+            cu = 50 + int(round(100 * draw()))      # 0.5-1.5 at.% in 1e-4 units
+            ni = int(round(100 * draw()))           # 0-1 at.%
+            mn = int(round(50 * draw()))            # 0-0.5 at.%
+            temp = 473.0 + 200.0 * draw()
+            nb = 1 if edge <= 24 else 2
+            nv = max(1, int(round(1e-4 * 2 * edge ** 3)))
+            jobs.append(dict(box=(edge, edge, edge), blocks=(nb, nb, nb),
+                             alloy=((FE, 10000 - cu - ni - mn), (CU, cu), (NI, ni), (MN, mn)), n_vacancies=nv,
+                             temperature=temp, precision=1, seed=42 + i + 1000 * rank))
+        return jobs
+    raise SystemExit("unknown workload %s" % name)
+
+
+def algorithmic_bytes(hops, evals, nact_sum, eam=True):
+    """Canonical bytes of the path: per vacancy evaluation the 145-site footprint
+    (occupancy byte + int32 density) and 8 FP64 rates; per hop the 78-site density
+    refresh (read + write), the occupancy swap and the event; per hop the selection
+    scan over the sector's rates (64 B per vacancy)."""
+    if eam:
+        return evals * (145 + 145 * 4 + 64) + hops * (78 * 2 * 4 + 2 + 16) + 64 * nact_sum
+    return evals * (113 + 64) + hops * (2 + 16) + 64 * nact_sum
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.path = os.path.join("/tmp", "akmc_clocks_%d_%d.csv" % (os.getpid(), device))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(workload):
+    """DRAM bytes per hop-kernel launch from the committed ncu summary, if any."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "k_hop_traffic.json")))
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def build_engine(ak, jobs, device, stream, log=0):
+    eng = ak.Engine(device=device, stream=stream, event_log_capacity=log)
+    lattices = []
+    eam = ak.eam_johnson(42)
+    for j in jobs:
+        occ = ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"])
+        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=j["precision"],
+                            temperature=j["temperature"], seed=j["seed"], eam=eam)
+        eng.add_job(cfg, occ)
+        lattices.append(occ)
+    eng.prepare()
+    return eng, lattices
+
+
+def cpu_baseline(jobs, seconds=15.0, rounds_per_chunk=8):
+    """The oracle (the reference CPU path restated) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    j = jobs[0]
+    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=po.MODEL_EAM, precision=j["precision"],
+                         temperature=j["temperature"], seed=j["seed"], pot_seed=42, alloy=j["alloy"],
+                         n_vacancies=j["n_vacancies"], log_events=0)
+    o = po.Oracle(cfg)
+    t0 = time.perf_counter()
+    rounds = 0
+    while time.perf_counter() - t0 < seconds:
+        o.run_rounds(rounds_per_chunk)
+        rounds += rounds_per_chunk
+    dt = time.perf_counter() - t0
+    return {"value": o.hops / dt, "unit": "hops/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "oracle, job 0 of the workload (%s cells, %d blocks), first %d sector rounds, %d hops, %.1f s"
+                      % ("x".join(map(str, j["box"])), int(np.prod(j["blocks"])), rounds, o.hops, dt)}
+
+
+def run_reference(args, jobs):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    j = jobs[0]
+    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=po.MODEL_EAM, precision=j["precision"],
+                         temperature=j["temperature"], seed=j["seed"], pot_seed=42, alloy=j["alloy"],
+                         n_vacancies=j["n_vacancies"], log_events=0)
+    o = po.Oracle(cfg)
+    rounds = args.rounds_per_step
+    for _ in range(args.warmup):
+        o.run_rounds(rounds)
+    h0 = o.hops
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.run_rounds(rounds)
+    dt = time.perf_counter() - t0
+    value = (o.hops - h0) / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "hops/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if j["precision"] == 0 else "f32c",
+        "data": "synthetic", "config": config_of(args, jobs),
+        "cpu_baseline": {"value": value, "unit": "hops/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "oracle (reference CPU path restated, OpenMP over domain blocks), job 0, "
+                                   "%d timed steps of %d sector rounds" % (args.steps, rounds)},
+        "e2e": {"value": value, "unit": "hops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_of(args, jobs):
+    j = jobs[0]
+    c = {"workload": {"scale": "BCC 256^3 cells Fe-1.34Cu-0.7Ni-0.3Mn, 16^3-cell domain blocks x 8 sectors, "
+                               "671 vacancies, EAM, T=563 K",
+                      "scale32": "BCC 256^3 cells Fe-1.34Cu-0.7Ni-0.3Mn, 16^3-cell blocks, 671 vacancies, EAM "
+                                 "FP32-compensated, T=563 K",
+                      "batched": "512 boxes, edge log-uniform 16-48 cells, Cu 0.5-1.5 / Ni 0-1 / Mn 0-0.5 at.%, "
+                                 "vacancy fraction 1e-4, T 473-673 K, EAM FP32-compensated",
+                      "serial": "BCC 20^3 cells Fe-1.34Cu, 20 vacancies, single domain, EAM, T=573 K"}[args.workload],
+         "jobs": len(jobs), "sites": int(sum(2 * np.prod(x["box"]) for x in jobs)),
+         "vacancies": int(sum(x["n_vacancies"] for x in jobs)), "rounds_per_step": args.rounds_per_step,
+         "sector_window_s": 3e-7, "energy_model": "synthetic Johnson EAM (5 shells, rc 5.6 A)",
+         "parallelism": "replicas x%d" % args.gpus,
+         "l2": "inputs larger than L2 (occupancy + int32 density cache of %.0f MB)"
+               % (5 * sum(2 * np.prod(x["box"]) for x in jobs) / 1e6)}
+    if len(jobs) == 1:
+        c["box"] = list(j["box"])
+        c["blocks"] = list(j["blocks"])
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="scale", choices=["scale", "scale32", "batched", "serial"])
+    ap.add_argument("--rounds-per-step", type=int, default=256)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    jobs = workload_jobs(args.workload, rank)
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, workload_jobs(args.workload, 0))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import build as akbuild
+    import akmc_b200 as ak
+
+    if rank == 0 or not os.path.exists(ak.lib_path()):
+        akbuild.build()
+    if dist:
+        dist.barrier()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    eng, lattices = build_engine(ak, jobs, local, stream.cuda_stream)
+    R = args.rounds_per_step
+    eam = True
+
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        eng.run_rounds(R)
+    eng.sync()
+    sync_all()
+    c0 = eng.counters()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    sync_all()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        eng.run_rounds(R)
+    ev1.record(stream)
+    eng.sync()
+    sync_all()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    c1 = eng.counters()
+    hops = c1["hops"] - c0["hops"]
+    t = torch.tensor([ms, float(hops)], dtype=torch.float64, device="cuda")
+    if dist:
+        tmax = t.clone()
+        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
+        t = tmax
+    ms_all, hops_all = float(t[0]), float(t[1])
+    value = hops_all / (ms_all / 1e3)
+
+    # roofline pass: same workload continued, hop kernel timed with events around every launch
+    eng.set_kernel_timing(True)
+    r0 = eng.counters()
+    for _ in range(max(1, args.steps // 2)):
+        eng.run_rounds(R)
+    eng.sync()
+    r1 = eng.counters()
+    hop_ms, launches = eng.kernel_timing()
+    eng.set_kernel_timing(False)
+    rh = r1["hops"] - r0["hops"]
+    bytes_alg = algorithmic_bytes(rh, r1["evaluations"] - r0["evaluations"], r1["n_act_sum"] - r0["n_act_sum"], eam)
+    peak, peak_kind = peaks()
+    achieved = bytes_alg / (hop_ms / 1e3) / 1e9 if hop_ms > 0 else 0.0
+    traffic = traffic_per_launch(args.workload)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_hop",
+                "bytes_per_launch": bytes_alg / max(1, launches), "avg_launch_us": 1e3 * hop_ms / max(1, launches),
+                "hops_per_launch": rh / max(1, launches),
+                "e_hop": (r1["evaluations"] - r0["evaluations"]) / max(1, rh),
+                "n_act_per_hop": (r1["n_act_sum"] - r0["n_act_sum"]) / max(1, rh)}
+
+    # end to end through the C ABI: lattice from pinned host memory, R rounds, lattice back
+    pinned = [torch.from_numpy(occ).pin_memory() for occ in lattices]
+    outs = [torch.empty(occ.size, dtype=torch.uint8).pin_memory() for occ in lattices]
+    sync_all()
+    e0 = eng.counters()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for j, p in enumerate(pinned):
+            eng.load_occupancy(j, p.numpy())
+        eng.run_rounds(R)
+        eng.sync()
+        for j, o in enumerate(outs):
+            lib_occ = eng.occupancy(j)
+            o.numpy()[:] = lib_occ
+    sync_all()
+    e_dt = time.perf_counter() - t0
+    e1 = eng.counters()
+    e_hops = e1["hops"] - e0["hops"]
+    et = torch.tensor([e_dt, float(e_hops)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
+    e2e = {"value": float(et[1]) / float(et[0]), "unit": "hops/s",
+           "h2d_bytes_per_step": int(sum(o.size for o in lattices)), "d2h_bytes_per_step": int(sum(o.size for o in lattices)),
+           "note": "each step restarts the jobs from the host lattices (upload, density rebuild), runs R rounds and "
+                   "reads the lattices back"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "hops/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if jobs[0]["precision"] == 0 else "f32c", "data": "synthetic",
+            "config": config_of(args, jobs), "roofline": roofline, "e2e": e2e,
+            "gpu_launches": 3 * R * args.steps, "clocks": clk,
+            "hops_timed": int(hops_all),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(jobs)
+        print(json.dumps(line))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

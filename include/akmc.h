@@ -165,8 +165,22 @@ AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int6
 AKMC_API akmc_status akmc_get_block_clocks(akmc_ctx* ctx, int32_t job, double* evo, int64_t* hops, int32_t n_blocks);
 /* Copies the event log (all jobs, device order) and empties it. */
 AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t capacity, int64_t* n_out);
-/* Device-side counters: [0] hops, [1] rate evaluations, [2] rounds run, [3] blocks processed. */
-AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out4);
+/* Device-side counters: [0] hops, [1] vacancy rate evaluations, [2] rounds run,
+ * [3] active blocks processed, [4] sum over hops of the sector's vacancy count,
+ * [5] region sites staged into shared memory, [6] region sites written back, [7] reserved. */
+AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out8);
+
+/* Replaces the lattice of a prepared job (same box and vacancy count) and
+ * restarts it: density cache rebuilt on the device, clocks, rounds and RNG
+ * streams reset as after akmc_prepare.  gpu_prepare's lattice upload
+ * (gpu_simulate.hip:1771-1831) for a new box. */
+AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8_t* occ, int64_t n_sites);
+
+/* Kernel timing mode: while enabled, akmc_run_rounds launches each round on its
+ * own (no CUDA graph) with CUDA events around the hop kernel on the context
+ * stream; akmc_get_kernel_timing returns their summed time and the launch count. */
+AKMC_API akmc_status akmc_set_kernel_timing(akmc_ctx* ctx, int32_t enable);
+AKMC_API akmc_status akmc_get_kernel_timing(akmc_ctx* ctx, double* hop_kernel_ms, int64_t* hop_launches);
 
 /*
  * Per-hop entry points for a single-domain job, with the host driving the
@@ -192,6 +206,49 @@ AKMC_API akmc_status akmc_create_lattice(const int64_t box[3], const int32_t typ
 /* Isolated-Cu count (profiles/m_event_hook.cpp:17-55) and Cu cluster-size histogram (1nn). */
 AKMC_API akmc_status akmc_cluster_stats(const uint8_t* occ, const int64_t box[3], int64_t* isolated_cu, int64_t* hist,
                                         int64_t hist_len);
+
+/*
+ * config.yaml of the reference (profiles/config/config_parsing.cpp:54-230, keys of
+ * examples/config.yaml) plus an optional `kmc:` block read only by this library:
+ * energy_model (pairbond|eam), precision (fp64|fp32c), blocks [bx,by,bz],
+ * creation (reference|xoshiro), sector_window, hop_budget, seed, pot_seed.
+ */
+typedef struct akmc_run_config {
+  int64_t box[3];
+  double lattice_const;
+  double cutoff_radius;
+  int32_t create_random;
+  int32_t n_types;            /* single-atom alloy entries, YAML order */
+  int32_t type_codes[4];
+  int64_t ratio[4];
+  int64_t va_count;
+  int64_t seed_create_types, seed_create_vacancy, seed_event_selection, seed_time_inc;
+  double temperature, physics_time, attempt_freq, dpasm1;
+  int64_t steps_limit;
+  int32_t isgenr;
+  int32_t energy_model, precision, creation;
+  int32_t blocks[3];
+  int32_t reserved;
+  double sector_window;
+  int64_t hop_budget;
+  uint64_t seed, pot_seed;
+  int64_t dump_interval, logs_interval;
+  char dump_file_path[256];
+  char logs_file[256];
+} akmc_run_config;
+
+AKMC_API akmc_status akmc_config_parse(const char* yaml_text, akmc_run_config* out, char* err, int32_t errlen);
+/* The lattice of a config: creation = reference reproduces creation::createRandom's
+ * mt19937 draw order (ghost sites included, src/creation.cpp:18-164). */
+AKMC_API akmc_status akmc_config_lattice(const akmc_run_config* cfg, uint8_t* occ, int64_t n_sites);
+AKMC_API akmc_status akmc_config_job(const akmc_run_config* cfg, const akmc_eam_tables* eam, akmc_job_config* out);
+/* SubLattice::startTimeLoop (sublattice.inl:24-190) for a single-domain job,
+ * driven from the host over akmc_calculate / akmc_select_and_perform with the
+ * job's xoshiro selection and time streams; events and the 8 sector clocks out. */
+AKMC_API akmc_status akmc_host_time_loop(akmc_ctx* ctx, int32_t job, int64_t n_rounds, uint64_t seed, double window,
+                                         akmc_event* events, int64_t capacity, int64_t* n_events, double* evo8);
+/* LatticeDump::dump format (profiles/io/lattice_dump.cpp:14-62). */
+AKMC_API akmc_status akmc_dump_lattice(const uint8_t* occ, const int64_t box[3], int32_t ghost, const char* path);
 
 /* Device checks of the shared arithmetic: port_exp/port_log of x[i] on the GPU. */
 AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out);

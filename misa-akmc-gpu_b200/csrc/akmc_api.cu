@@ -82,6 +82,9 @@ struct akmc_ctx {
   std::vector<cudaEvent_t> ev;
   double hop_ms = 0.0;
   int64_t hop_launches = 0;
+  // host images of the initial device records (akmc_load_occupancy resets from them)
+  std::vector<JobDev> h_jobs;
+  std::vector<BlockDev> h_blocks;
 };
 
 namespace {
@@ -316,6 +319,11 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     nb += j.nblocks;
     nv += static_cast<int32_t>(j.nvac);
     max_region = std::max(max_region, region_sites(j));
+    for (size_t k = 0; k + 1 < j.split[0].size(); ++k) {
+      const int w = j.split[0][k + 1] - j.split[0][k];
+      if (2 * (w - w / 2 + 4) > 64)  // staged rows hold at most 64 sites (two per lane)
+        return fail(ctx, AKMC_EINVAL, "sector wider than 28 cells in x; use more domain blocks");
+    }
   }
   ctx->nblocks = nb;
   ctx->nvac = nv;
@@ -468,7 +476,55 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.api_total = ctx->d_api_total;
   a.api_event = ctx->d_api_event;
   CK(cudaStreamSynchronize(ctx->stream));
+  ctx->h_jobs = hj;
+  ctx->h_blocks = hb;
   ctx->prepared = true;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8_t* occ, int64_t n_sites) {
+  if (!ctx || !occ) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  if (n_sites != j.nsites) return fail(ctx, AKMC_EINVAL, "n_sites does not match the job");
+  CK(cudaSetDevice(ctx->cfg.device));
+  CK(cudaMemcpyAsync(j.d_occ, occ, static_cast<size_t>(n_sites), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_vac_count, 0, 4, ctx->stream));
+  int e = launch_collect_vacancies(j.d_occ, n_sites, ctx->d_vac_site + j.vac0, ctx->d_vac_job + j.vac0, job,
+                                   static_cast<int32_t>(j.nvac), ctx->d_vac_count, ctx->stream);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("collect vacancies: ") + cuda_name(e));
+  if (j.has_eam) {
+    e = launch_init_rho(j.d_occ, j.d_rho, 2 * static_cast<int32_t>(j.cfg.box[0]), static_cast<int32_t>(j.cfg.box[1]),
+                        static_cast<int32_t>(j.cfg.box[2]), ctx->d_pots + j.pot, ctx->d_geo, ctx->d_status,
+                        ctx->stream);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("init rho: ") + cuda_name(e));
+  }
+  CK(cudaMemcpyAsync(ctx->d_jobs + job, &ctx->h_jobs[static_cast<size_t>(job)], sizeof(JobDev), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks + j.block0, &ctx->h_blocks[static_cast<size_t>(j.block0)],
+                     static_cast<size_t>(j.nblocks) * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
+  int32_t count = 0;
+  CK(cudaMemcpyAsync(&count, ctx->d_vac_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (count != j.nvac)
+    return fail(ctx, AKMC_EINVAL, "the lattice must hold the job's " + std::to_string(j.nvac) + " vacancies, found " +
+                                      std::to_string(count));
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_set_kernel_timing(akmc_ctx* ctx, int32_t enable) {
+  if (!ctx) return AKMC_EINVAL;
+  ctx->timing = enable != 0;
+  ctx->hop_ms = 0.0;
+  ctx->hop_launches = 0;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_kernel_timing(akmc_ctx* ctx, double* hop_kernel_ms, int64_t* hop_launches) {
+  if (!ctx || !hop_kernel_ms || !hop_launches) return AKMC_EINVAL;
+  *hop_kernel_ms = ctx->hop_ms;
+  *hop_launches = ctx->hop_launches;
   return AKMC_OK;
 }
 
@@ -645,16 +701,16 @@ AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t cap
   return AKMC_OK;
 }
 
-AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out4) {
-  if (!ctx || !out4) return AKMC_EINVAL;
+AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out8) {
+  if (!ctx || !out8) return AKMC_EINVAL;
   if (!ctx->prepared) {
-    for (int i = 0; i < 4; ++i) out4[i] = 0;
+    for (int i = 0; i < 8; ++i) out8[i] = 0;
     return AKMC_OK;
   }
-  unsigned long long c[4];
+  unsigned long long c[8];
   CK(cudaMemcpyAsync(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  for (int i = 0; i < 4; ++i) out4[i] = static_cast<int64_t>(c[i]);
+  for (int i = 0; i < 8; ++i) out8[i] = static_cast<int64_t>(c[i]);
   return AKMC_OK;
 }
 

@@ -43,7 +43,13 @@ struct Potential {
   double b1[5][5], b2[5][5];  // pair-bond 1nn / 2nn tables (V, Fe, Cu, Ni, Mn)
   const double* Fcoef;      // kTabN x 4 doubles
   const FCell32* F32;       // kTabN cells
+  int32_t fwin0;            // first F-table cell of the shared-memory window
+  int32_t pad;
 };
+
+// F-table cells kept in shared memory: rho in [bulk Fe - 6, bulk Fe + 2]; cells
+// outside the window are read from global memory (same values, slower).
+constexpr int kFWin = 1024;
 
 struct JobDev {
   uint8_t* occ;
@@ -79,6 +85,7 @@ enum : uint32_t {
   kErrHopCap = 4u,
   kErrLogOverflow = 8u,
   kErrApiState = 16u,
+  kErrTimeout = 32u,
 };
 
 enum : int32_t { kModeRound = 0, kModeCalc = 1, kModeSelectPerform = 2 };

@@ -71,6 +71,49 @@ struct Smem {
   int32_t vidx[kMaxV], vloc[kMaxV], vlid[kMaxV], ord[kMaxV];
   uint8_t vact[kMaxV], vavail[kMaxV], vdirty[kMaxV], vpad[kMaxV];
   double rates[kMaxV][8];
+  alignas(16) unsigned char fwin[kFWin * 32];  // F-table window: double c0..c3 or FCell32 per cell
+  alignas(8) uint64_t mbar;                    // completion barrier of the window's bulk copy
+  uint32_t mbar_phase;
+  int32_t win_pot;                             // potential (and precision) the window holds
+};
+
+// --- bulk copy global -> shared with an mbarrier (cp.async.bulk, TMA unit) -----------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Waits for the barrier phase with an iteration limit; false when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// F-table access: cells inside the shared-memory window, the rest from global memory.
+struct FTab {
+  const unsigned char* win;
+  int kw0;
+  const double* g64;
+  const FCell32* g32;
+  unsigned int* status;
 };
 
 __device__ __forceinline__ int local_delta(int32_t w, const Region& R) {
@@ -106,26 +149,46 @@ __device__ __forceinline__ int sdelta(int32_t e) { return static_cast<int16_t>(e
 __device__ __forceinline__ int sshs(int32_t e) { return (e >> 16) & 0xf; }
 __device__ __forceinline__ int ssht(int32_t e) { return (e >> 20) & 0xf; }
 
-__device__ __forceinline__ double F64(const Potential& P, int32_t r, unsigned int* status) {
-  int k = r >> kRhoCellShift;
-  if (r < 0 || k > kTabN - 2) {
-    atomicOr(status, kErrRhoRange);
-    k = r < 0 ? 0 : kTabN - 2;
-  }
+__device__ __forceinline__ double F64(const FTab& T, int32_t r) {
+  const int k = r >> kRhoCellShift;
   const double p = static_cast<double>(r & kRhoFracMask) * 0x1p-17;
-  const double2* c = reinterpret_cast<const double2*>(P.Fcoef) + 2 * k;
-  const double2 lo = __ldg(c), hi = __ldg(c + 1);
+  const unsigned kk = static_cast<unsigned>(k - T.kw0);
+  double2 lo, hi;
+  if (kk < static_cast<unsigned>(kFWin)) {
+    const double2* c = reinterpret_cast<const double2*>(T.win) + 2 * kk;
+    lo = c[0];
+    hi = c[1];
+  } else {
+    int kc = k;
+    if (r < 0 || k > kTabN - 2) {
+      atomicOr(T.status, kErrRhoRange);
+      kc = r < 0 ? 0 : kTabN - 2;
+    }
+    const double2* c = reinterpret_cast<const double2*>(T.g64) + 2 * kc;
+    lo = __ldg(c);
+    hi = __ldg(c + 1);
+  }
   return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
 }
 
-__device__ __forceinline__ FCell32 cell32(const Potential& P, int32_t r, unsigned int* status) {
-  int k = r >> kRhoCellShift;
-  if (r < 0 || k > kTabN - 2) {
-    atomicOr(status, kErrRhoRange);
-    k = r < 0 ? 0 : kTabN - 2;
+__device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
+  const int k = r >> kRhoCellShift;
+  const unsigned kk = static_cast<unsigned>(k - T.kw0);
+  float4 a, b;
+  if (kk < static_cast<unsigned>(kFWin)) {
+    const float4* q = reinterpret_cast<const float4*>(T.win) + 2 * kk;
+    a = q[0];
+    b = q[1];
+  } else {
+    int kc = k;
+    if (r < 0 || k > kTabN - 2) {
+      atomicOr(T.status, kErrRhoRange);
+      kc = r < 0 ? 0 : kTabN - 2;
+    }
+    const float4* q = reinterpret_cast<const float4*>(T.g32 + kc);
+    a = __ldg(q);
+    b = __ldg(q + 1);
   }
-  const float4* q = reinterpret_cast<const float4*>(P.F32 + k);
-  const float4 a = __ldg(q), b = __ldg(q + 1);
   FCell32 c;
   c.hi = a.x; c.lo = a.y; c.c1 = a.z; c.c2 = a.w; c.c3 = b.x;
   c.pad0 = c.pad1 = c.pad2 = 0.f;
@@ -141,8 +204,8 @@ enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };
 //  EAM:       q sums sites i = q, q+4, ... of the jump's site list, merged
 //             (p0 + p2) + (p1 + p3), then the moving atom's own embedding change.
 template <int KIND>
-__device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const Potential& P,
-                             const JobDev& J, unsigned int* status) {
+__device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const FTab& FT,
+                             const JobDev& J) {
   const int lane = threadIdx.x & 31;
   const int b = lane >> 2, q = lane & 3;
   const int l = sm.vloc[k];
@@ -182,25 +245,37 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     const int X = species_index(Xc);
     if (avail) {
       const int32_t* L = sm.jl[p][b];
-      for (int i = q; i < kJumpN; i += 4) {
-        const int32_t e = L[i];
+      // site term (F(r + d) - F(r)) + (phi_s - phi_t); a vacancy contributes nothing
+      auto term = [&](int32_t e, bool& atom) {
         const int j = l + sdelta(e);
         const uint8_t o = occ_s[j];
-        if (o == kV) continue;
-        const int Y = species_index(o);
+        atom = o != kV;
+        const int Y = atom ? species_index(o) : 0;
         const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
         const int32_t d = sm.fq[X * 8 + ss] - sm.fq[X * 8 + st];
-        const double Fa = F64(P, r + d, status);
-        const double Fb = F64(P, r, status);
-        const double T = (Fa - Fb) + (sm.phi64[(X * 4 + Y) * 8 + ss] - sm.phi64[(X * 4 + Y) * 8 + st]);
-        acc += T;
+        const double Fa = F64(FT, r + d);
+        const double Fb = F64(FT, r);
+        return (Fa - Fb) + (sm.phi64[(X * 4 + Y) * 8 + ss] - sm.phi64[(X * 4 + Y) * 8 + st]);
+      };
+      int i = q;
+      for (; i + 4 < kJumpN; i += 8) {  // two sites per iteration, accumulated in list order
+        bool a0, a1;
+        const double T0 = term(L[i], a0);
+        const double T1 = term(L[i + 4], a1);
+        if (a0) acc += T0;
+        if (a1) acc += T1;
+      }
+      for (; i < kJumpN; i += 4) {
+        bool a0;
+        const double T0 = term(L[i], a0);
+        if (a0) acc += T0;
       }
     }
     const double s2 = acc + __shfl_xor_sync(kFull, acc, 2);
     const double tsum = s2 + __shfl_xor_sync(kFull, s2, 1);
     if (avail && q == 0) {
-      const double EX = F64(P, rho_s[l] - sm.fq[X * 8 + 1], status) - F64(P, rho_s[tl], status);
+      const double EX = F64(FT, rho_s[l] - sm.fq[X * 8 + 1]) - F64(FT, rho_s[tl]);
       dE = EX + tsum;
     }
   } else {
@@ -210,18 +285,29 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     const int X = species_index(Xc);
     if (avail) {
       const int32_t* L = sm.jl[p][b];
-      for (int i = q; i < kJumpN; i += 4) {
-        const int32_t e = L[i];
+      auto term = [&](int32_t e, bool& atom) {
         const int j = l + sdelta(e);
         const uint8_t o = occ_s[j];
-        if (o == kV) continue;
-        const int Y = species_index(o);
+        atom = o != kV;
+        const int Y = atom ? species_index(o) : 0;
         const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
         const int32_t r1 = r + (sm.fq[X * 8 + ss] - sm.fq[X * 8 + st]);
-        const float T = dF32(cell32(P, r1, status), cell32(P, r, status), r1, r) +
-                        (sm.phi32[(X * 4 + Y) * 8 + ss] - sm.phi32[(X * 4 + Y) * 8 + st]);
-        kahan_add(acc, T);
+        return dF32(cell32(FT, r1), cell32(FT, r), r1, r) +
+               (sm.phi32[(X * 4 + Y) * 8 + ss] - sm.phi32[(X * 4 + Y) * 8 + st]);
+      };
+      int i = q;
+      for (; i + 4 < kJumpN; i += 8) {
+        bool a0, a1;
+        const float T0 = term(L[i], a0);
+        const float T1 = term(L[i + 4], a1);
+        if (a0) kahan_add(acc, T0);
+        if (a1) kahan_add(acc, T1);
+      }
+      for (; i < kJumpN; i += 4) {
+        bool a0;
+        const float T0 = term(L[i], a0);
+        if (a0) kahan_add(acc, T0);
       }
     }
     Comp32 o2;
@@ -235,7 +321,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     if (avail && q == 0) {
       const int32_t r1 = rho_s[l] - sm.fq[X * 8 + 1];
       const int32_t r0 = rho_s[tl];
-      const float EX = dF32(cell32(P, r1, status), cell32(P, r0, status), r1, r0);
+      const float EX = dF32(cell32(FT, r1), cell32(FT, r0), r1, r0);
       const float dEf = EX + (m.s - m.c);
       dE = static_cast<double>(dEf);
     }
@@ -249,17 +335,6 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     sm.vavail[k] = m;
   }
   __syncwarp();
-}
-
-__device__ __forceinline__ int64_t global_site(const JobDev& J, const Region& R, int l) {
-  const int lx = l % R.LX;
-  const int t = l / R.LX;
-  const int ly = t % R.LY;
-  const int lz = t / R.LY;
-  const int X = wrap1(R.ox + lx, J.sx);
-  const int y = wrap1(R.oy + ly, J.sy);
-  const int z = wrap1(R.oz + lz, J.sz);
-  return static_cast<int64_t>(X) + static_cast<int64_t>(J.sx) * (y + static_cast<int64_t>(J.sy) * z);
 }
 
 __device__ __forceinline__ void local_cell(const Region& R, int l, int& cx, int& cy, int& cz) {
@@ -287,18 +362,64 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   Region R;
   make_region(B, sec, R);
+  // F-table window: one bulk copy issued by lane 0, overlapped with the staging below
+  const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
+  const bool need_win = eam && sm.win_pot != win_key;
+  __syncwarp();
+  if (need_win && lane == 0) {
+    const void* src = KIND == kEam32 ? static_cast<const void*>(P.F32 + P.fwin0)
+                                     : static_cast<const void*>(P.Fcoef + 4 * static_cast<int64_t>(P.fwin0));
+    bulk_load(sm.fwin, src, kFWin * 32u, &sm.mbar);
+  }
   load_tables(sm, P, *a.geo, R, eam);
+  FTab FT;
+  FT.win = sm.fwin;
+  FT.kw0 = P.fwin0;
+  FT.g64 = P.Fcoef;
+  FT.g32 = P.F32;
+  FT.status = a.status;
 
-  // stage the region: one row (fixed y, z) at a time, lanes along x
-  for (int row = 0; row < R.LY * R.LZ; ++row) {
-    const int ly = row % R.LY, lz = row / R.LY;
-    const int gy = wrap1(R.oy + ly, J.sy), gz = wrap1(R.oz + lz, J.sz);
-    const int64_t base = static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
-    for (int lx = lane; lx < R.LX; lx += 32) {
-      const int gx = wrap1(R.ox + lx, J.sx);
-      const int l = lx + R.LX * row;
-      occ_s[l] = J.occ[base + gx];
-      if (eam) rho_s[l] = J.rho[base + gx];
+  // stage the region: rows (fixed y, z) of LX <= 64 sites, lanes along x; eight rows
+  // of loads are issued before any shared-memory store so they are all in flight
+  {
+    const int nrows = R.LY * R.LZ;
+    const int gx0 = wrap1(R.ox + lane, J.sx), gx1 = wrap1(R.ox + lane + 32, J.sx);
+    const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
+    for (int row0 = 0; row0 < nrows; row0 += 8) {
+      uint8_t ov[8][2];
+      int32_t rv[8][2];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int row = row0 + k;
+        if (row < nrows) {
+          const int ly = row % R.LY, lz = row / R.LY;
+          const int gy = wrap1(R.oy + ly, J.sy), gz = wrap1(R.oz + lz, J.sz);
+          const int64_t base = static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
+          if (has0) {
+            ov[k][0] = J.occ[base + gx0];
+            if (eam) rv[k][0] = J.rho[base + gx0];
+          }
+          if (has1) {
+            ov[k][1] = J.occ[base + gx1];
+            if (eam) rv[k][1] = J.rho[base + gx1];
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int row = row0 + k;
+        if (row < nrows) {
+          const int l = lane + R.LX * row;
+          if (has0) {
+            occ_s[l] = ov[k][0];
+            if (eam) rho_s[l] = rv[k][0];
+          }
+          if (has1) {
+            occ_s[l + 32] = ov[k][1];
+            if (eam) rho_s[l + 32] = rv[k][1];
+          }
+        }
+      }
     }
   }
   const int cnt = min(B.cnt, kMaxV);
@@ -327,8 +448,24 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       sm.ord[j] = i;
     }
   }
+  if (need_win) {
+    bool ok = true;
+    if (lane == 0) {
+      ok = mbar_wait(&sm.mbar, sm.mbar_phase);
+      if (ok) {
+        sm.mbar_phase ^= 1u;
+        sm.win_pot = win_key;
+      } else {
+        atomicOr(a.status, kErrTimeout);
+        mbar_wait(&sm.mbar, sm.mbar_phase);  // bounded second wait for the copy in flight
+        sm.win_pot = -1;
+      }
+    }
+    ok = __shfl_sync(kFull, ok ? 1 : 0, 0) != 0;
+    if (!ok) return;
+  }
   __syncwarp();
-  for (int k = 0; k < cnt; ++k) eval_vacancy<KIND>(sm, occ_s, rho_s, k, P, J, a.status);
+  for (int k = 0; k < cnt; ++k) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
   int64_t evals = cnt;
 
   uint64_t xs[4], xt[4];
@@ -396,23 +533,39 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       const int p = s & 1;
       const int tl = s + sm.d1[p][bsel];
       Xc = occ_s[tl];
+      // global coordinates of s; the hop writes through to global memory (the staged
+      // regions of concurrent blocks are disjoint, so global stays the shared truth)
+      from_g = sm.vlid[ksel];
+      const int sX = static_cast<int>(from_g % J.sx);
+      const int sT = static_cast<int>(from_g / J.sx);
+      const int sY = sT % J.sy, sZ = sT / J.sy;
+      auto gsite = [&](int32_t w) {
+        const int gx = wrap1(sX + unpack_dx(w), J.sx), gy = wrap1(sY + unpack_dy(w), J.sy),
+                  gz = wrap1(sZ + unpack_dz(w), J.sz);
+        return static_cast<int64_t>(gx) + static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
+      };
+      to_g = gsite(a.geo->nn1[p][bsel]);
       __syncwarp();
       if (lane == 0) {
         occ_s[tl] = kV;
         occ_s[s] = Xc;
+        J.occ[to_g] = kV;
+        J.occ[from_g] = Xc;
       }
       if (eam) {
         const int X = species_index(Xc);
         for (int i = lane; i < kRefreshN; i += 32) {
           const int32_t e = sm.rl[p][bsel][i];
-          rho_s[s + sdelta(e)] += sm.fq[X * 8 + sshs(e)] - sm.fq[X * 8 + ssht(e)];
+          const int j = s + sdelta(e);
+          const int32_t v = rho_s[j] + (sm.fq[X * 8 + sshs(e)] - sm.fq[X * 8 + ssht(e)]);
+          rho_s[j] = v;
+          J.rho[gsite(a.geo->refresh[p][bsel][i])] = v;
         }
       }
       __syncwarp();
       if (lane == 0) {
-        from_g = sm.vlid[ksel];
-        to_g = global_site(J, R, tl);
         sm.vloc[ksel] = tl;
+        sm.vlid[ksel] = static_cast<int32_t>(to_g);
         int cx, cy, cz;
         local_cell(R, tl, cx, cy, cz);
         const bool in = cx >= 2 && cx < 2 + R.w[0] && cy >= 2 && cy < 2 + R.w[1] && cz >= 2 && cz < 2 + R.w[2];
@@ -421,7 +574,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
         --nord;
         if (in) {
-          sm.vlid[ksel] = static_cast<int32_t>(to_g);
           int j = nord;
           while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[ksel]) {
             sm.ord[j] = sm.ord[j - 1];
@@ -449,7 +601,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       __syncwarp();
       for (int k = 0; k < cnt; ++k) {
         if (!sm.vdirty[k]) continue;
-        eval_vacancy<KIND>(sm, occ_s, rho_s, k, P, J, a.status);
+        eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
         if (lane == 0) sm.vdirty[k] = 0;
         __syncwarp();
       }
@@ -526,21 +678,11 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     atomicAdd(a.counters + 3, 1ull);
     atomicAdd(a.counters + 4, static_cast<unsigned long long>(nact_sum));
     atomicAdd(a.counters + 5, static_cast<unsigned long long>(R.n));
-    if (nh) atomicAdd(a.counters + 6, static_cast<unsigned long long>(R.n));
+    if (nh) atomicAdd(a.counters + 6, static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2)));
   }
   if (nh == 0) return;
-  for (int i = lane; i < cnt; i += 32) a.vac_site[sm.vidx[i]] = static_cast<int32_t>(global_site(J, R, sm.vloc[i]));
-  for (int row = 0; row < R.LY * R.LZ; ++row) {
-    const int ly = row % R.LY, lz = row / R.LY;
-    const int gy = wrap1(R.oy + ly, J.sy), gz = wrap1(R.oz + lz, J.sz);
-    const int64_t base = static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
-    for (int lx = lane; lx < R.LX; lx += 32) {
-      const int gx = wrap1(R.ox + lx, J.sx);
-      const int l = lx + R.LX * row;
-      J.occ[base + gx] = occ_s[l];
-      if (eam) J.rho[base + gx] = rho_s[l];
-    }
-  }
+  // the lattice was written through at every hop; only the vacancy positions remain
+  for (int i = lane; i < cnt; i += 32) a.vac_site[sm.vidx[i]] = sm.vlid[i];
 }
 
 __device__ __forceinline__ void carve(uint8_t* smem, int nreg, Smem*& sm, uint8_t*& occ_s, int32_t*& rho_s) {
@@ -598,9 +740,21 @@ __global__ void k_bucket(RoundArgs a) {
   }
 }
 
+__device__ void init_cta_smem(uint8_t* smem) {
+  Smem* sm = reinterpret_cast<Smem*>(smem);
+  if (threadIdx.x == 0) {
+    sm->win_pot = -1;
+    sm->mbar_phase = 0;
+    mbar_init(&sm->mbar);
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(32) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
+  if (static_cast<int>(blockIdx.x) >= na) return;
+  init_cta_smem(smem);
   for (int item = blockIdx.x; item < na; item += gridDim.x) {
     dispatch_block(a, a.active[item], smem);
     __syncwarp();
@@ -650,6 +804,7 @@ __global__ void k_api_block(RoundArgs a) {
     }
     return;
   }
+  init_cta_smem(smem);
   dispatch_block(a, J.block0, smem);
 }
 

@@ -192,6 +192,11 @@ int build_potential(const akmc_eam_tables* t, Potential& P, std::vector<double>&
     rmax += static_cast<int64_t>(counts[i]) * m;
   }
   if ((rmax >> kRhoCellShift) > kTabN - 3) return -2;
+  // shared-memory window of the F table around the density of bulk Fe
+  int64_t rbulk = 0;
+  for (int i = 0; i < nsh; ++i) rbulk += static_cast<int64_t>(counts[i]) * P.fq[0][i + 1];
+  const int kb = static_cast<int>(rbulk >> kRhoCellShift);
+  P.fwin0 = std::max(1, std::min(kb - (3 * kFWin) / 4, kTabN - 2 - kFWin));
   for (int k = 0; k + 1 < kTabN; ++k) {
     double c[4];
     cell_coefs(t->F, kTabN, k, c);

@@ -129,6 +129,42 @@ class ContextConfig(C.Structure):
     ]
 
 
+class RunConfig(C.Structure):
+    _fields_ = [
+        ("box", C.c_int64 * 3),
+        ("lattice_const", C.c_double),
+        ("cutoff_radius", C.c_double),
+        ("create_random", C.c_int32),
+        ("n_types", C.c_int32),
+        ("type_codes", C.c_int32 * 4),
+        ("ratio", C.c_int64 * 4),
+        ("va_count", C.c_int64),
+        ("seed_create_types", C.c_int64),
+        ("seed_create_vacancy", C.c_int64),
+        ("seed_event_selection", C.c_int64),
+        ("seed_time_inc", C.c_int64),
+        ("temperature", C.c_double),
+        ("physics_time", C.c_double),
+        ("attempt_freq", C.c_double),
+        ("dpasm1", C.c_double),
+        ("steps_limit", C.c_int64),
+        ("isgenr", C.c_int32),
+        ("energy_model", C.c_int32),
+        ("precision", C.c_int32),
+        ("creation", C.c_int32),
+        ("blocks", C.c_int32 * 3),
+        ("reserved", C.c_int32),
+        ("sector_window", C.c_double),
+        ("hop_budget", C.c_int64),
+        ("seed", C.c_uint64),
+        ("pot_seed", C.c_uint64),
+        ("dump_interval", C.c_int64),
+        ("logs_interval", C.c_int64),
+        ("dump_file_path", C.c_char * 256),
+        ("logs_file", C.c_char * 256),
+    ]
+
+
 # every symbol include/akmc.h declares, with (restype, argtypes)
 _vp, _i32, _i64, _u64, _d = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_double
 SIGNATURES = {
@@ -156,7 +192,44 @@ SIGNATURES = {
     "akmc_create_lattice": (C.c_int, [_vp, _vp, _vp, _i64, _u64, _vp, _i64]),
     "akmc_cluster_stats": (C.c_int, [_vp, _vp, C.POINTER(_i64), _vp, _i64]),
     "akmc_device_math": (C.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "akmc_load_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
+    "akmc_set_kernel_timing": (C.c_int, [_vp, _i32]),
+    "akmc_get_kernel_timing": (C.c_int, [_vp, C.POINTER(_d), C.POINTER(_i64)]),
+    "akmc_config_parse": (C.c_int, [C.c_char_p, C.POINTER(RunConfig), C.c_char_p, _i32]),
+    "akmc_config_lattice": (C.c_int, [C.POINTER(RunConfig), _vp, _i64]),
+    "akmc_config_job": (C.c_int, [C.POINTER(RunConfig), C.POINTER(EamTables), C.POINTER(JobConfig)]),
+    "akmc_host_time_loop": (C.c_int, [_vp, _i32, _i64, _u64, _d, _vp, _i64, C.POINTER(_i64), _vp]),
+    "akmc_dump_lattice": (C.c_int, [_vp, _vp, _i32, C.c_char_p]),
 }
+
+
+def config_parse(text):
+    cfg = RunConfig()
+    err = C.create_string_buffer(256)
+    rc = lib().akmc_config_parse(text.encode() if isinstance(text, str) else text, C.byref(cfg), err, 256)
+    if rc:
+        raise AkmcError(rc, err.value.decode())
+    return cfg
+
+
+def config_lattice(cfg):
+    n = int(2 * cfg.box[0] * cfg.box[1] * cfg.box[2])
+    occ = np.empty(n, np.uint8)
+    _check(lib().akmc_config_lattice(C.byref(cfg), _ptr(occ), n))
+    return occ
+
+
+def config_job(cfg, eam=None):
+    out = JobConfig()
+    _check(lib().akmc_config_job(C.byref(cfg), C.byref(eam) if eam is not None else None, C.byref(out)))
+    out._eam_ref = eam
+    return out
+
+
+def dump_lattice(occ, box, path, ghost=2):
+    occ = np.ascontiguousarray(occ, np.uint8)
+    box = np.asarray(box, np.int64)
+    _check(lib().akmc_dump_lattice(_ptr(occ), _ptr(box), ghost, path.encode()))
 
 _lib = None
 
@@ -344,9 +417,23 @@ class Engine:
         return out[: n.value].copy()
 
     def counters(self):
-        out = np.zeros(4, np.int64)
+        out = np.zeros(8, np.int64)
         self._ck(lib().akmc_get_counters(self.h, _ptr(out)))
-        return dict(hops=int(out[0]), evaluations=int(out[1]), rounds=int(out[2]), blocks=int(out[3]))
+        return dict(hops=int(out[0]), evaluations=int(out[1]), rounds=int(out[2]), blocks=int(out[3]),
+                    n_act_sum=int(out[4]), staged_sites=int(out[5]), written_sites=int(out[6]))
+
+    def load_occupancy(self, job, occ):
+        occ = np.ascontiguousarray(occ, np.uint8)
+        self._ck(lib().akmc_load_occupancy(self.h, job, _ptr(occ), occ.size))
+
+    def set_kernel_timing(self, enable):
+        self._ck(lib().akmc_set_kernel_timing(self.h, int(enable)))
+
+    def kernel_timing(self):
+        ms = C.c_double(0.0)
+        n = C.c_int64(0)
+        self._ck(lib().akmc_get_kernel_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def calculate(self, job, sector_id):
         t = C.c_double(0.0)
@@ -357,6 +444,14 @@ class Engine:
         ev = Event()
         self._ck(lib().akmc_select_and_perform(self.h, job, sector_id, u, C.byref(ev)))
         return ev
+
+    def host_time_loop(self, job, n_rounds, seed, window=3e-7, capacity=1 << 20):
+        ev = np.empty(capacity, EVENT_DTYPE)
+        n = C.c_int64(0)
+        evo = np.zeros(8, np.float64)
+        self._ck(lib().akmc_host_time_loop(self.h, job, n_rounds, seed, window, _ptr(ev), capacity, C.byref(n),
+                                           _ptr(evo)))
+        return ev[: n.value].copy(), evo
 
     def device_math(self, x):
         x = np.ascontiguousarray(x, np.float64)
