@@ -170,6 +170,13 @@ AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t cap
  * [5] region sites staged into shared memory, [6] region sites written back, [7] reserved. */
 AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out8);
 
+/* Cycle profile of the hop kernel's phases (thread 0, summed over blocks): [0] staging,
+ * [1] list sort and table window, [2] first evaluations, [3] selection, [4] perform,
+ * [5] re-evaluation and clock, [6] tail; EAM FP64 evaluation sub-phases: [8] site loop,
+ * [9] butterfly, [10] own-embedding term, [11] rate.  All zero unless the library was
+ * built with -DAKMC_PHASE_PROFILE. */
+AKMC_API akmc_status akmc_get_phase_cycles(akmc_ctx* ctx, int64_t* out16);
+
 /* Replaces the lattice of a prepared job (same box and vacancy count) and
  * restarts it: density cache rebuilt on the device, clocks, rounds and RNG
  * streams reset as after akmc_prepare.  gpu_prepare's lattice upload

@@ -42,8 +42,9 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in _inputs())
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
+def build(force=False, verbose=False, extra_flags=(), lib_path=None):
+    lib = lib_path or LIB
+    if not force and not extra_flags and up_to_date():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(HERE, "_build")
@@ -58,22 +59,22 @@ def build(force=False, verbose=False):
         "-fPIC,-fvisibility=hidden,-ffp-contract=off",
         "-I" + os.path.join(ROOT, "include"),
         "-I" + CSRC,
-    ] + ARCH
+    ] + ARCH + list(extra_flags)
     for s in SOURCES:
         src = os.path.join(CSRC, s)
         if not os.path.exists(src):
             continue
-        obj = os.path.join(objdir, s + ".o")
+        obj = os.path.join(objdir, s + (".prof" if extra_flags else "") + ".o")
         cmd = [nvcc()] + common + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lpthread"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", lib] + objs + ["-lpthread"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

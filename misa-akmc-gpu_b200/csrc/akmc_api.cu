@@ -340,7 +340,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device));
   int smem_sm = 0;
   CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
-  int per_sm = std::max(1, std::min(32, static_cast<int>(smem_sm / (ctx->smem + 1024))));
+  // 256-thread CTAs at <= 128 registers: at most two per SM
+  int per_sm = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
   ctx->hop_grid = std::max(1, std::min(nb, sms * per_sm));
 
   // geometry and potentials
@@ -427,7 +428,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(&ctx->d_active, static_cast<size_t>(nb)));
   CK(dalloc(&ctx->d_n_active, 1));
   CK(dalloc(&ctx->d_status, 1));
-  CK(dalloc(&ctx->d_counters, 8));
+  CK(dalloc(&ctx->d_counters, 24));
   CK(dalloc(&ctx->d_vac_count, 1));
   CK(dalloc(&ctx->d_log_count, 1));
   CK(dalloc(&ctx->d_api_total, 1));
@@ -441,7 +442,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   }
   CK(cudaMemsetAsync(ctx->d_n_active, 0, 4, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_counters, 0, 64, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_counters, 0, 192, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_log_count, 0, 8, ctx->stream));
   for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
     HostJob& j = ctx->jobs[ji];
@@ -698,6 +699,17 @@ AKMC_API akmc_status akmc_get_events(akmc_ctx* ctx, akmc_event* out, int64_t cap
   CK(cudaStreamSynchronize(ctx->stream));
   *n_out = m;
   if (static_cast<int64_t>(n) > ctx->cfg.event_log_capacity) return fail(ctx, AKMC_EOVERFLOW, "event log overflowed");
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_phase_cycles(akmc_ctx* ctx, int64_t* out16) {
+  if (!ctx || !out16) return AKMC_EINVAL;
+  for (int i = 0; i < 16; ++i) out16[i] = 0;
+  if (!ctx->prepared) return AKMC_OK;
+  unsigned long long c[16];
+  CK(cudaMemcpyAsync(c, ctx->d_counters + 8, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < 16; ++i) out16[i] = static_cast<int64_t>(c[i]);
   return AKMC_OK;
 }
 

@@ -4,11 +4,12 @@
 // runs as three launches:
 //   k_bucket   one thread per vacancy: find its domain block, keep it if it lies in
 //              the block's active sector, append it to the block's list;
-//   k_hop      one warp per active block: stage the sector plus a 2-cell halo
-//              (occupancy bytes and the int32 density cache) into shared memory,
-//              run the hop loop there (rates, ordered total, selection, perform with
-//              density refresh, recompute of the vacancies the hop touched, clock),
-//              write the region back;
+//   k_hop      one CTA of 8 warps per active block: stage the sector plus a 2-cell
+//              halo (occupancy bytes and the int32 density cache) into shared memory
+//              and run the hop loop there.  Warp w evaluates jump direction w of a
+//              vacancy (its 32 lanes split the 76 sites of the jump); thread 0 forms
+//              the ordered total, selects, and keeps the vacancy list; each hop writes
+//              its two occupancy bytes and 78 densities through to global memory;
 //   k_finalize one thread per block: clock of blocks without vacancies, next round.
 // Concurrently active sectors are at least 4 cells apart, so the staged regions of
 // different blocks never overlap and no atomics are needed on the lattice.
@@ -22,6 +23,8 @@ namespace akmc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kThreads = 288;  // warps 0..7 evaluate jump directions 0..7; warp 8 controls
+constexpr int kCtl = 256;      // control thread: first lane of warp 8
 
 __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >= m ? v - m : v); }
 
@@ -58,7 +61,7 @@ __device__ __forceinline__ void make_region(const BlockDev& B, int sec, Region& 
   R.n = R.LX * R.LY * R.LZ;
 }
 
-// Shared-memory working set of one warp (followed by the staged region).
+// Shared-memory working set of one CTA (followed by the staged region).
 struct Smem {
   double b1[25], b2[25];
   double phi64[4 * 4 * 8];
@@ -69,12 +72,21 @@ struct Smem {
   int32_t jl[2][8][kJumpN];     // int16 delta | sh_s << 16 | sh_t << 20
   int32_t rl[2][8][kRefreshN];
   int32_t vidx[kMaxV], vloc[kMaxV], vlid[kMaxV], ord[kMaxV];
-  uint8_t vact[kMaxV], vavail[kMaxV], vdirty[kMaxV], vpad[kMaxV];
+  int16_t vcx[kMaxV], vcy[kMaxV], vcz[kMaxV];  // local coordinates (x in doubled sites)
+  int32_t vgx[kMaxV], vgy[kMaxV], vgz[kMaxV];  // global coordinates
+  uint8_t vdirty[kMaxV];
+  uint8_t vavb[kMaxV][8];       // jump b of vacancy k available (target is an atom)
   double rates[kMaxV][8];
   alignas(16) unsigned char fwin[kFWin * 32];  // F-table window: double c0..c3 or FCell32 per cell
   alignas(8) uint64_t mbar;                    // completion barrier of the window's bulk copy
   uint32_t mbar_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
+  // hop-loop control, written by thread 0 between barriers
+  double ctl_total, ctl_u, ctl_time;
+  int64_t ctl_from, ctl_to;
+  int32_t ctl_ksel, ctl_bsel, ctl_nord, ctl_nd, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop;
+  int32_t ctl_gx, ctl_gy, ctl_gz;
+  uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
 };
 
 // --- bulk copy global -> shared with an mbarrier (cp.async.bulk, TMA unit) -----------
@@ -114,32 +126,55 @@ struct FTab {
   const double* g64;
   const FCell32* g32;
   unsigned int* status;
+  unsigned long long* prof;  // sub-phase cycles of the evaluation (profiling builds)
+  double* fc;                // F(rho) of every staged site (FP64 form)
 };
+
+#ifdef AKMC_PHASE_PROFILE
+#define EVAL_T(i)                                                                       \
+  do {                                                                                  \
+    if (threadIdx.x == 0) {                                                             \
+      const long long t_ = clock64();                                                   \
+      atomicAdd(FT.prof + (i), static_cast<unsigned long long>(t_ - tev));              \
+      tev = t_;                                                                         \
+    }                                                                                   \
+  } while (0)
+#else
+#define EVAL_T(i) \
+  do {            \
+  } while (0)
+#endif
 
 __device__ __forceinline__ int local_delta(int32_t w, const Region& R) {
   return unpack_dx(w) + R.LX * (unpack_dy(w) + R.LY * unpack_dz(w));
 }
 
+// Region layout after Smem: int32 densities, double F(rho) cache (16-byte aligned), bytes.
+__device__ __forceinline__ double* fcache_of(int32_t* rho_s, int nreg) {
+  return reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(rho_s) +
+                                   ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15)));
+}
+
 __device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, const Region& R, bool eam) {
-  const int lane = threadIdx.x;
-  for (int i = lane; i < 25; i += 32) {
-    sm.b1[i] = P.b1[i / 5][i % 5];
-    sm.b2[i] = P.b2[i / 5][i % 5];
+  const int tid = threadIdx.x;
+  if (tid < 25) {
+    sm.b1[tid] = P.b1[tid / 5][tid % 5];
+    sm.b2[tid] = P.b2[tid / 5][tid % 5];
   }
-  for (int i = lane; i < 128; i += 32) {
-    sm.phi64[i] = (&P.phi64[0][0][0])[i];
-    sm.phi32[i] = (&P.phi32[0][0][0])[i];
+  if (tid < 128) {
+    sm.phi64[tid] = (&P.phi64[0][0][0])[tid];
+    sm.phi32[tid] = (&P.phi32[0][0][0])[tid];
   }
-  if (lane < 32) sm.fq[lane] = (&P.fq[0][0])[lane];
-  if (lane < 16) sm.d1[lane >> 3][lane & 7] = local_delta(G.nn1[lane >> 3][lane & 7], R);
-  if (lane < 6) sm.d2[lane] = local_delta(G.nn2[lane], R);
+  if (tid < 32) sm.fq[tid] = (&P.fq[0][0])[tid];
+  if (tid < 16) sm.d1[tid >> 3][tid & 7] = local_delta(G.nn1[tid >> 3][tid & 7], R);
+  if (tid < 6) sm.d2[tid] = local_delta(G.nn2[tid], R);
   if (eam) {
-    for (int i = lane; i < 2 * 8 * kJumpN; i += 32) {
-      const int32_t w = (&G.jump[0][0][0])[i];
+    for (int i = tid; i < 2 * 8 * kJumpN; i += kThreads) {
+      const int32_t w = __ldg(&G.jump[0][0][0] + i);
       (&sm.jl[0][0][0])[i] = (local_delta(w, R) & 0xffff) | (unpack_sh_s(w) << 16) | (unpack_sh_t(w) << 20);
     }
-    for (int i = lane; i < 2 * 8 * kRefreshN; i += 32) {
-      const int32_t w = (&G.refresh[0][0][0])[i];
+    for (int i = tid; i < 2 * 8 * kRefreshN; i += kThreads) {
+      const int32_t w = __ldg(&G.refresh[0][0][0] + i);
       (&sm.rl[0][0][0])[i] = (local_delta(w, R) & 0xffff) | (unpack_sh_s(w) << 16) | (unpack_sh_t(w) << 20);
     }
   }
@@ -151,7 +186,8 @@ __device__ __forceinline__ int ssht(int32_t e) { return (e >> 20) & 0xf; }
 
 __device__ __forceinline__ double F64(const FTab& T, int32_t r) {
   const int k = r >> kRhoCellShift;
-  const double p = static_cast<double>(r & kRhoFracMask) * 0x1p-17;
+  // p = (r mod 2^17) * 2^-17, built in the exponent field: 1 + m 2^-17 minus 1 (both exact)
+  const double p = __hiloint2double(0x3FF00000 | ((r & kRhoFracMask) << 3), 0) - 1.0;
   const unsigned kk = static_cast<unsigned>(k - T.kw0);
   double2 lo, hi;
   if (kk < static_cast<unsigned>(kFWin)) {
@@ -197,26 +233,31 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
 
 enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };
 
-// Rates of vacancy k of the list, all 8 jumps, warp-collective.
-// Lane = 4 b + q: jump b, quarter q.
-//  pair-bond: q selects one of the four bond counts of VacRatesSolver::deltaE
+// Rates of vacancy k, all 8 jumps, CTA-collective (no barrier inside; the caller
+// synchronises before the rates are read).  Warp b evaluates jump b.
+//  pair-bond: lanes 0..3 run the four bond counts of VacRatesSolver::deltaE
 //             (vacancy_rates_solver.cpp:45-116), each summed in the reference order;
-//  EAM:       q sums sites i = q, q+4, ... of the jump's site list, merged
-//             (p0 + p2) + (p1 + p3), then the moving atom's own embedding change.
+//  EAM:       lane q sums sites i = q, q+32, q+64 of the jump's list; the 32 partials
+//             merge by a xor butterfly (16, 8, 4, 2, 1), then the moving atom's own
+//             embedding change is added.
 template <int KIND>
 __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const FTab& FT,
                              const JobDev& J) {
   const int lane = threadIdx.x & 31;
-  const int b = lane >> 2, q = lane & 3;
+  const int b = threadIdx.x >> 5;
+  const int q = lane;
   const int l = sm.vloc[k];
   const int p = l & 1;
   const int tl = l + sm.d1[p][b];
   const uint8_t Xc = occ_s[tl];
   const bool avail = is_atom(Xc);
   double dE = 0.0;
+#ifdef AKMC_PHASE_PROFILE
+  long long tev = clock64();
+#endif
   if (KIND == kPairBond) {
     double energy = 0.0;
-    if (avail) {
+    if (avail && q < 4) {
       const bool at_t = (q & 1) != 0;
       const int center = at_t ? tl : l;
       const int pc = at_t ? (p ^ 1) : p;
@@ -245,39 +286,31 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     const int X = species_index(Xc);
     if (avail) {
       const int32_t* L = sm.jl[p][b];
-      // site term (F(r + d) - F(r)) + (phi_s - phi_t); a vacancy contributes nothing
-      auto term = [&](int32_t e, bool& atom) {
+#pragma unroll 3
+      for (int i = q; i < kJumpN; i += 32) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
+        const int32_t e = L[i];
         const int j = l + sdelta(e);
         const uint8_t o = occ_s[j];
-        atom = o != kV;
-        const int Y = atom ? species_index(o) : 0;
         const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
         const int32_t d = sm.fq[X * 8 + ss] - sm.fq[X * 8 + st];
         const double Fa = F64(FT, r + d);
-        const double Fb = F64(FT, r);
-        return (Fa - Fb) + (sm.phi64[(X * 4 + Y) * 8 + ss] - sm.phi64[(X * 4 + Y) * 8 + st]);
-      };
-      int i = q;
-      for (; i + 4 < kJumpN; i += 8) {  // two sites per iteration, accumulated in list order
-        bool a0, a1;
-        const double T0 = term(L[i], a0);
-        const double T1 = term(L[i + 4], a1);
-        if (a0) acc += T0;
-        if (a1) acc += T1;
-      }
-      for (; i < kJumpN; i += 4) {
-        bool a0;
-        const double T0 = term(L[i], a0);
-        if (a0) acc += T0;
+        const double Fb = FT.fc[j];  // F(rho_j), cached
+        if (o != kV) {
+          const int Y = species_index(o);
+          acc += (Fa - Fb) + (sm.phi64[(X * 4 + Y) * 8 + ss] - sm.phi64[(X * 4 + Y) * 8 + st]);
+        }
       }
     }
-    const double s2 = acc + __shfl_xor_sync(kFull, acc, 2);
-    const double tsum = s2 + __shfl_xor_sync(kFull, s2, 1);
+#pragma unroll
+    EVAL_T(0);
+    for (int m = 16; m >= 1; m >>= 1) acc = acc + __shfl_xor_sync(kFull, acc, m);
+    EVAL_T(1);
     if (avail && q == 0) {
-      const double EX = F64(FT, rho_s[l] - sm.fq[X * 8 + 1]) - F64(FT, rho_s[tl]);
-      dE = EX + tsum;
+      const double EX = F64(FT, rho_s[l] - sm.fq[X * 8 + 1]) - FT.fc[tl];
+      dE = EX + acc;
     }
+    EVAL_T(2);
   } else {
     Comp32 acc;
     acc.s = 0.f;
@@ -285,70 +318,71 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     const int X = species_index(Xc);
     if (avail) {
       const int32_t* L = sm.jl[p][b];
-      auto term = [&](int32_t e, bool& atom) {
+#pragma unroll 3
+      for (int i = q; i < kJumpN; i += 32) {
+        const int32_t e = L[i];
         const int j = l + sdelta(e);
         const uint8_t o = occ_s[j];
-        atom = o != kV;
-        const int Y = atom ? species_index(o) : 0;
         const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
         const int32_t r1 = r + (sm.fq[X * 8 + ss] - sm.fq[X * 8 + st]);
-        return dF32(cell32(FT, r1), cell32(FT, r), r1, r) +
-               (sm.phi32[(X * 4 + Y) * 8 + ss] - sm.phi32[(X * 4 + Y) * 8 + st]);
-      };
-      int i = q;
-      for (; i + 4 < kJumpN; i += 8) {
-        bool a0, a1;
-        const float T0 = term(L[i], a0);
-        const float T1 = term(L[i + 4], a1);
-        if (a0) kahan_add(acc, T0);
-        if (a1) kahan_add(acc, T1);
-      }
-      for (; i < kJumpN; i += 4) {
-        bool a0;
-        const float T0 = term(L[i], a0);
-        if (a0) kahan_add(acc, T0);
+        const float dF = dF32(cell32(FT, r1), cell32(FT, r), r1, r);
+        if (o != kV) {
+          const int Y = species_index(o);
+          kahan_add(acc, dF + (sm.phi32[(X * 4 + Y) * 8 + ss] - sm.phi32[(X * 4 + Y) * 8 + st]));
+        }
       }
     }
-    Comp32 o2;
-    o2.s = __shfl_xor_sync(kFull, acc.s, 2);
-    o2.c = __shfl_xor_sync(kFull, acc.c, 2);
-    Comp32 m = comp_merge(acc, o2);
-    Comp32 o1;
-    o1.s = __shfl_xor_sync(kFull, m.s, 1);
-    o1.c = __shfl_xor_sync(kFull, m.c, 1);
-    m = comp_merge(m, o1);
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+      Comp32 o;
+      o.s = __shfl_xor_sync(kFull, acc.s, m);
+      o.c = __shfl_xor_sync(kFull, acc.c, m);
+      acc = comp_merge(acc, o);
+    }
     if (avail && q == 0) {
       const int32_t r1 = rho_s[l] - sm.fq[X * 8 + 1];
       const int32_t r0 = rho_s[tl];
       const float EX = dF32(cell32(FT, r1), cell32(FT, r0), r1, r0);
-      const float dEf = EX + (m.s - m.c);
+      const float dEf = EX + (acc.s - acc.c);
       dE = static_cast<double>(dEf);
     }
   }
-  if (q == 0) sm.rates[k][b] = avail ? arrhenius(J.nu, J.kT, Xc, dE) : 0.0;
-  const unsigned bal = __ballot_sync(kFull, avail && q == 0);
-  if (lane == 0) {
-    uint8_t m = 0;
-    for (int bb = 0; bb < 8; ++bb)
-      if ((bal >> (4 * bb)) & 1u) m |= static_cast<uint8_t>(1u << bb);
-    sm.vavail[k] = m;
+  if (q == 0) {
+    sm.rates[k][b] = avail ? arrhenius(J.nu, J.kT, Xc, dE) : 0.0;
+    sm.vavb[k][b] = avail ? 1 : 0;
   }
-  __syncwarp();
+  if (KIND == kEam64) EVAL_T(3);
 }
 
-__device__ __forceinline__ void local_cell(const Region& R, int l, int& cx, int& cy, int& cz) {
-  const int lx = l % R.LX;
-  const int t = l / R.LX;
-  cx = lx >> 1;
-  cy = t % R.LY;
-  cz = t / R.LY;
-}
+// Phase profile (builds with -DAKMC_PHASE_PROFILE): thread 0 accumulates the cycles
+// between consecutive CTA barriers into counters[8 + phase].
+#ifdef AKMC_PHASE_PROFILE
+#define AKMC_PHASE(i)                                                                           \
+  do {                                                                                          \
+    if (threadIdx.x == 0) {                                                                     \
+      const long long t_ = clock64();                                                           \
+      atomicAdd(a.counters + 8 + (i), static_cast<unsigned long long>(t_ - tph));               \
+      tph = t_;                                                                                 \
+    }                                                                                           \
+  } while (0)
+#else
+#define AKMC_PHASE(i) \
+  do {              \
+  } while (0)
+#endif
 
-// The hop loop of one block's active sector (or one per-hop API step).
+// The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
+// Warps 0..7 evaluate rates (warp b = jump b); thread kCtl (first lane of warp 8)
+// keeps the ordered vacancy list, forms the total, selects, and runs the clock.
 template <int KIND>
 __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s) {
-  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const bool evaluator = warp < 8;
+#ifdef AKMC_PHASE_PROFILE
+  long long tph = clock64();
+#endif
   BlockDev& B = a.blocks[gb];
   JobDev& J = a.jobs[B.job];
   const Potential& P = a.pots[J.pot];
@@ -362,11 +396,11 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   Region R;
   make_region(B, sec, R);
-  // F-table window: one bulk copy issued by lane 0, overlapped with the staging below
+  // F-table window: one bulk copy issued by the control thread, overlapped with the staging
   const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
   const bool need_win = eam && sm.win_pot != win_key;
-  __syncwarp();
-  if (need_win && lane == 0) {
+  __syncthreads();  // every thread has read win_pot; the previous item's readers are done
+  if (need_win && tid == kCtl) {
     const void* src = KIND == kEam32 ? static_cast<const void*>(P.F32 + P.fwin0)
                                      : static_cast<const void*>(P.Fcoef + 4 * static_cast<int64_t>(P.fwin0));
     bulk_load(sm.fwin, src, kFWin * 32u, &sm.mbar);
@@ -378,19 +412,22 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   FT.g64 = P.Fcoef;
   FT.g32 = P.F32;
   FT.status = a.status;
+  FT.prof = a.counters + 16;
+  FT.fc = fcache_of(rho_s, R.n);
 
-  // stage the region: rows (fixed y, z) of LX <= 64 sites, lanes along x; eight rows
-  // of loads are issued before any shared-memory store so they are all in flight
+  // stage the region: warp w takes rows w, w+9, ...; four rows of loads are issued
+  // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
   {
     const int nrows = R.LY * R.LZ;
     const int gx0 = wrap1(R.ox + lane, J.sx), gx1 = wrap1(R.ox + lane + 32, J.sx);
     const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
-    for (int row0 = 0; row0 < nrows; row0 += 8) {
-      uint8_t ov[8][2];
-      int32_t rv[8][2];
+    constexpr int kW = kThreads / 32;
+    for (int row0 = warp; row0 < nrows; row0 += 4 * kW) {
+      uint8_t ov[4][2];
+      int32_t rv[4][2];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int row = row0 + k;
+      for (int k = 0; k < 4; ++k) {
+        const int row = row0 + kW * k;
         if (row < nrows) {
           const int ly = row % R.LY, lz = row / R.LY;
           const int gy = wrap1(R.oy + ly, J.sy), gz = wrap1(R.oz + lz, J.sz);
@@ -406,8 +443,8 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         }
       }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int row = row0 + k;
+      for (int k = 0; k < 4; ++k) {
+        const int row = row0 + kW * k;
         if (row < nrows) {
           const int l = lane + R.LX * row;
           if (has0) {
@@ -423,22 +460,29 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
   }
   const int cnt = min(B.cnt, kMaxV);
-  for (int i = lane; i < cnt; i += 32) {
-    const int v = a.blk_list[static_cast<int64_t>(gb) * kMaxV + i];
+  if (tid < cnt) {
+    const int v = a.blk_list[static_cast<int64_t>(gb) * kMaxV + tid];
     const int s = a.vac_site[v];
     const int X = s % J.sx;
     const int t = s / J.sx;
     const int y = t % J.sy;
     const int z = t / J.sy;
-    sm.vidx[i] = v;
-    sm.vloc[i] = (X - R.ox) + R.LX * ((y - R.oy) + R.LY * (z - R.oz));
-    sm.vlid[i] = s;
-    sm.vact[i] = 1;
-    sm.vdirty[i] = 0;
+    const int lx = X - R.ox, ly = y - R.oy, lz = z - R.oz;
+    sm.vidx[tid] = v;
+    sm.vloc[tid] = lx + R.LX * (ly + R.LY * lz);
+    sm.vlid[tid] = s;
+    sm.vcx[tid] = static_cast<int16_t>(lx);
+    sm.vcy[tid] = static_cast<int16_t>(ly);
+    sm.vcz[tid] = static_cast<int16_t>(lz);
+    sm.vgx[tid] = X;
+    sm.vgy[tid] = y;
+    sm.vgz[tid] = z;
+    sm.vdirty[tid] = 0;
   }
-  __syncwarp();
-  int nord = cnt;
-  if (lane == 0) {  // z-y-x scan order of ABVIModel::calcRates = ascending site id inside a sector
+  __syncthreads();
+  AKMC_PHASE(0);
+  if (tid == kCtl) {
+    // z-y-x scan order of ABVIModel::calcRates = ascending site id inside a sector
     for (int i = 0; i < cnt; ++i) {
       int j = i;
       while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[i]) {
@@ -447,128 +491,142 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
       sm.ord[j] = i;
     }
-  }
-  if (need_win) {
-    bool ok = true;
-    if (lane == 0) {
-      ok = mbar_wait(&sm.mbar, sm.mbar_phase);
-      if (ok) {
+    for (int i = 0; i < 4; ++i) {
+      sm.xs[i] = B.xs[i];
+      sm.xt[i] = B.xt[i];
+    }
+    sm.ctl_ok = 1;
+    if (need_win) {
+      if (mbar_wait(&sm.mbar, sm.mbar_phase)) {
         sm.mbar_phase ^= 1u;
         sm.win_pot = win_key;
       } else {
         atomicOr(a.status, kErrTimeout);
         mbar_wait(&sm.mbar, sm.mbar_phase);  // bounded second wait for the copy in flight
         sm.win_pot = -1;
+        sm.ctl_ok = 0;
       }
     }
-    ok = __shfl_sync(kFull, ok ? 1 : 0, 0) != 0;
-    if (!ok) return;
   }
-  __syncwarp();
-  for (int k = 0; k < cnt; ++k) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
-  int64_t evals = cnt;
+  __syncthreads();
+  AKMC_PHASE(1);
+  if (!sm.ctl_ok) return;
+  if (KIND == kEam64) {  // F(rho) of every staged site, reused by all jumps that touch it
+    for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
+    __syncthreads();
+  }
+  if (evaluator)
+    for (int k = 0; k < cnt; ++k) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
 
-  uint64_t xs[4], xt[4];
-  for (int i = 0; i < 4; ++i) {
-    xs[i] = B.xs[i];
-    xt[i] = B.xt[i];
-  }
   const int64_t hop0 = B.hops;
-  int64_t nh = 0;
-  int64_t nact_sum = 0;
+  int64_t nh = 0, nact_sum = 0, evals = cnt;
+  int nord = cnt;
   double sector_time = 0.0;
   const int D = eam ? 4 : 3;
+  __syncthreads();  // initial rates visible
+  AKMC_PHASE(2);
   while (true) {
-    double total = 0.0;
-    if (lane == 0) {
+    if (tid == kCtl) {
+      // ordered total and selection; unavailable jumps hold 0.0, and adding 0.0
+      // leaves a positive sum unchanged, so both run branch-free over 8 jumps
+      double total = 0.0;
       for (int i = 0; i < nord; ++i) {
-        const int k = sm.ord[i];
-        const uint8_t m = sm.vavail[k];
-        for (int bb = 0; bb < 8; ++bb)
-          if ((m >> bb) & 1) total += sm.rates[k][bb];
+        const double* r = sm.rates[sm.ord[i]];
+#pragma unroll
+        for (int bb = 0; bb < 8; ++bb) total += r[bb];
       }
-    }
-    total = __shfl_sync(kFull, total, 0);
-    if (a.mode == kModeCalc) {
-      if (lane == 0) *a.api_total = total;
-      break;
-    }
-    if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
-      if (a.mode == kModeSelectPerform && lane == 0) {
-        a.api_event->from_site = -1;
-        a.api_event->total = total;
-      }
-      sector_time = thr;
-      break;
-    }
-    double u = 0.0;
-    int ksel = -1, bsel = -1;
-    if (lane == 0) {
-      u = a.mode == kModeSelectPerform ? a.api_u : uniform_co(xs);
-      const double expected = u * total;  // ModelAdapter::selectAndPerform
-      double acc = 0.0;
-      for (int i = 0; i < nord && ksel < 0; ++i) {  // ABVIModel::select (kmc.cpp:242-309)
-        const int k = sm.ord[i];
-        const uint8_t m = sm.vavail[k];
-        for (int bb = 0; bb < 8; ++bb) {
-          if (!((m >> bb) & 1)) continue;
-          acc += sm.rates[k][bb];
-          if (acc > expected) {
-            ksel = k;
-            bsel = bb;
-            break;
+      int stop = 0, ksel = -1, bsel = -1;
+      double u = 0.0;
+      if (a.mode == kModeCalc) {
+        *a.api_total = total;
+        stop = 1;
+      } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
+        if (a.mode == kModeSelectPerform) {
+          a.api_event->from_site = -1;
+          a.api_event->total = total;
+        }
+        sector_time = thr;
+        stop = 1;
+      } else {
+        u = a.mode == kModeSelectPerform ? a.api_u : uniform_co(sm.xs);
+        const double expected = u * total;  // ModelAdapter::selectAndPerform
+        double acc = 0.0;
+        for (int i = 0; i < nord && ksel < 0; ++i) {  // ABVIModel::select (kmc.cpp:242-309)
+          const int k = sm.ord[i];
+          const double* r = sm.rates[k];
+#pragma unroll
+          for (int bb = 0; bb < 8; ++bb) {
+            acc += r[bb];
+            if (ksel < 0 && acc > expected) {
+              ksel = k;
+              bsel = bb;
+            }
           }
         }
       }
+      sm.ctl_total = total;
+      sm.ctl_u = u;
+      sm.ctl_ksel = ksel;
+      sm.ctl_bsel = bsel;
+      sm.ctl_stop = stop;
+      if (ksel >= 0) {  // publish the hop before anyone rewrites the list or the lattice
+        const int sl = sm.vloc[ksel];
+        sm.ctl_s = sl;
+        sm.ctl_from = sm.vlid[ksel];
+        sm.ctl_X = occ_s[sl + sm.d1[sl & 1][bsel]];
+        sm.ctl_gx = sm.vgx[ksel];
+        sm.ctl_gy = sm.vgy[ksel];
+        sm.ctl_gz = sm.vgz[ksel];
+      }
     }
-    ksel = __shfl_sync(kFull, ksel, 0);
-    bsel = __shfl_sync(kFull, bsel, 0);
+    __syncthreads();  // (A) selection visible
+    AKMC_PHASE(3);
+    if (sm.ctl_stop) break;
+    const int ksel = sm.ctl_ksel, bsel = sm.ctl_bsel;
+    const double total = sm.ctl_total;
     const int nact_before = nord;
-    int nd = 0;
-    int64_t from_g = -1, to_g = -1;
-    uint8_t Xc = 0;
     if (ksel >= 0) {
-      // ABVIModel::perform (kmc.cpp:358-396) on the staged region
-      const int s = sm.vloc[ksel];
+      // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
+      const int s = sm.ctl_s;
       const int p = s & 1;
       const int tl = s + sm.d1[p][bsel];
-      Xc = occ_s[tl];
-      // global coordinates of s; the hop writes through to global memory (the staged
-      // regions of concurrent blocks are disjoint, so global stays the shared truth)
-      from_g = sm.vlid[ksel];
-      const int sX = static_cast<int>(from_g % J.sx);
-      const int sT = static_cast<int>(from_g / J.sx);
-      const int sY = sT % J.sy, sZ = sT / J.sy;
-      auto gsite = [&](int32_t w) {
+      const uint8_t Xc = static_cast<uint8_t>(sm.ctl_X);
+      const int64_t from_g = sm.ctl_from;
+      const int sX = sm.ctl_gx, sY = sm.ctl_gy, sZ = sm.ctl_gz;
+      auto gsite = [&](int32_t w) {  // site ids fit in int32 (checked when the job is added)
         const int gx = wrap1(sX + unpack_dx(w), J.sx), gy = wrap1(sY + unpack_dy(w), J.sy),
                   gz = wrap1(sZ + unpack_dz(w), J.sz);
-        return static_cast<int64_t>(gx) + static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
+        return gx + J.sx * (gy + J.sy * gz);
       };
-      to_g = gsite(a.geo->nn1[p][bsel]);
-      __syncwarp();
-      if (lane == 0) {
+      if (eam && tid < kRefreshN) {
+        const int X = species_index(Xc);
+        const int32_t e = sm.rl[p][bsel][tid];
+        const int j = s + sdelta(e);
+        const int32_t v = rho_s[j] + (sm.fq[X * 8 + sshs(e)] - sm.fq[X * 8 + ssht(e)]);
+        rho_s[j] = v;
+        if (KIND == kEam64) FT.fc[j] = F64(FT, v);
+        J.rho[gsite(__ldg(&a.geo->refresh[p][bsel][tid]))] = v;
+      }
+      if (tid == kCtl) {
+        const int32_t wg = __ldg(&a.geo->nn1[p][bsel]);
+        const int64_t to_g = gsite(wg);
         occ_s[tl] = kV;
         occ_s[s] = Xc;
         J.occ[to_g] = kV;
         J.occ[from_g] = Xc;
-      }
-      if (eam) {
-        const int X = species_index(Xc);
-        for (int i = lane; i < kRefreshN; i += 32) {
-          const int32_t e = sm.rl[p][bsel][i];
-          const int j = s + sdelta(e);
-          const int32_t v = rho_s[j] + (sm.fq[X * 8 + sshs(e)] - sm.fq[X * 8 + ssht(e)]);
-          rho_s[j] = v;
-          J.rho[gsite(a.geo->refresh[p][bsel][i])] = v;
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
+        // move the vacancy: local coordinates by the jump offset, no division needed
+        const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
+        const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
+        sm.vcx[ksel] = static_cast<int16_t>(nlx);
+        sm.vcy[ksel] = static_cast<int16_t>(nly);
+        sm.vcz[ksel] = static_cast<int16_t>(nlz);
         sm.vloc[ksel] = tl;
         sm.vlid[ksel] = static_cast<int32_t>(to_g);
-        int cx, cy, cz;
-        local_cell(R, tl, cx, cy, cz);
-        const bool in = cx >= 2 && cx < 2 + R.w[0] && cy >= 2 && cy < 2 + R.w[1] && cz >= 2 && cz < 2 + R.w[2];
+        sm.vgx[ksel] = wrap1(sX + unpack_dx(wg), J.sx);
+        sm.vgy[ksel] = wrap1(sY + unpack_dy(wg), J.sy);
+        sm.vgz[ksel] = wrap1(sZ + unpack_dz(wg), J.sz);
+        const int cx = nlx >> 1;
+        const bool in = cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
         int pos = 0;
         while (sm.ord[pos] != ksel) ++pos;
         for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
@@ -581,94 +639,97 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           }
           sm.ord[j] = ksel;
           ++nord;
-        } else {
-          sm.vact[ksel] = 0;
         }
-        int sx, sy, sz;
-        local_cell(R, s, sx, sy, sz);
+        int nd = 0;
         for (int i = 0; i < nord; ++i) {
           const int k = sm.ord[i];
-          int vx, vy, vz;
-          local_cell(R, sm.vloc[k], vx, vy, vz);
-          if (abs(vx - sx) <= D && abs(vy - sy) <= D && abs(vz - sz) <= D) {
-            sm.vdirty[k] = 1;
-            ++nd;
-          }
+          const bool dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
+          sm.vdirty[k] = dirty ? 1 : 0;
+          nd += dirty ? 1 : 0;
+        }
+        sm.ctl_nord = nord;
+        sm.ctl_nd = nd;
+        sm.ctl_to = to_g;
+      }
+    }
+    __syncthreads();  // (B) lattice, list and dirty marks updated
+    AKMC_PHASE(4);
+    if (ksel >= 0) {
+      nord = sm.ctl_nord;
+      if (evaluator) {
+        for (int i = 0; i < nord; ++i) {
+          const int k = sm.ord[i];
+          if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
         }
       }
-      nord = __shfl_sync(kFull, nord, 0);
-      nd = __shfl_sync(kFull, nd, 0);
-      __syncwarp();
-      for (int k = 0; k < cnt; ++k) {
-        if (!sm.vdirty[k]) continue;
-        eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
-        if (lane == 0) sm.vdirty[k] = 0;
-        __syncwarp();
-      }
-      evals += nd;
+      evals += sm.ctl_nd;
       nact_sum += nact_before;
       ++nh;
     }
-    if (a.mode == kModeSelectPerform) {
-      if (lane == 0) {
+    if (tid == kCtl) {  // the clock runs while the evaluator warps recompute rates
+      int stop = 0;
+      if (a.mode == kModeSelectPerform) {
         akmc_event* e = a.api_event;
         e->round = 0;
         e->hop = hop0;
-        e->from_site = from_g;
-        e->to_site = to_g;
+        e->from_site = ksel >= 0 ? sm.ctl_from : -1;
+        e->to_site = ksel >= 0 ? sm.ctl_to : -1;
         e->block = B.local_id;
-        e->species = Xc;
-        e->u = u;
+        e->species = ksel >= 0 ? sm.ctl_X : 0;
+        e->u = sm.ctl_u;
         e->total = total;
         e->dt = 0.0;
         e->n_act = nact_before;
-        e->n_dirty = nd;
+        e->n_dirty = ksel >= 0 ? sm.ctl_nd : 0;
         e->job = B.job;
         e->reserved = 0;
-      }
-      break;
-    }
-    if (lane == 0) {
-      const double u2 = uniform_oc(xt);  // sublattice.inl:118-120
-      const double dt = -port_log(u2) / total;
-      sector_time += dt;
-      if (ksel >= 0 && a.log_cap > 0) {
-        const unsigned long long slot = atomicAdd(a.log_count, 1ull);
-        if (slot < static_cast<unsigned long long>(a.log_cap)) {
-          akmc_event* e = a.log + slot;
-          e->round = B.round;
-          e->hop = hop0 + nh - 1;
-          e->from_site = from_g;
-          e->to_site = to_g;
-          e->block = B.local_id;
-          e->species = Xc;
-          e->u = u;
-          e->total = total;
-          e->dt = dt;
-          e->n_act = nact_before;
-          e->n_dirty = nd;
-          e->job = B.job;
-          e->reserved = 0;
-        } else {
-          atomicOr(a.status, kErrLogOverflow);
+        stop = 1;
+      } else {
+        const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
+        const double dt = -port_log(u2) / total;
+        sector_time += dt;
+        if (ksel >= 0 && a.log_cap > 0) {
+          const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+          if (slot < static_cast<unsigned long long>(a.log_cap)) {
+            akmc_event* e = a.log + slot;
+            e->round = B.round;
+            e->hop = hop0 + nh - 1;
+            e->from_site = sm.ctl_from;
+            e->to_site = sm.ctl_to;
+            e->block = B.local_id;
+            e->species = sm.ctl_X;
+            e->u = sm.ctl_u;
+            e->total = total;
+            e->dt = dt;
+            e->n_act = nact_before;
+            e->n_dirty = sm.ctl_nd;
+            e->job = B.job;
+            e->reserved = 0;
+          } else {
+            atomicOr(a.status, kErrLogOverflow);
+          }
+        }
+        if (!(sector_time < thr)) stop = 1;
+        if (nh >= a.hop_cap) {
+          atomicOr(a.status, kErrHopCap);
+          stop = 1;
         }
       }
+      sm.ctl_next_stop = stop;
     }
-    sector_time = __shfl_sync(kFull, sector_time, 0);
-    if (!(sector_time < thr)) break;
-    if (nh >= a.hop_cap) {
-      if (lane == 0) atomicOr(a.status, kErrHopCap);
-      break;
-    }
+    __syncthreads();  // (C) new rates and the clock decision visible
+    AKMC_PHASE(5);
+    if (sm.ctl_next_stop) break;
   }
-  __syncwarp();
+  __syncthreads();
+  AKMC_PHASE(6);
   if (a.mode == kModeCalc) return;
-  if (lane == 0) {
+  if (tid == kCtl) {
     if (a.mode == kModeRound) {
       B.evo[sec] += sector_time;
       for (int i = 0; i < 4; ++i) {
-        B.xs[i] = xs[i];
-        B.xt[i] = xt[i];
+        B.xs[i] = sm.xs[i];
+        B.xt[i] = sm.xt[i];
       }
     }
     B.hops += nh;
@@ -682,14 +743,14 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   if (nh == 0) return;
   // the lattice was written through at every hop; only the vacancy positions remain
-  for (int i = lane; i < cnt; i += 32) a.vac_site[sm.vidx[i]] = sm.vlid[i];
+  if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[tid];
 }
 
 __device__ __forceinline__ void carve(uint8_t* smem, int nreg, Smem*& sm, uint8_t*& occ_s, int32_t*& rho_s) {
   sm = reinterpret_cast<Smem*>(smem);
   uint8_t* p = smem + ((sizeof(Smem) + 15) & ~static_cast<size_t>(15));
   rho_s = reinterpret_cast<int32_t*>(p);
-  occ_s = p + static_cast<size_t>(nreg) * 4;
+  occ_s = reinterpret_cast<uint8_t*>(fcache_of(rho_s, nreg) + nreg);
 }
 
 __device__ void dispatch_block(const RoundArgs& a, int gb, uint8_t* smem) {
@@ -747,18 +808,15 @@ __device__ void init_cta_smem(uint8_t* smem) {
     sm->mbar_phase = 0;
     mbar_init(&sm->mbar);
   }
-  __syncwarp();
+  __syncthreads();
 }
 
-__global__ void __launch_bounds__(32) k_hop(RoundArgs a) {
+__global__ void __maxnreg__(112) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
   if (static_cast<int>(blockIdx.x) >= na) return;
   init_cta_smem(smem);
-  for (int item = blockIdx.x; item < na; item += gridDim.x) {
-    dispatch_block(a, a.active[item], smem);
-    __syncwarp();
-  }
+  for (int item = blockIdx.x; item < na; item += gridDim.x) dispatch_block(a, a.active[item], smem);
 }
 
 __global__ void k_finalize(RoundArgs a) {
@@ -791,7 +849,7 @@ __global__ void k_finalize(RoundArgs a) {
   }
 }
 
-__global__ void k_api_block(RoundArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) k_api_block(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const JobDev& J = a.jobs[a.api_job];
   if (*a.n_active == 0) {  // no vacancy in the sector
@@ -807,7 +865,6 @@ __global__ void k_api_block(RoundArgs a) {
   init_cta_smem(smem);
   dispatch_block(a, J.block0, smem);
 }
-
 __global__ void k_api_reset(RoundArgs a) {
   const JobDev& J = a.jobs[a.api_job];
   a.blocks[J.block0].cnt = 0;
@@ -861,14 +918,15 @@ __global__ void k_device_math(const double* x, int64_t n, double* e, double* l) 
 }  // namespace
 
 size_t hop_smem_bytes(int max_region_sites) {
-  return ((sizeof(Smem) + 15) & ~static_cast<size_t>(15)) + static_cast<size_t>(max_region_sites) * 5 + 16;
+  return ((sizeof(Smem) + 15) & ~static_cast<size_t>(15)) + ((static_cast<size_t>(max_region_sites) * 4 + 15) & ~static_cast<size_t>(15)) +
+         static_cast<size_t>(max_region_sites) * 9 + 16;
 }
 
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a.nvac > 0) k_bucket<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
   if (ev0) cudaEventRecord(static_cast<cudaEvent_t>(ev0), st);
-  k_hop<<<hop_grid, 32, smem, st>>>(a);
+  k_hop<<<hop_grid, kThreads, smem, st>>>(a);
   if (ev1) cudaEventRecord(static_cast<cudaEvent_t>(ev1), st);
   k_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
@@ -877,7 +935,7 @@ int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, vo
 int launch_api(const RoundArgs& a, size_t smem, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a.nvac > 0) k_bucket<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
-  k_api_block<<<1, 32, smem, st>>>(a);
+  k_api_block<<<1, kThreads, smem, st>>>(a);
   k_api_reset<<<1, 1, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
 }

@@ -193,6 +193,7 @@ SIGNATURES = {
     "akmc_cluster_stats": (C.c_int, [_vp, _vp, C.POINTER(_i64), _vp, _i64]),
     "akmc_device_math": (C.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "akmc_load_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
+    "akmc_get_phase_cycles": (C.c_int, [_vp, _vp]),
     "akmc_set_kernel_timing": (C.c_int, [_vp, _i32]),
     "akmc_get_kernel_timing": (C.c_int, [_vp, C.POINTER(_d), C.POINTER(_i64)]),
     "akmc_config_parse": (C.c_int, [C.c_char_p, C.POINTER(RunConfig), C.c_char_p, _i32]),
@@ -421,6 +422,11 @@ class Engine:
         self._ck(lib().akmc_get_counters(self.h, _ptr(out)))
         return dict(hops=int(out[0]), evaluations=int(out[1]), rounds=int(out[2]), blocks=int(out[3]),
                     n_act_sum=int(out[4]), staged_sites=int(out[5]), written_sites=int(out[6]))
+
+    def phase_cycles(self):
+        out = np.zeros(16, np.int64)
+        self._ck(lib().akmc_get_phase_cycles(self.h, _ptr(out)))
+        return out
 
     def load_occupancy(self, job, occ):
         occ = np.ascontiguousarray(occ, np.uint8)

@@ -559,16 +559,34 @@ struct Job {
     return e_after - e_before;
   }
 
-  // EAM dE in the defined order: 4 interleaved partial sums over the jump's site
-  // list (entry i -> partial i mod 4), merged (p0+p2)+(p1+p3), plus the moving
-  // atom's own embedding change.
+  // EAM dE in the defined order: 32 interleaved partial sums over the jump's site
+  // list (entry i -> partial i mod 32), merged by a xor butterfly (partner distance
+  // 16, 8, 4, 2, 1; p[i] <- p[i] + p[i ^ m]), plus the moving atom's own embedding
+  // change.
+  static double butterfly32(double* p) {
+    for (int m = 16; m >= 1; m >>= 1) {
+      double t[32];
+      for (int i = 0; i < 32; ++i) t[i] = p[i] + p[i ^ m];
+      for (int i = 0; i < 32; ++i) p[i] = t[i];
+    }
+    return p[0];
+  }
+  static Comp butterfly32(Comp* p) {
+    for (int m = 16; m >= 1; m >>= 1) {
+      Comp t[32];
+      for (int i = 0; i < 32; ++i) t[i] = comp_merge(p[i], p[i ^ m]);
+      for (int i = 0; i < 32; ++i) p[i] = t[i];
+    }
+    return p[0];
+  }
   double dE_eam64(int64_t s, int b, uint8_t Xc) const {
     int64_t X0, y0, z0;
     coords(s, X0, y0, z0);
     const int p = static_cast<int>(X0 & 1);
     const int X = species_index(Xc);
     const auto& L = geo.dE[p][b];
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double acc[32];
+    for (double& v : acc) v = 0.0;
     for (size_t i = 0; i < L.size(); ++i) {
       const auto& e = L[i];
       const int64_t j = site(X0 + e.dx, y0 + e.dy, z0 + e.dz);
@@ -580,9 +598,9 @@ struct Job {
       const double Fa = eam.F64(r + d);
       const double Fb = eam.F64(r);
       const double T = (Fa - Fb) + (eam.phi64[X][Y][e.sh_s] - eam.phi64[X][Y][e.sh_t]);
-      acc[i & 3] += T;
+      acc[i & 31] += T;
     }
-    const double tsum = (acc[0] + acc[2]) + (acc[1] + acc[3]);
+    const double tsum = butterfly32(acc);
     const int64_t t = site(X0 + kNN1[p][b].dx, y0 + kNN1[p][b].dy, z0 + kNN1[p][b].dz);
     const double EX = eam.F64(rho[static_cast<size_t>(s)] - eam.fq[X][1]) - eam.F64(rho[static_cast<size_t>(t)]);
     return EX + tsum;
@@ -594,7 +612,7 @@ struct Job {
     const int p = static_cast<int>(X0 & 1);
     const int X = species_index(Xc);
     const auto& L = geo.dE[p][b];
-    Comp acc[4];
+    Comp acc[32];
     for (size_t i = 0; i < L.size(); ++i) {
       const auto& e = L[i];
       const int64_t j = site(X0 + e.dx, y0 + e.dy, z0 + e.dz);
@@ -604,9 +622,9 @@ struct Job {
       const int32_t r = rho[static_cast<size_t>(j)];
       const int32_t d = eam.fq[X][e.sh_s] - eam.fq[X][e.sh_t];
       const float T = eam.dF32(r + d, r) + (eam.phi32[X][Y][e.sh_s] - eam.phi32[X][Y][e.sh_t]);
-      kahan_add(acc[i & 3], T);
+      kahan_add(acc[i & 31], T);
     }
-    const Comp m = comp_merge(comp_merge(acc[0], acc[2]), comp_merge(acc[1], acc[3]));
+    const Comp m = butterfly32(acc);
     const int64_t t = site(X0 + kNN1[p][b].dx, y0 + kNN1[p][b].dy, z0 + kNN1[p][b].dz);
     const float EX = eam.dF32(rho[static_cast<size_t>(s)] - eam.fq[X][1], rho[static_cast<size_t>(t)]);
     const float dE = EX + (m.s - m.c);

@@ -205,3 +205,45 @@ def test_sector_overflow_is_reported(ak):
         with pytest.raises(ak.AkmcError) as ei:
             eng.sync()
         assert ei.value.status == -7
+
+
+def test_cpp_host_time_loop_matches_oracle(ak):
+    # akmc_host_time_loop: SubLattice::startTimeLoop in C++ over the per-hop entry points
+    o = oracle_job(box=(16, 16, 16), n_vacancies=6, seed=9)
+    with ak.Engine() as eng:
+        device_job(eng, o, (16, 16, 16), seed=9)
+        eng.prepare()
+        ev, evo = eng.host_time_loop(0, 40, 9)
+        o.run_rounds(40)
+        oe = o.events()
+        assert len(ev) == len(oe) > 20
+        for f in ("round", "from_site", "to_site", "species"):
+            assert np.array_equal(ev[f], oe[f]), f
+        for f in ("u", "total", "dt"):
+            assert np.array_equal(ev[f].view(np.uint64), np.ascontiguousarray(oe[f]).view(np.uint64)), f
+        evo_o, _ = o.block_state()
+        assert np.array_equal(evo.view(np.uint64), evo_o[0].view(np.uint64))
+        assert np.array_equal(eng.occupancy(0), o.occupancy())
+
+
+def test_load_occupancy_restarts_the_trajectory(ak):
+    o = oracle_job(box=(20, 20, 20), seed=5)
+    occ0 = o.occupancy()
+    with ak.Engine(event_log_capacity=1 << 18) as eng:
+        device_job(eng, o, (20, 20, 20), seed=5)
+        eng.prepare()
+        eng.run_rounds(64)
+        first = eng.events()
+        occ1 = eng.occupancy(0)
+        eng.load_occupancy(0, occ0)
+        assert np.array_equal(eng.occupancy(0), occ0)
+        assert eng.job_state(0)["round"] == 0
+        eng.run_rounds(64)
+        second = eng.events()
+        assert len(first) > 100
+        assert_same_events(second, np.sort(first, order=["round", "block", "hop"]))
+        assert np.array_equal(eng.occupancy(0), occ1)
+        bad = occ0.copy()
+        bad[np.nonzero(bad == 0)[0][0]] = 1  # one vacancy fewer than the job holds
+        with pytest.raises(ak.AkmcError):
+            eng.load_occupancy(0, bad)
