@@ -4,12 +4,13 @@
 // runs as three launches:
 //   k_bucket   one thread per vacancy: find its domain block, keep it if it lies in
 //              the block's active sector, append it to the block's list;
-//   k_hop      one CTA of 8 warps per active block: stage the sector plus a 2-cell
+//   k_hop      one CTA of 9 warps per active block: stage the sector plus a 2-cell
 //              halo (occupancy bytes and the int32 density cache) into shared memory
-//              and run the hop loop there.  Warp w evaluates jump direction w of a
-//              vacancy (its 32 lanes split the 76 sites of the jump); thread 0 forms
-//              the ordered total, selects, and keeps the vacancy list; each hop writes
-//              its two occupancy bytes and 78 densities through to global memory;
+//              and run the hop loop there.  Warp w < 8 evaluates jump direction w of a
+//              vacancy (its 32 lanes split the 76 sites of the jump); warp 8 forms the
+//              ordered total, selects, performs the hop and keeps the vacancy list and
+//              the clock; each hop writes its two occupancy bytes and 78 densities
+//              through to global memory;
 //   k_finalize one thread per block: clock of blocks without vacancies, next round.
 // Concurrently active sectors are at least 4 cells apart, so the staged regions of
 // different blocks never overlap and no atomics are needed on the lattice.
@@ -64,13 +65,15 @@ __device__ __forceinline__ void make_region(const BlockDev& B, int sec, Region& 
 // Shared-memory working set of one CTA (followed by the staged region).
 struct Smem {
   double b1[25], b2[25];
-  double phi64[4 * 4 * 8];
-  float phi32[4 * 4 * 8];
-  int32_t fq[4 * 8];
-  int32_t d1[2][8];
+  double dphi64[4 * 4 * 64];    // phi_XY(shell s) - phi_XY(shell t), index (X*4+Y)*64 + s*8 + t
+  float dphi32[4 * 4 * 64];
+  int32_t dfq[4 * 64];          // f_X(shell s) - f_X(shell t) in Q.24, index X*64 + s*8 + t
+  int32_t fq1[4];               // f_X at the first shell
+  int32_t d1[2][8];             // 1nn local offsets by x parity
+  int32_t w1[2][8];             // 1nn packed (dx, dy, dz)
   int32_t d2[6];
-  int32_t jl[2][8][kJumpN];     // int16 delta | sh_s << 16 | sh_t << 20
-  int32_t rl[2][8][kRefreshN];
+  int32_t jl[2][8][kJumpN];     // int16 local offset | (s*8+t) << 16
+  int32_t rl[2][8][kRefreshN];  // packed (dx, dy, dz) | (s*8+t) << 24
   int32_t vidx[kMaxV], vloc[kMaxV], vlid[kMaxV], ord[kMaxV];
   int16_t vcx[kMaxV], vcy[kMaxV], vcz[kMaxV];  // local coordinates (x in doubled sites)
   int32_t vgx[kMaxV], vgy[kMaxV], vgz[kMaxV];  // global coordinates
@@ -161,50 +164,61 @@ __device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, con
     sm.b1[tid] = P.b1[tid / 5][tid % 5];
     sm.b2[tid] = P.b2[tid / 5][tid % 5];
   }
-  if (tid < 128) {
-    sm.phi64[tid] = (&P.phi64[0][0][0])[tid];
-    sm.phi32[tid] = (&P.phi32[0][0][0])[tid];
+  if (tid < 16) {
+    const int32_t w = G.nn1[tid >> 3][tid & 7];
+    sm.d1[tid >> 3][tid & 7] = local_delta(w, R);
+    sm.w1[tid >> 3][tid & 7] = w;
   }
-  if (tid < 32) sm.fq[tid] = (&P.fq[0][0])[tid];
-  if (tid < 16) sm.d1[tid >> 3][tid & 7] = local_delta(G.nn1[tid >> 3][tid & 7], R);
   if (tid < 6) sm.d2[tid] = local_delta(G.nn2[tid], R);
   if (eam) {
+    if (tid < 4) sm.fq1[tid] = P.fq[tid][1];
+    for (int i = tid; i < 4 * 4 * 64; i += kThreads) {
+      const int xy = i >> 6, hs = (i >> 3) & 7, ht = i & 7;
+      const double* ph = &P.phi64[0][0][0] + xy * 8;
+      const float* pf = &P.phi32[0][0][0] + xy * 8;
+      sm.dphi64[i] = ph[hs] - ph[ht];
+      sm.dphi32[i] = pf[hs] - pf[ht];
+      if (i < 4 * 64) sm.dfq[i] = P.fq[i >> 6][hs] - P.fq[i >> 6][ht];
+    }
     for (int i = tid; i < 2 * 8 * kJumpN; i += kThreads) {
       const int32_t w = __ldg(&G.jump[0][0][0] + i);
-      (&sm.jl[0][0][0])[i] = (local_delta(w, R) & 0xffff) | (unpack_sh_s(w) << 16) | (unpack_sh_t(w) << 20);
+      (&sm.jl[0][0][0])[i] = (local_delta(w, R) & 0xffff) | ((unpack_sh_s(w) * 8 + unpack_sh_t(w)) << 16);
     }
     for (int i = tid; i < 2 * 8 * kRefreshN; i += kThreads) {
       const int32_t w = __ldg(&G.refresh[0][0][0] + i);
-      (&sm.rl[0][0][0])[i] = (local_delta(w, R) & 0xffff) | (unpack_sh_s(w) << 16) | (unpack_sh_t(w) << 20);
+      (&sm.rl[0][0][0])[i] = (w & 0xffffff) | ((unpack_sh_s(w) * 8 + unpack_sh_t(w)) << 24);
     }
   }
 }
 
 __device__ __forceinline__ int sdelta(int32_t e) { return static_cast<int16_t>(e & 0xffff); }
-__device__ __forceinline__ int sshs(int32_t e) { return (e >> 16) & 0xf; }
-__device__ __forceinline__ int ssht(int32_t e) { return (e >> 20) & 0xf; }
+__device__ __forceinline__ int jshells(int32_t e) { return (e >> 16) & 63; }
+__device__ __forceinline__ int rshells(int32_t e) { return (e >> 24) & 63; }
+
+// Cells outside the shared-memory window (rare): global memory, range-checked.
+__device__ __noinline__ double F64_far(const FTab& T, int32_t r, double p) {
+  const int k = r >> kRhoCellShift;
+  int kc = k;
+  if (r < 0 || k > kTabN - 2) {
+    atomicOr(T.status, kErrRhoRange);
+    kc = r < 0 ? 0 : kTabN - 2;
+  }
+  const double2* c = reinterpret_cast<const double2*>(T.g64) + 2 * kc;
+  const double2 lo = __ldg(c), hi = __ldg(c + 1);
+  return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
+}
 
 __device__ __forceinline__ double F64(const FTab& T, int32_t r) {
   const int k = r >> kRhoCellShift;
   // p = (r mod 2^17) * 2^-17, built in the exponent field: 1 + m 2^-17 minus 1 (both exact)
   const double p = __hiloint2double(0x3FF00000 | ((r & kRhoFracMask) << 3), 0) - 1.0;
   const unsigned kk = static_cast<unsigned>(k - T.kw0);
-  double2 lo, hi;
   if (kk < static_cast<unsigned>(kFWin)) {
     const double2* c = reinterpret_cast<const double2*>(T.win) + 2 * kk;
-    lo = c[0];
-    hi = c[1];
-  } else {
-    int kc = k;
-    if (r < 0 || k > kTabN - 2) {
-      atomicOr(T.status, kErrRhoRange);
-      kc = r < 0 ? 0 : kTabN - 2;
-    }
-    const double2* c = reinterpret_cast<const double2*>(T.g64) + 2 * kc;
-    lo = __ldg(c);
-    hi = __ldg(c + 1);
+    const double2 lo = c[0], hi = c[1];
+    return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
   }
-  return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
+  return F64_far(T, r, p);
 }
 
 __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
@@ -290,15 +304,14 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
       for (int i = q; i < kJumpN; i += 32) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
         const int32_t e = L[i];
         const int j = l + sdelta(e);
+        const int h = jshells(e);
         const uint8_t o = occ_s[j];
-        const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
-        const int32_t d = sm.fq[X * 8 + ss] - sm.fq[X * 8 + st];
-        const double Fa = F64(FT, r + d);
+        const double Fa = F64(FT, r + sm.dfq[X * 64 + h]);
         const double Fb = FT.fc[j];  // F(rho_j), cached
         if (o != kV) {
           const int Y = species_index(o);
-          acc += (Fa - Fb) + (sm.phi64[(X * 4 + Y) * 8 + ss] - sm.phi64[(X * 4 + Y) * 8 + st]);
+          acc += (Fa - Fb) + sm.dphi64[(X * 4 + Y) * 64 + h];
         }
       }
     }
@@ -307,7 +320,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     for (int m = 16; m >= 1; m >>= 1) acc = acc + __shfl_xor_sync(kFull, acc, m);
     EVAL_T(1);
     if (avail && q == 0) {
-      const double EX = F64(FT, rho_s[l] - sm.fq[X * 8 + 1]) - FT.fc[tl];
+      const double EX = F64(FT, rho_s[l] - sm.fq1[X]) - FT.fc[tl];
       dE = EX + acc;
     }
     EVAL_T(2);
@@ -322,14 +335,14 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
       for (int i = q; i < kJumpN; i += 32) {
         const int32_t e = L[i];
         const int j = l + sdelta(e);
+        const int h = jshells(e);
         const uint8_t o = occ_s[j];
-        const int ss = sshs(e), st = ssht(e);
         const int32_t r = rho_s[j];
-        const int32_t r1 = r + (sm.fq[X * 8 + ss] - sm.fq[X * 8 + st]);
+        const int32_t r1 = r + sm.dfq[X * 64 + h];
         const float dF = dF32(cell32(FT, r1), cell32(FT, r), r1, r);
         if (o != kV) {
           const int Y = species_index(o);
-          kahan_add(acc, dF + (sm.phi32[(X * 4 + Y) * 8 + ss] - sm.phi32[(X * 4 + Y) * 8 + st]));
+          kahan_add(acc, dF + sm.dphi32[(X * 4 + Y) * 64 + h]);
         }
       }
     }
@@ -341,7 +354,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
       acc = comp_merge(acc, o);
     }
     if (avail && q == 0) {
-      const int32_t r1 = rho_s[l] - sm.fq[X * 8 + 1];
+      const int32_t r1 = rho_s[l] - sm.fq1[X];
       const int32_t r0 = rho_s[tl];
       const float EX = dF32(cell32(FT, r1), cell32(FT, r0), r1, r0);
       const float dEf = EX + (acc.s - acc.c);
@@ -490,11 +503,14 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         --j;
       }
       sm.ord[j] = i;
+      sm.vdirty[i] = 1;  // the first evaluation pass computes every vacancy
     }
     for (int i = 0; i < 4; ++i) {
       sm.xs[i] = B.xs[i];
       sm.xt[i] = B.xt[i];
     }
+    sm.ctl_nord = cnt;
+    sm.ctl_next_stop = 0;
     sm.ctl_ok = 1;
     if (need_win) {
       if (mbar_wait(&sm.mbar, sm.mbar_phase)) {
@@ -515,212 +531,236 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
     __syncthreads();
   }
-  if (evaluator)
-    for (int k = 0; k < cnt; ++k) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
 
+  // Hop loop, two CTA barriers per hop:
+  //  (E) warps 0..7 evaluate the dirty vacancies; the control thread runs the clock of
+  //      the hop just performed and decides whether the sector is done;
+  //  (S) the control warp selects the next hop and performs it: lane 0 updates the
+  //      occupancy and the vacancy list, the lanes refresh the 78 densities.
+  // Control state (clock, counters, list length) lives in the control thread's registers.
   const int64_t hop0 = B.hops;
   int64_t nh = 0, nact_sum = 0, evals = cnt;
-  int nord = cnt;
-  double sector_time = 0.0;
+  int nord = cnt, nact_last = 0;
+  double sector_time = 0.0, total_last = 0.0;
+  bool clock_due = false;  // a selection with a positive total happened since the last clock
   const int D = eam ? 4 : 3;
-  __syncthreads();  // initial rates visible
-  AKMC_PHASE(2);
+  bool first = true;
   while (true) {
-    if (tid == kCtl) {
-      // ordered total and selection; unavailable jumps hold 0.0, and adding 0.0
-      // leaves a positive sum unchanged, so both run branch-free over 8 jumps
-      double total = 0.0;
-      for (int i = 0; i < nord; ++i) {
-        const double* r = sm.rates[sm.ord[i]];
-#pragma unroll
-        for (int bb = 0; bb < 8; ++bb) total += r[bb];
+    if (evaluator) {
+      const int n = sm.ctl_nord;
+      for (int i = 0; i < n; ++i) {
+        const int k = sm.ord[i];
+        if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
       }
-      int stop = 0, ksel = -1, bsel = -1;
-      double u = 0.0;
-      if (a.mode == kModeCalc) {
-        *a.api_total = total;
-        stop = 1;
-      } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
-        if (a.mode == kModeSelectPerform) {
-          a.api_event->from_site = -1;
-          a.api_event->total = total;
-        }
-        sector_time = thr;
-        stop = 1;
-      } else {
-        u = a.mode == kModeSelectPerform ? a.api_u : uniform_co(sm.xs);
-        const double expected = u * total;  // ModelAdapter::selectAndPerform
-        double acc = 0.0;
-        for (int i = 0; i < nord && ksel < 0; ++i) {  // ABVIModel::select (kmc.cpp:242-309)
-          const int k = sm.ord[i];
-          const double* r = sm.rates[k];
-#pragma unroll
-          for (int bb = 0; bb < 8; ++bb) {
-            acc += r[bb];
-            if (ksel < 0 && acc > expected) {
-              ksel = k;
-              bsel = bb;
-            }
-          }
-        }
-      }
-      sm.ctl_total = total;
-      sm.ctl_u = u;
-      sm.ctl_ksel = ksel;
-      sm.ctl_bsel = bsel;
-      sm.ctl_stop = stop;
-      if (ksel >= 0) {  // publish the hop before anyone rewrites the list or the lattice
-        const int sl = sm.vloc[ksel];
-        sm.ctl_s = sl;
-        sm.ctl_from = sm.vlid[ksel];
-        sm.ctl_X = occ_s[sl + sm.d1[sl & 1][bsel]];
-        sm.ctl_gx = sm.vgx[ksel];
-        sm.ctl_gy = sm.vgy[ksel];
-        sm.ctl_gz = sm.vgz[ksel];
-      }
-    }
-    __syncthreads();  // (A) selection visible
-    AKMC_PHASE(3);
-    if (sm.ctl_stop) break;
-    const int ksel = sm.ctl_ksel, bsel = sm.ctl_bsel;
-    const double total = sm.ctl_total;
-    const int nact_before = nord;
-    if (ksel >= 0) {
-      // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
-      const int s = sm.ctl_s;
-      const int p = s & 1;
-      const int tl = s + sm.d1[p][bsel];
-      const uint8_t Xc = static_cast<uint8_t>(sm.ctl_X);
-      const int64_t from_g = sm.ctl_from;
-      const int sX = sm.ctl_gx, sY = sm.ctl_gy, sZ = sm.ctl_gz;
-      auto gsite = [&](int32_t w) {  // site ids fit in int32 (checked when the job is added)
-        const int gx = wrap1(sX + unpack_dx(w), J.sx), gy = wrap1(sY + unpack_dy(w), J.sy),
-                  gz = wrap1(sZ + unpack_dz(w), J.sz);
-        return gx + J.sx * (gy + J.sy * gz);
-      };
-      if (eam && tid < kRefreshN) {
-        const int X = species_index(Xc);
-        const int32_t e = sm.rl[p][bsel][tid];
-        const int j = s + sdelta(e);
-        const int32_t v = rho_s[j] + (sm.fq[X * 8 + sshs(e)] - sm.fq[X * 8 + ssht(e)]);
-        rho_s[j] = v;
-        if (KIND == kEam64) FT.fc[j] = F64(FT, v);
-        J.rho[gsite(__ldg(&a.geo->refresh[p][bsel][tid]))] = v;
-      }
-      if (tid == kCtl) {
-        const int32_t wg = __ldg(&a.geo->nn1[p][bsel]);
-        const int64_t to_g = gsite(wg);
-        occ_s[tl] = kV;
-        occ_s[s] = Xc;
-        J.occ[to_g] = kV;
-        J.occ[from_g] = Xc;
-        // move the vacancy: local coordinates by the jump offset, no division needed
-        const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
-        const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
-        sm.vcx[ksel] = static_cast<int16_t>(nlx);
-        sm.vcy[ksel] = static_cast<int16_t>(nly);
-        sm.vcz[ksel] = static_cast<int16_t>(nlz);
-        sm.vloc[ksel] = tl;
-        sm.vlid[ksel] = static_cast<int32_t>(to_g);
-        sm.vgx[ksel] = wrap1(sX + unpack_dx(wg), J.sx);
-        sm.vgy[ksel] = wrap1(sY + unpack_dy(wg), J.sy);
-        sm.vgz[ksel] = wrap1(sZ + unpack_dz(wg), J.sz);
-        const int cx = nlx >> 1;
-        const bool in = cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
-        int pos = 0;
-        while (sm.ord[pos] != ksel) ++pos;
-        for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
-        --nord;
-        if (in) {
-          int j = nord;
-          while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[ksel]) {
-            sm.ord[j] = sm.ord[j - 1];
-            --j;
-          }
-          sm.ord[j] = ksel;
-          ++nord;
-        }
-        int nd = 0;
-        for (int i = 0; i < nord; ++i) {
-          const int k = sm.ord[i];
-          const bool dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
-          sm.vdirty[k] = dirty ? 1 : 0;
-          nd += dirty ? 1 : 0;
-        }
-        sm.ctl_nord = nord;
-        sm.ctl_nd = nd;
-        sm.ctl_to = to_g;
-      }
-    }
-    __syncthreads();  // (B) lattice, list and dirty marks updated
-    AKMC_PHASE(4);
-    if (ksel >= 0) {
-      nord = sm.ctl_nord;
-      if (evaluator) {
-        for (int i = 0; i < nord; ++i) {
-          const int k = sm.ord[i];
-          if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
-        }
-      }
-      evals += sm.ctl_nd;
-      nact_sum += nact_before;
-      ++nh;
-    }
-    if (tid == kCtl) {  // the clock runs while the evaluator warps recompute rates
+    } else if (tid == kCtl && clock_due) {
+      clock_due = false;
       int stop = 0;
-      if (a.mode == kModeSelectPerform) {
-        akmc_event* e = a.api_event;
-        e->round = 0;
-        e->hop = hop0;
-        e->from_site = ksel >= 0 ? sm.ctl_from : -1;
-        e->to_site = ksel >= 0 ? sm.ctl_to : -1;
-        e->block = B.local_id;
-        e->species = ksel >= 0 ? sm.ctl_X : 0;
-        e->u = sm.ctl_u;
-        e->total = total;
-        e->dt = 0.0;
-        e->n_act = nact_before;
-        e->n_dirty = ksel >= 0 ? sm.ctl_nd : 0;
-        e->job = B.job;
-        e->reserved = 0;
+      const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
+      const double dt = -port_log(u2) / total_last;
+      sector_time += dt;
+      if (sm.ctl_ksel >= 0 && a.log_cap > 0) {
+        const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+        if (slot < static_cast<unsigned long long>(a.log_cap)) {
+          akmc_event* e = a.log + slot;
+          e->round = B.round;
+          e->hop = hop0 + nh - 1;
+          e->from_site = sm.ctl_from;
+          e->to_site = sm.ctl_to;
+          e->block = B.local_id;
+          e->species = sm.ctl_X;
+          e->u = sm.ctl_u;
+          e->total = total_last;
+          e->dt = dt;
+          e->n_act = nact_last;
+          e->n_dirty = sm.ctl_nd;
+          e->job = B.job;
+          e->reserved = 0;
+        } else {
+          atomicOr(a.status, kErrLogOverflow);
+        }
+      }
+      if (!(sector_time < thr)) stop = 1;
+      if (nh >= a.hop_cap) {
+        atomicOr(a.status, kErrHopCap);
         stop = 1;
-      } else {
-        const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
-        const double dt = -port_log(u2) / total;
-        sector_time += dt;
-        if (ksel >= 0 && a.log_cap > 0) {
-          const unsigned long long slot = atomicAdd(a.log_count, 1ull);
-          if (slot < static_cast<unsigned long long>(a.log_cap)) {
-            akmc_event* e = a.log + slot;
-            e->round = B.round;
-            e->hop = hop0 + nh - 1;
-            e->from_site = sm.ctl_from;
-            e->to_site = sm.ctl_to;
-            e->block = B.local_id;
-            e->species = sm.ctl_X;
-            e->u = sm.ctl_u;
-            e->total = total;
-            e->dt = dt;
-            e->n_act = nact_before;
-            e->n_dirty = sm.ctl_nd;
-            e->job = B.job;
-            e->reserved = 0;
-          } else {
-            atomicOr(a.status, kErrLogOverflow);
-          }
-        }
-        if (!(sector_time < thr)) stop = 1;
-        if (nh >= a.hop_cap) {
-          atomicOr(a.status, kErrHopCap);
-          stop = 1;
-        }
       }
       sm.ctl_next_stop = stop;
     }
-    __syncthreads();  // (C) new rates and the clock decision visible
-    AKMC_PHASE(5);
+    __syncthreads();  // (E) rates and the clock decision visible
+    AKMC_PHASE(first ? 2 : 5);
+    first = false;
     if (sm.ctl_next_stop) break;
+    if (warp == 8) {
+      if (lane == 0) {
+        // ordered total and selection; unavailable jumps hold 0.0, and adding 0.0
+        // leaves a positive sum unchanged, so both run branch-free over 8 jumps
+        double total = 0.0;
+        for (int i = 0; i < nord; ++i) {
+          const double* r = sm.rates[sm.ord[i]];
+#pragma unroll
+          for (int bb = 0; bb < 8; ++bb) total += r[bb];
+        }
+        int stop = 0, ksel = -1, bsel = -1;
+        double u = 0.0;
+        if (a.mode == kModeCalc) {
+          *a.api_total = total;
+          stop = 1;
+        } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
+          if (a.mode == kModeSelectPerform) {
+            a.api_event->from_site = -1;
+            a.api_event->total = total;
+          }
+          sector_time = thr;
+          stop = 1;
+        } else {
+          u = a.mode == kModeSelectPerform ? a.api_u : uniform_co(sm.xs);
+          const double expected = u * total;  // ModelAdapter::selectAndPerform
+          double acc = 0.0;
+          for (int i = 0; i < nord && ksel < 0; ++i) {  // ABVIModel::select (kmc.cpp:242-309)
+            const int k = sm.ord[i];
+            const double* r = sm.rates[k];
+#pragma unroll
+            for (int bb = 0; bb < 8; ++bb) {
+              acc += r[bb];
+              if (ksel < 0 && acc > expected) {
+                ksel = k;
+                bsel = bb;
+              }
+            }
+          }
+          clock_due = a.mode == kModeRound;
+          total_last = total;
+          nact_last = nord;
+        }
+        sm.ctl_u = u;
+        sm.ctl_ksel = ksel;
+        sm.ctl_bsel = bsel;
+        if (ksel >= 0) {
+          const int sl = sm.vloc[ksel];
+          sm.ctl_s = sl;
+          sm.ctl_from = sm.vlid[ksel];
+          sm.ctl_X = occ_s[sl + sm.d1[sl & 1][bsel]];
+          sm.ctl_gx = sm.vgx[ksel];
+          sm.ctl_gy = sm.vgy[ksel];
+          sm.ctl_gz = sm.vgz[ksel];
+        } else if (!stop && a.mode == kModeSelectPerform) {  // u * total reached no event
+          akmc_event* e = a.api_event;
+          e->round = 0;
+          e->hop = hop0;
+          e->from_site = -1;
+          e->to_site = -1;
+          e->block = B.local_id;
+          e->species = 0;
+          e->u = u;
+          e->total = total;
+          e->dt = 0.0;
+          e->n_act = nord;
+          e->n_dirty = 0;
+          e->job = B.job;
+          e->reserved = 0;
+          stop = 1;
+        }
+        sm.ctl_stop = stop;
+      }
+      __syncwarp();
+      const int ksel = sm.ctl_ksel, bsel = sm.ctl_bsel;
+      if (!sm.ctl_stop && ksel >= 0) {
+        // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
+        const int s = sm.ctl_s;
+        const int p = s & 1;
+        const uint8_t Xc = static_cast<uint8_t>(sm.ctl_X);
+        const int sX = sm.ctl_gx, sY = sm.ctl_gy, sZ = sm.ctl_gz;
+        auto gsite = [&](int32_t w) {  // site ids fit in int32 (checked when the job is added)
+          const int gx = wrap1(sX + unpack_dx(w), J.sx), gy = wrap1(sY + unpack_dy(w), J.sy),
+                    gz = wrap1(sZ + unpack_dz(w), J.sz);
+          return gx + J.sx * (gy + J.sy * gz);
+        };
+        if (eam) {  // the 78 exact density deltas, in shared memory and through to global memory
+          const int X = species_index(Xc);
+          for (int i = lane; i < kRefreshN; i += 32) {
+            const int32_t e = sm.rl[p][bsel][i];
+            const int j = s + local_delta(e, R);
+            const int32_t v = rho_s[j] + sm.dfq[X * 64 + rshells(e)];
+            rho_s[j] = v;
+            if (KIND == kEam64) FT.fc[j] = F64(FT, v);
+            J.rho[gsite(e)] = v;
+          }
+        }
+        if (lane == 0) {
+          const int32_t wg = sm.w1[p][bsel];
+          const int tl = s + sm.d1[p][bsel];
+          const int64_t to_g = gsite(wg);
+          occ_s[tl] = kV;
+          occ_s[s] = Xc;
+          J.occ[to_g] = kV;
+          J.occ[sm.ctl_from] = Xc;
+          // move the vacancy: local coordinates by the jump offset, no division needed
+          const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
+          const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
+          sm.vcx[ksel] = static_cast<int16_t>(nlx);
+          sm.vcy[ksel] = static_cast<int16_t>(nly);
+          sm.vcz[ksel] = static_cast<int16_t>(nlz);
+          sm.vloc[ksel] = tl;
+          sm.vlid[ksel] = static_cast<int32_t>(to_g);
+          sm.vgx[ksel] = wrap1(sX + unpack_dx(wg), J.sx);
+          sm.vgy[ksel] = wrap1(sY + unpack_dy(wg), J.sy);
+          sm.vgz[ksel] = wrap1(sZ + unpack_dz(wg), J.sz);
+          const int cx = nlx >> 1;
+          const bool in = cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
+          int pos = 0;
+          while (sm.ord[pos] != ksel) ++pos;
+          for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
+          --nord;
+          if (in) {
+            int j = nord;
+            while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[ksel]) {
+              sm.ord[j] = sm.ord[j - 1];
+              --j;
+            }
+            sm.ord[j] = ksel;
+            ++nord;
+          }
+          int nd = 0;
+          for (int i = 0; i < nord; ++i) {
+            const int k = sm.ord[i];
+            const bool dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
+            sm.vdirty[k] = dirty ? 1 : 0;
+            nd += dirty ? 1 : 0;
+          }
+          sm.ctl_nord = nord;
+          sm.ctl_nd = nd;
+          sm.ctl_to = to_g;
+          evals += nd;
+          nact_sum += nact_last;
+          ++nh;
+          if (a.mode == kModeSelectPerform) {
+            akmc_event* e = a.api_event;
+            e->round = 0;
+            e->hop = hop0;
+            e->from_site = sm.ctl_from;
+            e->to_site = to_g;
+            e->block = B.local_id;
+            e->species = Xc;
+            e->u = sm.ctl_u;
+            e->total = total_last;
+            e->dt = 0.0;
+            e->n_act = nact_last;
+            e->n_dirty = nd;
+            e->job = B.job;
+            e->reserved = 0;
+            sm.ctl_stop = 1;
+          }
+        }
+      } else if (lane == 0 && !sm.ctl_stop) {
+        sm.ctl_nord = nord;  // no event: nothing dirty, the clock still advances
+        for (int i = 0; i < nord; ++i) sm.vdirty[sm.ord[i]] = 0;
+      }
+    }
+    __syncthreads();  // (S) selection, lattice, list and dirty marks updated
+    AKMC_PHASE(3);
+    if (sm.ctl_stop) break;
   }
+
   __syncthreads();
   AKMC_PHASE(6);
   if (a.mode == kModeCalc) return;
@@ -741,7 +781,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     atomicAdd(a.counters + 5, static_cast<unsigned long long>(R.n));
     if (nh) atomicAdd(a.counters + 6, static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2)));
   }
-  if (nh == 0) return;
   // the lattice was written through at every hop; only the vacancy positions remain
   if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[tid];
 }
