@@ -51,6 +51,9 @@ enum { AKMC_V = 0, AKMC_FE = 1, AKMC_CU = 2, AKMC_NI = 4, AKMC_MN = 8 };
 /* Maximum vacancies in the active sector of one domain block. */
 #define AKMC_MAX_SECTOR_VACANCIES 64
 
+/* Most domain blocks (summed over the jobs of a context) that akmc_run_rounds_noalloc serves. */
+#define AKMC_NOALLOC_MAX_BLOCKS 8192
+
 /*
  * EAM model on the rigid BCC lattice: pair and density functions at the five
  * shells within the cutoff (species order Fe, Cu, Ni, Mn) and the embedding
@@ -149,6 +152,16 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx);
  * SubLattice::startTimeLoop, sublattice.inl:64-177, for all domain blocks at
  * once).  Asynchronous on the context stream; errors surface at akmc_sync. */
 AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds);
+/* No reference counterpart.  akmc_run_rounds without any allocation: the same
+ * three launches per round, one by one (no CUDA graph is instantiated), with the
+ * per-round scratch (block vacancy lists, active-block list, active count) in a
+ * fixed device array of the library instead of context memory.  It serves up to
+ * AKMC_NOALLOC_MAX_BLOCKS domain blocks and returns AKMC_EINVAL beyond that.
+ * The first call on a device looks up the scratch address with that device
+ * current; make it before any stream capture.  The scratch is shared by all
+ * contexts of a device: calls whose rounds overlap on the device race.  Kernel
+ * timing mode is not applied. */
+AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
 /* Runs until every job is done (hop budget or max_rounds) or max_rounds pass. */
 AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds);
 AKMC_API akmc_status akmc_sync(akmc_ctx* ctx);

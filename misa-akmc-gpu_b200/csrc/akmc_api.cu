@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -587,6 +588,49 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
     left -= ctx->graph_rounds;
   }
   for (; left > 0; --left) {
+    const int e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, nullptr, nullptr);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+  }
+  return AKMC_OK;
+}
+
+namespace {
+// Per-device address of the fixed round scratch, looked up on the first call with the device current.
+constexpr int kNoAllocDevices = 64;
+std::mutex g_noalloc_mu;
+int32_t* g_noalloc_base[kNoAllocDevices] = {};
+}  // namespace
+
+AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (ctx->nblocks > kNoAllocMaxBlocks)
+    return fail(ctx, AKMC_EINVAL, "akmc_run_rounds_noalloc: " + std::to_string(ctx->nblocks) +
+                                      " domain blocks exceed AKMC_NOALLOC_MAX_BLOCKS (" +
+                                      std::to_string(kNoAllocMaxBlocks) + ")");
+  const int dev = ctx->cfg.device;
+  if (dev < 0 || dev >= kNoAllocDevices)
+    return fail(ctx, AKMC_EINVAL, "akmc_run_rounds_noalloc: device index beyond " + std::to_string(kNoAllocDevices));
+  if (n_rounds <= 0) return AKMC_OK;
+  CK(cudaSetDevice(dev));
+  int32_t* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+      const int e = noalloc_scratch(&g_noalloc_base[dev]);
+      if (e) return fail(ctx, AKMC_ECUDA, std::string("cudaGetSymbolAddress(round scratch): ") + cuda_name(e));
+    }
+    base = g_noalloc_base[dev];
+  }
+  RoundArgs a = ctx->args;
+  a.mode = kModeRound;
+  a.blk_list = base;
+  a.active = base + static_cast<size_t>(kNoAllocMaxBlocks) * kMaxV;
+  a.n_active = a.active + kNoAllocMaxBlocks;
+  // k_bucket appends to the active list from a zero count (k_finalize re-zeroes it each
+  // round); the block lists and the active list are written before they are read.
+  CK(cudaMemsetAsync(a.n_active, 0, sizeof(int32_t), ctx->stream));
+  for (int64_t r = 0; r < n_rounds; ++r) {
     const int e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, nullptr, nullptr);
     if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
   }

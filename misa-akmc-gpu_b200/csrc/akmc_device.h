@@ -9,6 +9,7 @@
 namespace akmc {
 
 constexpr int kMaxV = AKMC_MAX_SECTOR_VACANCIES;  // vacancies per block and sector
+constexpr int kNoAllocMaxBlocks = AKMC_NOALLOC_MAX_BLOCKS;
 constexpr int kJumpN = 76;                        // |N(s) u N(t)| - 2 sites per jump
 constexpr int kRefreshN = 78;                     // density refresh sites per jump
 constexpr int kShellNb = 58;                      // neighbours within the 5-shell cutoff
@@ -128,5 +129,8 @@ int launch_api(const RoundArgs& a, size_t smem, void* stream);
 int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, const Potential* pot,
                     const Geometry* geo, unsigned int* status, void* stream);
 int launch_device_math(const double* x, int64_t n, double* e, double* l, void* stream);
+// Device address of the fixed round scratch (current device): kNoAllocMaxBlocks * kMaxV
+// block-list slots, then kNoAllocMaxBlocks active-list slots, then the active count.
+int noalloc_scratch(int32_t** base);
 
 }  // namespace akmc

@@ -1012,4 +1012,16 @@ int launch_device_math(const double* x, int64_t n, double* e, double* l, void* s
   return static_cast<int>(cudaGetLastError());
 }
 
+// Round scratch of akmc_run_rounds_noalloc (2.1 MB): block vacancy lists, active-block
+// list and active count for kNoAllocMaxBlocks blocks, with the count 256-byte aligned.
+constexpr size_t kNoAllocWords = static_cast<size_t>(kNoAllocMaxBlocks) * (kMaxV + 1) + 64;
+static __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocWords];
+
+int noalloc_scratch(int32_t** base) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  *base = e == cudaSuccess ? static_cast<int32_t*>(p) : nullptr;
+  return static_cast<int>(e);
+}
+
 }  // namespace akmc

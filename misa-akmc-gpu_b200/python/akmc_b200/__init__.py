@@ -19,6 +19,7 @@ FP64, FP32C = 0, 1
 RNG_XOSHIRO = 0
 V, FE, CU, NI, MN = 0, 1, 2, 4, 8
 MAX_SECTOR_VACANCIES = 64
+NOALLOC_MAX_BLOCKS = 8192
 SECTOR_ORDER = (0, 7, 2, 5, 3, 4, 1, 6)
 
 STATUS = {
@@ -176,6 +177,7 @@ SIGNATURES = {
     "akmc_add_job": (C.c_int, [_vp, C.POINTER(JobConfig), _vp, _i64, C.POINTER(_i32)]),
     "akmc_prepare": (C.c_int, [_vp]),
     "akmc_run_rounds": (C.c_int, [_vp, _i64]),
+    "akmc_run_rounds_noalloc": (C.c_int, [_vp, _i64]),
     "akmc_run": (C.c_int, [_vp, _i64]),
     "akmc_sync": (C.c_int, [_vp]),
     "akmc_stream": (_vp, [_vp]),
@@ -375,6 +377,11 @@ class Engine:
 
     def run_rounds(self, n):
         self._ck(lib().akmc_run_rounds(self.h, n))
+
+    def run_rounds_noalloc(self, n):
+        """akmc_run_rounds without allocation: round scratch in a fixed device array
+        (at most NOALLOC_MAX_BLOCKS domain blocks; calls on one device must not overlap)."""
+        self._ck(lib().akmc_run_rounds_noalloc(self.h, n))
 
     def run(self, max_rounds=0):
         self._ck(lib().akmc_run(self.h, max_rounds))
