@@ -85,11 +85,13 @@ struct Smem {
   uint32_t mbar_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
   // hop-loop control, written by thread 0 between barriers
-  double ctl_total, ctl_u, ctl_time;
-  int64_t ctl_from, ctl_to;
-  int32_t ctl_ksel, ctl_bsel, ctl_nord, ctl_nd, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop;
-  int32_t ctl_gx, ctl_gy, ctl_gz;
+  double pre[kMaxV * 8];   // running sums of the ordered rates
+  double ctl_u, ctl_unext, ctl_expected;
+  int32_t ctl_from, ctl_to;
+  int32_t ctl_ksel, ctl_bsel, ctl_nord, ctl_nd, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop, ctl_hop, ctl_n8;
+  int32_t ctl_gx, ctl_gy, ctl_gz, ctl_qx, ctl_qy, ctl_qz;
   uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
+  uint64_t xsn[4];        // selection stream after the uniform drawn ahead
 };
 
 // --- bulk copy global -> shared with an mbarrier (cp.async.bulk, TMA unit) -----------
@@ -131,6 +133,15 @@ struct FTab {
   unsigned int* status;
   unsigned long long* prof;  // sub-phase cycles of the evaluation (profiling builds)
   double* fc;                // F(rho) of every staged site (FP64 form)
+};
+
+// Job constants of the running block, held in registers (the job record sits in global
+// memory, where every store of the hop loop would otherwise force a reload).
+struct JobC {
+  uint8_t* occ;
+  int32_t* rho;
+  int sx, sy, sz;
+  double nu, kT;
 };
 
 #ifdef AKMC_PHASE_PROFILE
@@ -256,7 +267,7 @@ enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };
 //             embedding change is added.
 template <int KIND>
 __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const FTab& FT,
-                             const JobDev& J) {
+                             const JobC& jc, const int32_t (&jr)[2][3]) {
   const int lane = threadIdx.x & 31;
   const int b = threadIdx.x >> 5;
   const int q = lane;
@@ -298,11 +309,14 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
   } else if (KIND == kEam64) {
     double acc = 0.0;
     const int X = species_index(Xc);
+    // the moving atom's own embedding change; every lane reads the same cells (broadcast),
+    // so its latency overlaps the site loop
+    const double EX = avail ? F64(FT, rho_s[l] - sm.fq1[X]) - FT.fc[tl] : 0.0;
     if (avail) {
-      const int32_t* L = sm.jl[p][b];
-#pragma unroll 3
-      for (int i = q; i < kJumpN; i += 32) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
-        const int32_t e = L[i];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
+        if (q + 32 * u >= kJumpN) break;
+        const int32_t e = p ? jr[1][u] : jr[0][u];
         const int j = l + sdelta(e);
         const int h = jshells(e);
         const uint8_t o = occ_s[j];
@@ -319,10 +333,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     EVAL_T(0);
     for (int m = 16; m >= 1; m >>= 1) acc = acc + __shfl_xor_sync(kFull, acc, m);
     EVAL_T(1);
-    if (avail && q == 0) {
-      const double EX = F64(FT, rho_s[l] - sm.fq1[X]) - FT.fc[tl];
-      dE = EX + acc;
-    }
+    if (avail && q == 0) dE = EX + acc;
     EVAL_T(2);
   } else {
     Comp32 acc;
@@ -330,10 +341,10 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     acc.c = 0.f;
     const int X = species_index(Xc);
     if (avail) {
-      const int32_t* L = sm.jl[p][b];
-#pragma unroll 3
-      for (int i = q; i < kJumpN; i += 32) {
-        const int32_t e = L[i];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        if (q + 32 * u >= kJumpN) break;
+        const int32_t e = p ? jr[1][u] : jr[0][u];
         const int j = l + sdelta(e);
         const int h = jshells(e);
         const uint8_t o = occ_s[j];
@@ -362,7 +373,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     }
   }
   if (q == 0) {
-    sm.rates[k][b] = avail ? arrhenius(J.nu, J.kT, Xc, dE) : 0.0;
+    sm.rates[k][b] = avail ? arrhenius(jc.nu, jc.kT, Xc, dE) : 0.0;
     sm.vavb[k][b] = avail ? 1 : 0;
   }
   if (KIND == kEam64) EVAL_T(3);
@@ -386,8 +397,8 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
 #endif
 
 // The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
-// Warps 0..7 evaluate rates (warp b = jump b); thread kCtl (first lane of warp 8)
-// keeps the ordered vacancy list, forms the total, selects, and runs the clock.
+// Warps 0..7 evaluate rates (warp b = jump b) and refresh densities; warp 8 keeps the
+// ordered vacancy list, selects, performs the occupancy swap and runs the clock.
 template <int KIND>
 __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s) {
   const int tid = threadIdx.x;
@@ -397,7 +408,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   long long tph = clock64();
 #endif
   BlockDev& B = a.blocks[gb];
-  JobDev& J = a.jobs[B.job];
+  const JobDev& J = a.jobs[B.job];
   const Potential& P = a.pots[J.pot];
   const bool eam = KIND != kPairBond;
   const int sec = a.mode == kModeRound ? sector_of_round(B.round) : a.api_sector;
@@ -407,6 +418,14 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     thr = static_cast<double>(step + 1) * J.window - B.evo[sec];
     if (!(0.0 < thr)) return;  // sector_time stays 0 (sublattice.inl:82)
   }
+  JobC jc;
+  jc.occ = J.occ;
+  jc.rho = J.rho;
+  jc.sx = J.sx;
+  jc.sy = J.sy;
+  jc.sz = J.sz;
+  jc.nu = J.nu;
+  jc.kT = J.kT;
   Region R;
   make_region(B, sec, R);
   // F-table window: one bulk copy issued by the control thread, overlapped with the staging
@@ -432,7 +451,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
   {
     const int nrows = R.LY * R.LZ;
-    const int gx0 = wrap1(R.ox + lane, J.sx), gx1 = wrap1(R.ox + lane + 32, J.sx);
+    const int gx0 = wrap1(R.ox + lane, jc.sx), gx1 = wrap1(R.ox + lane + 32, jc.sx);
     const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
     constexpr int kW = kThreads / 32;
     for (int row0 = warp; row0 < nrows; row0 += 4 * kW) {
@@ -443,15 +462,15 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         const int row = row0 + kW * k;
         if (row < nrows) {
           const int ly = row % R.LY, lz = row / R.LY;
-          const int gy = wrap1(R.oy + ly, J.sy), gz = wrap1(R.oz + lz, J.sz);
-          const int64_t base = static_cast<int64_t>(J.sx) * (gy + static_cast<int64_t>(J.sy) * gz);
+          const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
+          const int64_t base = static_cast<int64_t>(jc.sx) * (gy + static_cast<int64_t>(jc.sy) * gz);
           if (has0) {
-            ov[k][0] = J.occ[base + gx0];
-            if (eam) rv[k][0] = J.rho[base + gx0];
+            ov[k][0] = jc.occ[base + gx0];
+            if (eam) rv[k][0] = jc.rho[base + gx0];
           }
           if (has1) {
-            ov[k][1] = J.occ[base + gx1];
-            if (eam) rv[k][1] = J.rho[base + gx1];
+            ov[k][1] = jc.occ[base + gx1];
+            if (eam) rv[k][1] = jc.rho[base + gx1];
           }
         }
       }
@@ -476,10 +495,10 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   if (tid < cnt) {
     const int v = a.blk_list[static_cast<int64_t>(gb) * kMaxV + tid];
     const int s = a.vac_site[v];
-    const int X = s % J.sx;
-    const int t = s / J.sx;
-    const int y = t % J.sy;
-    const int z = t / J.sy;
+    const int X = s % jc.sx;
+    const int t = s / jc.sx;
+    const int y = t % jc.sy;
+    const int z = t / jc.sy;
     const int lx = X - R.ox, ly = y - R.oy, lz = z - R.oz;
     sm.vidx[tid] = v;
     sm.vloc[tid] = lx + R.LX * (ly + R.LY * lz);
@@ -490,7 +509,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.vgx[tid] = X;
     sm.vgy[tid] = y;
     sm.vgz[tid] = z;
-    sm.vdirty[tid] = 0;
+    sm.vdirty[tid] = 1;  // the first evaluation pass computes every vacancy
   }
   __syncthreads();
   AKMC_PHASE(0);
@@ -503,7 +522,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         --j;
       }
       sm.ord[j] = i;
-      sm.vdirty[i] = 1;  // the first evaluation pass computes every vacancy
     }
     for (int i = 0; i < 4; ++i) {
       sm.xs[i] = B.xs[i];
@@ -511,6 +529,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
     sm.ctl_nord = cnt;
     sm.ctl_next_stop = 0;
+    sm.ctl_hop = 0;
     sm.ctl_ok = 1;
     if (need_win) {
       if (mbar_wait(&sm.mbar, sm.mbar_phase)) {
@@ -531,13 +550,39 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
     __syncthreads();
   }
+  // this lane's entries of its warp's jump list, both x parities
+  int32_t jr[2][3];
+#pragma unroll
+  for (int u = 0; u < 3; ++u) {
+    const int i = lane + 32 * u;
+    const bool in = eam && evaluator && i < kJumpN;
+    jr[0][u] = in ? sm.jl[0][warp][i] : 0;
+    jr[1][u] = in ? sm.jl[1][warp][i] : 0;
+  }
+
+  // The 78 exact density deltas of the hop just performed (ABVIModel::perform's lattice
+  // change seen by the density cache), in shared memory and through to global memory.
+  auto refresh = [&](int i) {
+    const int s = sm.ctl_s, bsel = sm.ctl_bsel;
+    const int p = s & 1;
+    const int X = species_index(static_cast<uint8_t>(sm.ctl_X));
+    const int32_t e = sm.rl[p][bsel][i];
+    const int j = s + local_delta(e, R);
+    const int32_t v = rho_s[j] + sm.dfq[X * 64 + rshells(e)];
+    rho_s[j] = v;
+    if (KIND == kEam64) FT.fc[j] = F64(FT, v);
+    const int gx = wrap1(sm.ctl_gx + unpack_dx(e), jc.sx), gy = wrap1(sm.ctl_gy + unpack_dy(e), jc.sy),
+              gz = wrap1(sm.ctl_gz + unpack_dz(e), jc.sz);
+    jc.rho[gx + jc.sx * (gy + jc.sy * gz)] = v;  // site ids fit in int32 (checked at akmc_add_job)
+  };
 
   // Hop loop, two CTA barriers per hop:
-  //  (E) warps 0..7 evaluate the dirty vacancies; the control thread runs the clock of
-  //      the hop just performed and decides whether the sector is done;
-  //  (S) the control warp selects the next hop and performs it: lane 0 updates the
-  //      occupancy and the vacancy list, the lanes refresh the 78 densities.
-  // Control state (clock, counters, list length) lives in the control thread's registers.
+  //  (E) warps 0..7 refresh the densities of the hop just performed, then evaluate the
+  //      dirty vacancies; the control thread runs the clock of that hop, decides whether
+  //      the sector is done and draws the next selection uniform ahead of time;
+  //  (S) the control warp forms the ordered total, selects the next hop and performs it
+  //      on the occupancy and the vacancy list.
+  // Clock and counters live in the control thread's registers.
   const int64_t hop0 = B.hops;
   int64_t nh = 0, nact_sum = 0, evals = cnt;
   int nord = cnt, nact_last = 0;
@@ -547,44 +592,56 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   bool first = true;
   while (true) {
     if (evaluator) {
+      if (eam && sm.ctl_hop) {
+        if (tid < kRefreshN) refresh(tid);
+        asm volatile("bar.sync 1, 256;" ::: "memory");  // the evaluator warps only
+      }
       const int n = sm.ctl_nord;
       for (int i = 0; i < n; ++i) {
         const int k = sm.ord[i];
-        if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, J);
+        if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr);
       }
-    } else if (tid == kCtl && clock_due) {
-      clock_due = false;
-      int stop = 0;
-      const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
-      const double dt = -port_log(u2) / total_last;
-      sector_time += dt;
-      if (sm.ctl_ksel >= 0 && a.log_cap > 0) {
-        const unsigned long long slot = atomicAdd(a.log_count, 1ull);
-        if (slot < static_cast<unsigned long long>(a.log_cap)) {
-          akmc_event* e = a.log + slot;
-          e->round = B.round;
-          e->hop = hop0 + nh - 1;
-          e->from_site = sm.ctl_from;
-          e->to_site = sm.ctl_to;
-          e->block = B.local_id;
-          e->species = sm.ctl_X;
-          e->u = sm.ctl_u;
-          e->total = total_last;
-          e->dt = dt;
-          e->n_act = nact_last;
-          e->n_dirty = sm.ctl_nd;
-          e->job = B.job;
-          e->reserved = 0;
-        } else {
-          atomicOr(a.status, kErrLogOverflow);
+    } else if (tid == kCtl) {
+      if (clock_due) {
+        clock_due = false;
+        int stop = 0;
+        const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
+        const double dt = -port_log(u2) / total_last;
+        sector_time += dt;
+        if (sm.ctl_hop && a.log_cap > 0) {
+          const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+          if (slot < static_cast<unsigned long long>(a.log_cap)) {
+            akmc_event* e = a.log + slot;
+            e->round = B.round;
+            e->hop = hop0 + nh - 1;
+            e->from_site = sm.ctl_from;
+            e->to_site = sm.ctl_to;
+            e->block = B.local_id;
+            e->species = sm.ctl_X;
+            e->u = sm.ctl_u;
+            e->total = total_last;
+            e->dt = dt;
+            e->n_act = nact_last;
+            e->n_dirty = sm.ctl_nd;
+            e->job = B.job;
+            e->reserved = 0;
+          } else {
+            atomicOr(a.status, kErrLogOverflow);
+          }
         }
+        if (!(sector_time < thr)) stop = 1;
+        if (nh >= a.hop_cap) {
+          atomicOr(a.status, kErrHopCap);
+          stop = 1;
+        }
+        sm.ctl_next_stop = stop;
       }
-      if (!(sector_time < thr)) stop = 1;
-      if (nh >= a.hop_cap) {
-        atomicOr(a.status, kErrHopCap);
-        stop = 1;
+      if (a.mode == kModeRound && !sm.ctl_next_stop) {
+        // the next selection's uniform, committed only if a selection consumes it
+        uint64_t x[4] = {sm.xs[0], sm.xs[1], sm.xs[2], sm.xs[3]};
+        sm.ctl_unext = uniform_co(x);
+        for (int i = 0; i < 4; ++i) sm.xsn[i] = x[i];
       }
-      sm.ctl_next_stop = stop;
     }
     __syncthreads();  // (E) rates and the clock decision visible
     AKMC_PHASE(first ? 2 : 5);
@@ -592,16 +649,22 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     if (sm.ctl_next_stop) break;
     if (warp == 8) {
       if (lane == 0) {
-        // ordered total and selection; unavailable jumps hold 0.0, and adding 0.0
-        // leaves a positive sum unchanged, so both run branch-free over 8 jumps
+        // ordered total; the running sums are kept: they are the selection scan's
+        // accumulator values (ABVIModel::select, kmc.cpp:242-309) in the same order.
+        // Unavailable jumps hold 0.0, and adding 0.0 leaves a positive sum unchanged.
         double total = 0.0;
+        int n8 = 0;
         for (int i = 0; i < nord; ++i) {
           const double* r = sm.rates[sm.ord[i]];
 #pragma unroll
-          for (int bb = 0; bb < 8; ++bb) total += r[bb];
+          for (int bb = 0; bb < 8; ++bb) {
+            total += r[bb];
+            sm.pre[n8 + bb] = total;
+          }
+          n8 += 8;
         }
-        int stop = 0, ksel = -1, bsel = -1;
-        double u = 0.0;
+        int stop = 0;
+        double u = 0.0, expected = 0.0;
         if (a.mode == kModeCalc) {
           *a.api_total = total;
           stop = 1;
@@ -613,123 +676,129 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           sector_time = thr;
           stop = 1;
         } else {
-          u = a.mode == kModeSelectPerform ? a.api_u : uniform_co(sm.xs);
-          const double expected = u * total;  // ModelAdapter::selectAndPerform
-          double acc = 0.0;
-          for (int i = 0; i < nord && ksel < 0; ++i) {  // ABVIModel::select (kmc.cpp:242-309)
-            const int k = sm.ord[i];
-            const double* r = sm.rates[k];
-#pragma unroll
-            for (int bb = 0; bb < 8; ++bb) {
-              acc += r[bb];
-              if (ksel < 0 && acc > expected) {
-                ksel = k;
-                bsel = bb;
-              }
-            }
+          if (a.mode == kModeSelectPerform) {
+            u = a.api_u;
+          } else {
+            u = sm.ctl_unext;
+            for (int i = 0; i < 4; ++i) sm.xs[i] = sm.xsn[i];
           }
+          expected = u * total;  // ModelAdapter::selectAndPerform
           clock_due = a.mode == kModeRound;
           total_last = total;
           nact_last = nord;
         }
         sm.ctl_u = u;
-        sm.ctl_ksel = ksel;
-        sm.ctl_bsel = bsel;
-        if (ksel >= 0) {
-          const int sl = sm.vloc[ksel];
-          sm.ctl_s = sl;
-          sm.ctl_from = sm.vlid[ksel];
-          sm.ctl_X = occ_s[sl + sm.d1[sl & 1][bsel]];
-          sm.ctl_gx = sm.vgx[ksel];
-          sm.ctl_gy = sm.vgy[ksel];
-          sm.ctl_gz = sm.vgz[ksel];
-        } else if (!stop && a.mode == kModeSelectPerform) {  // u * total reached no event
-          akmc_event* e = a.api_event;
-          e->round = 0;
-          e->hop = hop0;
-          e->from_site = -1;
-          e->to_site = -1;
-          e->block = B.local_id;
-          e->species = 0;
-          e->u = u;
-          e->total = total;
-          e->dt = 0.0;
-          e->n_act = nord;
-          e->n_dirty = 0;
-          e->job = B.job;
-          e->reserved = 0;
-          stop = 1;
-        }
+        sm.ctl_expected = expected;
+        sm.ctl_n8 = stop ? 0 : n8;
         sm.ctl_stop = stop;
       }
       __syncwarp();
-      const int ksel = sm.ctl_ksel, bsel = sm.ctl_bsel;
-      if (!sm.ctl_stop && ksel >= 0) {
-        // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
-        const int s = sm.ctl_s;
-        const int p = s & 1;
-        const uint8_t Xc = static_cast<uint8_t>(sm.ctl_X);
-        const int sX = sm.ctl_gx, sY = sm.ctl_gy, sZ = sm.ctl_gz;
-        auto gsite = [&](int32_t w) {  // site ids fit in int32 (checked when the job is added)
-          const int gx = wrap1(sX + unpack_dx(w), J.sx), gy = wrap1(sY + unpack_dy(w), J.sy),
-                    gz = wrap1(sZ + unpack_dz(w), J.sz);
-          return gx + J.sx * (gy + J.sy * gz);
-        };
-        if (eam) {  // the 78 exact density deltas, in shared memory and through to global memory
-          const int X = species_index(Xc);
-          for (int i = lane; i < kRefreshN; i += 32) {
-            const int32_t e = sm.rl[p][bsel][i];
-            const int j = s + local_delta(e, R);
-            const int32_t v = rho_s[j] + sm.dfq[X * 64 + rshells(e)];
-            rho_s[j] = v;
-            if (KIND == kEam64) FT.fc[j] = F64(FT, v);
-            J.rho[gsite(e)] = v;
-          }
-        }
-        if (lane == 0) {
-          const int32_t wg = sm.w1[p][bsel];
+      // first running sum above u * total, 32 entries per step
+      const int n8 = sm.ctl_n8;
+      const double expected = sm.ctl_expected;
+      int isel = -1;
+      for (int base = 0; base < n8 && isel < 0; base += 32) {
+        const int i = base + lane;
+        const unsigned m = __ballot_sync(kFull, i < n8 && sm.pre[i] > expected);
+        if (m) isel = base + __ffs(m) - 1;
+      }
+      if (lane == 0) {
+        const int stop = sm.ctl_stop;
+        sm.ctl_hop = isel >= 0;
+        if (isel >= 0) {
+          // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
+          const int ksel = sm.ord[isel >> 3], bsel = isel & 7;
+          const int s = sm.vloc[ksel];
+          const int p = s & 1;
           const int tl = s + sm.d1[p][bsel];
-          const int64_t to_g = gsite(wg);
+          const uint8_t Xc = occ_s[tl];
+          const int32_t wg = sm.w1[p][bsel];
+          const int sX = sm.vgx[ksel], sY = sm.vgy[ksel], sZ = sm.vgz[ksel];
+          const int ngx = wrap1(sX + unpack_dx(wg), jc.sx), ngy = wrap1(sY + unpack_dy(wg), jc.sy),
+                    ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
+          const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
+          const int32_t from_g = sm.vlid[ksel];
+          sm.ctl_ksel = ksel;
+          sm.ctl_bsel = bsel;
+          sm.ctl_s = s;
+          sm.ctl_X = Xc;
+          sm.ctl_from = from_g;
+          sm.ctl_to = to_g;
+          sm.ctl_gx = sX;
+          sm.ctl_gy = sY;
+          sm.ctl_gz = sZ;
           occ_s[tl] = kV;
           occ_s[s] = Xc;
-          J.occ[to_g] = kV;
-          J.occ[sm.ctl_from] = Xc;
+          jc.occ[to_g] = kV;
+          jc.occ[from_g] = Xc;
           // move the vacancy: local coordinates by the jump offset, no division needed
           const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
           const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
+          sm.ctl_qx = qx;
+          sm.ctl_qy = qy;
+          sm.ctl_qz = qz;
           sm.vcx[ksel] = static_cast<int16_t>(nlx);
           sm.vcy[ksel] = static_cast<int16_t>(nly);
           sm.vcz[ksel] = static_cast<int16_t>(nlz);
           sm.vloc[ksel] = tl;
-          sm.vlid[ksel] = static_cast<int32_t>(to_g);
-          sm.vgx[ksel] = wrap1(sX + unpack_dx(wg), J.sx);
-          sm.vgy[ksel] = wrap1(sY + unpack_dy(wg), J.sy);
-          sm.vgz[ksel] = wrap1(sZ + unpack_dz(wg), J.sz);
+          sm.vlid[ksel] = to_g;
+          sm.vgx[ksel] = ngx;
+          sm.vgy[ksel] = ngy;
+          sm.vgz[ksel] = ngz;
           const int cx = nlx >> 1;
           const bool in = cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
-          int pos = 0;
-          while (sm.ord[pos] != ksel) ++pos;
+          int pos = isel >> 3;  // ksel's place in the ordered list
           for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
           --nord;
           if (in) {
             int j = nord;
-            while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[ksel]) {
+            while (j > 0 && sm.vlid[sm.ord[j - 1]] > to_g) {
               sm.ord[j] = sm.ord[j - 1];
               --j;
             }
             sm.ord[j] = ksel;
             ++nord;
           }
-          int nd = 0;
-          for (int i = 0; i < nord; ++i) {
-            const int k = sm.ord[i];
-            const bool dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
-            sm.vdirty[k] = dirty ? 1 : 0;
-            nd += dirty ? 1 : 0;
-          }
           sm.ctl_nord = nord;
+        } else if (!stop) {  // u * total reached no event: nothing performed, the clock runs
+          if (a.mode == kModeSelectPerform) {
+            akmc_event* e = a.api_event;
+            e->round = 0;
+            e->hop = hop0;
+            e->from_site = -1;
+            e->to_site = -1;
+            e->block = B.local_id;
+            e->species = 0;
+            e->u = sm.ctl_u;
+            e->total = total_last;
+            e->dt = 0.0;
+            e->n_act = nord;
+            e->n_dirty = 0;
+            e->job = B.job;
+            e->reserved = 0;
+            sm.ctl_stop = 1;
+          }
+          sm.ctl_nord = 0;  // nothing to re-evaluate
+        }
+      }
+      __syncwarp();
+      if (isel >= 0) {
+        // dirty marks: vacancies within D cells of the hop's origin, 32 per step
+        const int n = sm.ctl_nord;
+        const int qx = sm.ctl_qx, qy = sm.ctl_qy, qz = sm.ctl_qz;
+        int nd = 0;
+        for (int base = 0; base < n; base += 32) {
+          const int i = base + lane;
+          bool dirty = false;
+          if (i < n) {
+            const int k = sm.ord[i];
+            dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
+            sm.vdirty[k] = dirty ? 1 : 0;
+          }
+          nd += __popc(__ballot_sync(kFull, dirty));
+        }
+        if (lane == 0) {
           sm.ctl_nd = nd;
-          sm.ctl_to = to_g;
           evals += nd;
           nact_sum += nact_last;
           ++nh;
@@ -738,9 +807,9 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
             e->round = 0;
             e->hop = hop0;
             e->from_site = sm.ctl_from;
-            e->to_site = to_g;
+            e->to_site = sm.ctl_to;
             e->block = B.local_id;
-            e->species = Xc;
+            e->species = sm.ctl_X;
             e->u = sm.ctl_u;
             e->total = total_last;
             e->dt = 0.0;
@@ -751,16 +820,15 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
             sm.ctl_stop = 1;
           }
         }
-      } else if (lane == 0 && !sm.ctl_stop) {
-        sm.ctl_nord = nord;  // no event: nothing dirty, the clock still advances
-        for (int i = 0; i < nord; ++i) sm.vdirty[sm.ord[i]] = 0;
       }
     }
     __syncthreads();  // (S) selection, lattice, list and dirty marks updated
     AKMC_PHASE(3);
-    if (sm.ctl_stop) break;
+    if (sm.ctl_stop) {
+      if (eam && sm.ctl_hop && tid < kRefreshN) refresh(tid);  // the per-hop entry point's hop
+      break;
+    }
   }
-
   __syncthreads();
   AKMC_PHASE(6);
   if (a.mode == kModeCalc) return;
@@ -773,7 +841,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
     B.hops += nh;
-    if (nh) atomicAdd(reinterpret_cast<unsigned long long*>(&J.hops), static_cast<unsigned long long>(nh));
+    if (nh) atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[B.job].hops), static_cast<unsigned long long>(nh));
     atomicAdd(a.counters + 0, static_cast<unsigned long long>(nh));
     atomicAdd(a.counters + 1, static_cast<unsigned long long>(evals));
     atomicAdd(a.counters + 3, 1ull);
@@ -850,7 +918,7 @@ __device__ void init_cta_smem(uint8_t* smem) {
   __syncthreads();
 }
 
-__global__ void __maxnreg__(112) k_hop(RoundArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
   if (static_cast<int>(blockIdx.x) >= na) return;
