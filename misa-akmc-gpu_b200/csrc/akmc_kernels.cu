@@ -77,7 +77,7 @@ struct Smem {
   int32_t vidx[kMaxV], vloc[kMaxV], vlid[kMaxV], ord[kMaxV];
   int16_t vcx[kMaxV], vcy[kMaxV], vcz[kMaxV];  // local coordinates (x in doubled sites)
   int32_t vgx[kMaxV], vgy[kMaxV], vgz[kMaxV];  // global coordinates
-  uint8_t vdirty[kMaxV];
+  uint8_t vact[kMaxV];          // vacancy still inside the active sector
   uint8_t vavb[kMaxV][8];       // jump b of vacancy k available (target is an atom)
   double rates[kMaxV][8];
   alignas(16) unsigned char fwin[kFWin * 32];  // F-table window: double c0..c3 or FCell32 per cell
@@ -88,8 +88,8 @@ struct Smem {
   double pre[kMaxV * 8];   // running sums of the ordered rates
   double ctl_u, ctl_unext, ctl_expected;
   int32_t ctl_from, ctl_to;
-  int32_t ctl_ksel, ctl_bsel, ctl_nord, ctl_nd, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop, ctl_hop, ctl_n8;
-  int32_t ctl_gx, ctl_gy, ctl_gz, ctl_qx, ctl_qy, ctl_qz;
+  int32_t ctl_ksel, ctl_bsel, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop, ctl_hop, ctl_n8;
+  int32_t ctl_gx, ctl_gy, ctl_gz, ctl_qx, ctl_qy, ctl_qz, ctl_pos;
   uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
   uint64_t xsn[4];        // selection stream after the uniform drawn ahead
 };
@@ -509,7 +509,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.vgx[tid] = X;
     sm.vgy[tid] = y;
     sm.vgz[tid] = z;
-    sm.vdirty[tid] = 1;  // the first evaluation pass computes every vacancy
+    sm.vact[tid] = 1;
   }
   __syncthreads();
   AKMC_PHASE(0);
@@ -527,7 +527,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       sm.xs[i] = B.xs[i];
       sm.xt[i] = B.xt[i];
     }
-    sm.ctl_nord = cnt;
     sm.ctl_next_stop = 0;
     sm.ctl_hop = 0;
     sm.ctl_ok = 1;
@@ -578,10 +577,11 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
 
   // Hop loop, two CTA barriers per hop:
   //  (E) warps 0..7 refresh the densities of the hop just performed, then evaluate the
-  //      dirty vacancies; the control thread runs the clock of that hop, decides whether
-  //      the sector is done and draws the next selection uniform ahead of time;
+  //      vacancies it made dirty; the control warp counts them, moves the hopped vacancy
+  //      in the ordered list, runs the clock of the hop, decides whether the sector is
+  //      done and draws the next selection uniform ahead of time;
   //  (S) the control warp forms the ordered total, selects the next hop and performs it
-  //      on the occupancy and the vacancy list.
+  //      on the occupancy and the vacancy record.
   // Clock and counters live in the control thread's registers.
   const int64_t hop0 = B.hops;
   int64_t nh = 0, nact_sum = 0, evals = cnt;
@@ -590,60 +590,102 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   bool clock_due = false;  // a selection with a positive total happened since the last clock
   const int D = eam ? 4 : 3;
   bool first = true;
+  // vacancies to evaluate: all active ones on the first pass, then those within D cells
+  // of the last hop's origin (every warp derives the same set)
+  auto dirty_mask = [&](int base) -> unsigned {
+    const int k = base + lane;
+    bool d = false;
+    if (k < cnt && sm.vact[k]) {
+      d = first || (abs((sm.vcx[k] >> 1) - sm.ctl_qx) <= D && abs(sm.vcy[k] - sm.ctl_qy) <= D &&
+                    abs(sm.vcz[k] - sm.ctl_qz) <= D);
+    }
+    return __ballot_sync(kFull, d);
+  };
   while (true) {
+    const bool hopped = !first && sm.ctl_hop;
     if (evaluator) {
-      if (eam && sm.ctl_hop) {
+      if (eam && hopped) {
         if (tid < kRefreshN) refresh(tid);
         asm volatile("bar.sync 1, 256;" ::: "memory");  // the evaluator warps only
       }
-      const int n = sm.ctl_nord;
-      for (int i = 0; i < n; ++i) {
-        const int k = sm.ord[i];
-        if (sm.vdirty[k]) eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr);
-      }
-    } else if (tid == kCtl) {
-      if (clock_due) {
-        clock_due = false;
-        int stop = 0;
-        const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
-        const double dt = -port_log(u2) / total_last;
-        sector_time += dt;
-        if (sm.ctl_hop && a.log_cap > 0) {
-          const unsigned long long slot = atomicAdd(a.log_count, 1ull);
-          if (slot < static_cast<unsigned long long>(a.log_cap)) {
-            akmc_event* e = a.log + slot;
-            e->round = B.round;
-            e->hop = hop0 + nh - 1;
-            e->from_site = sm.ctl_from;
-            e->to_site = sm.ctl_to;
-            e->block = B.local_id;
-            e->species = sm.ctl_X;
-            e->u = sm.ctl_u;
-            e->total = total_last;
-            e->dt = dt;
-            e->n_act = nact_last;
-            e->n_dirty = sm.ctl_nd;
-            e->job = B.job;
-            e->reserved = 0;
-          } else {
-            atomicOr(a.status, kErrLogOverflow);
+      if (first || hopped) {
+        for (int base = 0; base < cnt; base += 32) {
+          unsigned m = dirty_mask(base);
+          while (m) {
+            const int k = base + __ffs(m) - 1;
+            m &= m - 1;
+            eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr);
           }
         }
-        if (!(sector_time < thr)) stop = 1;
-        if (nh >= a.hop_cap) {
-          atomicOr(a.status, kErrHopCap);
-          stop = 1;
-        }
-        sm.ctl_next_stop = stop;
       }
-      if (a.mode == kModeRound && !sm.ctl_next_stop) {
-        // the next selection's uniform, committed only if a selection consumes it
-        uint64_t x[4] = {sm.xs[0], sm.xs[1], sm.xs[2], sm.xs[3]};
-        sm.ctl_unext = uniform_co(x);
-        for (int i = 0; i < 4; ++i) sm.xsn[i] = x[i];
+    } else {  // control warp
+      int nd = 0;
+      if (hopped)
+        for (int base = 0; base < cnt; base += 32) nd += __popc(dirty_mask(base));
+      if (lane == 0) {
+        if (hopped) {
+          // the hopped vacancy leaves its place in the ordered list and re-enters at its
+          // new site id if it is still inside the sector
+          const int ksel = sm.ctl_ksel;
+          for (int i = sm.ctl_pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
+          --nord;
+          if (sm.vact[ksel]) {
+            const int32_t key = sm.vlid[ksel];
+            int j = nord;
+            while (j > 0 && sm.vlid[sm.ord[j - 1]] > key) {
+              sm.ord[j] = sm.ord[j - 1];
+              --j;
+            }
+            sm.ord[j] = ksel;
+            ++nord;
+          }
+          evals += nd;
+          nact_sum += nact_last;
+          ++nh;
+        }
+        if (clock_due) {
+          clock_due = false;
+          int stop = 0;
+          const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
+          const double dt = -port_log(u2) / total_last;
+          sector_time += dt;
+          if (hopped && a.log_cap > 0) {
+            const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+            if (slot < static_cast<unsigned long long>(a.log_cap)) {
+              akmc_event* e = a.log + slot;
+              e->round = B.round;
+              e->hop = hop0 + nh - 1;
+              e->from_site = sm.ctl_from;
+              e->to_site = sm.ctl_to;
+              e->block = B.local_id;
+              e->species = sm.ctl_X;
+              e->u = sm.ctl_u;
+              e->total = total_last;
+              e->dt = dt;
+              e->n_act = nact_last;
+              e->n_dirty = nd;
+              e->job = B.job;
+              e->reserved = 0;
+            } else {
+              atomicOr(a.status, kErrLogOverflow);
+            }
+          }
+          if (!(sector_time < thr)) stop = 1;
+          if (nh >= a.hop_cap) {
+            atomicOr(a.status, kErrHopCap);
+            stop = 1;
+          }
+          sm.ctl_next_stop = stop;
+        }
+        if (a.mode == kModeRound && !sm.ctl_next_stop) {
+          // the next selection's uniform, committed only if a selection consumes it
+          uint64_t x[4] = {sm.xs[0], sm.xs[1], sm.xs[2], sm.xs[3]};
+          sm.ctl_unext = uniform_co(x);
+          for (int i = 0; i < 4; ++i) sm.xsn[i] = x[i];
+        }
       }
     }
-    __syncthreads();  // (E) rates and the clock decision visible
+    __syncthreads();  // (E) rates, list and the clock decision visible
     AKMC_PHASE(first ? 2 : 5);
     first = false;
     if (sm.ctl_next_stop) break;
@@ -703,7 +745,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         if (m) isel = base + __ffs(m) - 1;
       }
       if (lane == 0) {
-        const int stop = sm.ctl_stop;
         sm.ctl_hop = isel >= 0;
         if (isel >= 0) {
           // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
@@ -718,8 +759,13 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
                     ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
           const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
           const int32_t from_g = sm.vlid[ksel];
+          occ_s[tl] = kV;
+          occ_s[s] = Xc;
+          jc.occ[to_g] = kV;
+          jc.occ[from_g] = Xc;
           sm.ctl_ksel = ksel;
           sm.ctl_bsel = bsel;
+          sm.ctl_pos = isel >> 3;
           sm.ctl_s = s;
           sm.ctl_X = Xc;
           sm.ctl_from = from_g;
@@ -727,10 +773,6 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           sm.ctl_gx = sX;
           sm.ctl_gy = sY;
           sm.ctl_gz = sZ;
-          occ_s[tl] = kV;
-          occ_s[s] = Xc;
-          jc.occ[to_g] = kV;
-          jc.occ[from_g] = Xc;
           // move the vacancy: local coordinates by the jump offset, no division needed
           const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
           const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
@@ -746,83 +788,53 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           sm.vgy[ksel] = ngy;
           sm.vgz[ksel] = ngz;
           const int cx = nlx >> 1;
-          const bool in = cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
-          int pos = isel >> 3;  // ksel's place in the ordered list
-          for (int i = pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
-          --nord;
-          if (in) {
-            int j = nord;
-            while (j > 0 && sm.vlid[sm.ord[j - 1]] > to_g) {
-              sm.ord[j] = sm.ord[j - 1];
-              --j;
-            }
-            sm.ord[j] = ksel;
-            ++nord;
-          }
-          sm.ctl_nord = nord;
-        } else if (!stop) {  // u * total reached no event: nothing performed, the clock runs
-          if (a.mode == kModeSelectPerform) {
-            akmc_event* e = a.api_event;
-            e->round = 0;
-            e->hop = hop0;
-            e->from_site = -1;
-            e->to_site = -1;
-            e->block = B.local_id;
-            e->species = 0;
-            e->u = sm.ctl_u;
-            e->total = total_last;
-            e->dt = 0.0;
-            e->n_act = nord;
-            e->n_dirty = 0;
-            e->job = B.job;
-            e->reserved = 0;
-            sm.ctl_stop = 1;
-          }
-          sm.ctl_nord = 0;  // nothing to re-evaluate
+          sm.vact[ksel] =
+              cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
+        } else if (!sm.ctl_stop && a.mode == kModeSelectPerform) {  // u * total reached no event
+          akmc_event* e = a.api_event;
+          e->round = 0;
+          e->hop = hop0;
+          e->from_site = -1;
+          e->to_site = -1;
+          e->block = B.local_id;
+          e->species = 0;
+          e->u = sm.ctl_u;
+          e->total = total_last;
+          e->dt = 0.0;
+          e->n_act = nord;
+          e->n_dirty = 0;
+          e->job = B.job;
+          e->reserved = 0;
+          sm.ctl_stop = 1;
         }
       }
-      __syncwarp();
-      if (isel >= 0) {
-        // dirty marks: vacancies within D cells of the hop's origin, 32 per step
-        const int n = sm.ctl_nord;
-        const int qx = sm.ctl_qx, qy = sm.ctl_qy, qz = sm.ctl_qz;
+      if (a.mode == kModeSelectPerform && isel >= 0) {  // the per-hop entry point stops here
+        __syncwarp();
         int nd = 0;
-        for (int base = 0; base < n; base += 32) {
-          const int i = base + lane;
-          bool dirty = false;
-          if (i < n) {
-            const int k = sm.ord[i];
-            dirty = abs((sm.vcx[k] >> 1) - qx) <= D && abs(sm.vcy[k] - qy) <= D && abs(sm.vcz[k] - qz) <= D;
-            sm.vdirty[k] = dirty ? 1 : 0;
-          }
-          nd += __popc(__ballot_sync(kFull, dirty));
-        }
+        for (int base = 0; base < cnt; base += 32) nd += __popc(dirty_mask(base));
         if (lane == 0) {
-          sm.ctl_nd = nd;
+          akmc_event* e = a.api_event;
+          e->round = 0;
+          e->hop = hop0;
+          e->from_site = sm.ctl_from;
+          e->to_site = sm.ctl_to;
+          e->block = B.local_id;
+          e->species = sm.ctl_X;
+          e->u = sm.ctl_u;
+          e->total = total_last;
+          e->dt = 0.0;
+          e->n_act = nact_last;
+          e->n_dirty = nd;
+          e->job = B.job;
+          e->reserved = 0;
+          nh = 1;
           evals += nd;
           nact_sum += nact_last;
-          ++nh;
-          if (a.mode == kModeSelectPerform) {
-            akmc_event* e = a.api_event;
-            e->round = 0;
-            e->hop = hop0;
-            e->from_site = sm.ctl_from;
-            e->to_site = sm.ctl_to;
-            e->block = B.local_id;
-            e->species = sm.ctl_X;
-            e->u = sm.ctl_u;
-            e->total = total_last;
-            e->dt = 0.0;
-            e->n_act = nact_last;
-            e->n_dirty = nd;
-            e->job = B.job;
-            e->reserved = 0;
-            sm.ctl_stop = 1;
-          }
+          sm.ctl_stop = 1;
         }
       }
     }
-    __syncthreads();  // (S) selection, lattice, list and dirty marks updated
+    __syncthreads();  // (S) selection, lattice and vacancy record updated
     AKMC_PHASE(3);
     if (sm.ctl_stop) {
       if (eam && sm.ctl_hop && tid < kRefreshN) refresh(tid);  // the per-hop entry point's hop
