@@ -34,8 +34,8 @@ struct HostJob {
 
 struct DevPot {
   Potential P;
-  double* d_coef = nullptr;
-  FCell32* d_f32 = nullptr;
+  double* d_coef = nullptr;  // planes (c0, c1) then (c2, c3), kTabN cells each
+  float* d_f32 = nullptr;    // planes (hi, lo, c1, c2) then c3
   std::vector<double> coef;
   std::vector<FCell32> f32;
   bool has_eam = false;
@@ -358,13 +358,30 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(cudaMemcpyAsync(ctx->d_geo, &geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
   std::vector<Potential> hp;
   for (auto& p : ctx->pots) {
-    CK(dalloc(&p.d_coef, p.coef.size()));
-    CK(dalloc(&p.d_f32, p.f32.size()));
-    CK(cudaMemcpyAsync(p.d_coef, p.coef.data(), p.coef.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.d_f32, p.f32.data(), p.f32.size() * sizeof(FCell32), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<double> c64(static_cast<size_t>(kTabN) * 4);
+    std::vector<float> c32(static_cast<size_t>(kTabN) * 5);
+    for (size_t k = 0; k < static_cast<size_t>(kTabN); ++k) {
+      for (int j = 0; j < 2; ++j) {
+        c64[2 * k + j] = p.coef[4 * k + j];
+        c64[2 * kTabN + 2 * k + j] = p.coef[4 * k + 2 + j];
+      }
+      const FCell32& f = p.f32[k];
+      c32[4 * k + 0] = f.hi;
+      c32[4 * k + 1] = f.lo;
+      c32[4 * k + 2] = f.c1;
+      c32[4 * k + 3] = f.c2;
+      c32[4 * static_cast<size_t>(kTabN) + k] = f.c3;
+    }
+    CK(dalloc(&p.d_coef, c64.size()));
+    CK(dalloc(&p.d_f32, c32.size()));
+    CK(cudaMemcpyAsync(p.d_coef, c64.data(), c64.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(p.d_f32, c32.data(), c32.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the staging vectors go out of scope
     Potential P = p.P;
-    P.Fcoef = p.d_coef;
-    P.F32 = p.d_f32;
+    P.F64lo = reinterpret_cast<const double2*>(p.d_coef);
+    P.F64hi = reinterpret_cast<const double2*>(p.d_coef) + kTabN;
+    P.F32a = reinterpret_cast<const float4*>(p.d_f32);
+    P.F32b = p.d_f32 + 4 * static_cast<size_t>(kTabN);
     hp.push_back(P);
   }
   CK(dalloc(&ctx->d_pots, hp.size()));
@@ -462,6 +479,9 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.vac_job = ctx->d_vac_job;
   a.nvac = nv;
   a.mode = kModeRound;
+  a.kind_mask = 0;
+  for (const auto& j : ctx->jobs)
+    a.kind_mask |= 1 << (j.cfg.energy_model == AKMC_MODEL_PAIRBOND ? 0 : (j.cfg.precision == AKMC_FP32C ? 2 : 1));
   a.blk_list = ctx->d_blk_list;
   a.active = ctx->d_active;
   a.n_active = ctx->d_n_active;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <vector_types.h>
 
 #include "../../include/akmc.h"
 #include "akmc_common.cuh"
@@ -42,8 +43,12 @@ struct Potential {
   double phi64[4][4][8];    // pair energy by (moving species, neighbour species, shell code)
   float phi32[4][4][8];
   double b1[5][5], b2[5][5];  // pair-bond 1nn / 2nn tables (V, Fe, Cu, Ni, Mn)
-  const double* Fcoef;      // kTabN x 4 doubles
-  const FCell32* F32;       // kTabN cells
+  // F(rho) cells in two planes, so that a cell's two 16-byte halves fall into
+  // different shared-memory bank groups for random cells
+  const double2* F64lo;     // (c0, c1) per cell
+  const double2* F64hi;     // (c2, c3) per cell
+  const float4* F32a;       // (hi, lo, c1, c2) per cell
+  const float* F32b;        // c3 per cell
   int32_t fwin0;            // first F-table cell of the shared-memory window
   int32_t pad;
 };
@@ -100,6 +105,7 @@ struct RoundArgs {
   int32_t* vac_job;
   int32_t nvac;
   int32_t mode;
+  int32_t kind_mask;  // energy kinds present: bit 0 pair-bond, 1 EAM FP64, 2 EAM FP32-comp
   int32_t* blk_list;  // nblocks * kMaxV
   int32_t* active;    // nblocks
   int32_t* n_active;

@@ -80,7 +80,9 @@ struct Smem {
   uint8_t vact[kMaxV];          // vacancy still inside the active sector
   uint8_t vavb[kMaxV][8];       // jump b of vacancy k available (target is an atom)
   double rates[kMaxV][8];
-  alignas(16) unsigned char fwin[kFWin * 32];  // F-table window: double c0..c3 or FCell32 per cell
+  // F-table window, two planes: FP64 (c0, c1) x kFWin then (c2, c3) x kFWin;
+  // FP32 (hi, lo, c1, c2) x kFWin then c3 x kFWin
+  alignas(16) unsigned char fwin[kFWin * 32];
   alignas(8) uint64_t mbar;                    // completion barrier of the window's bulk copy
   uint32_t mbar_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
@@ -102,9 +104,13 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// Arms the barrier for `bytes` of bulk copies (then issued with bulk_copy).
+__device__ __forceinline__ void bulk_expect(uint64_t* bar, uint32_t bytes) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Global -> shared bulk copy; addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
@@ -128,8 +134,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
 struct FTab {
   const unsigned char* win;
   int kw0;
-  const double* g64;
-  const FCell32* g32;
+  const double2* g64lo;
+  const double2* g64hi;
+  const float4* g32a;
+  const float* g32b;
   unsigned int* status;
   unsigned long long* prof;  // sub-phase cycles of the evaluation (profiling builds)
   double* fc;                // F(rho) of every staged site (FP64 form)
@@ -207,15 +215,15 @@ __device__ __forceinline__ int jshells(int32_t e) { return (e >> 16) & 63; }
 __device__ __forceinline__ int rshells(int32_t e) { return (e >> 24) & 63; }
 
 // Cells outside the shared-memory window (rare): global memory, range-checked.
-__device__ __noinline__ double F64_far(const FTab& T, int32_t r, double p) {
+__device__ __noinline__ double F64_far(const double2* g64lo, const double2* g64hi, unsigned int* status, int32_t r,
+                                       double p) {
   const int k = r >> kRhoCellShift;
   int kc = k;
   if (r < 0 || k > kTabN - 2) {
-    atomicOr(T.status, kErrRhoRange);
+    atomicOr(status, kErrRhoRange);
     kc = r < 0 ? 0 : kTabN - 2;
   }
-  const double2* c = reinterpret_cast<const double2*>(T.g64) + 2 * kc;
-  const double2 lo = __ldg(c), hi = __ldg(c + 1);
+  const double2 lo = __ldg(g64lo + kc), hi = __ldg(g64hi + kc);
   return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
 }
 
@@ -225,33 +233,32 @@ __device__ __forceinline__ double F64(const FTab& T, int32_t r) {
   const double p = __hiloint2double(0x3FF00000 | ((r & kRhoFracMask) << 3), 0) - 1.0;
   const unsigned kk = static_cast<unsigned>(k - T.kw0);
   if (kk < static_cast<unsigned>(kFWin)) {
-    const double2* c = reinterpret_cast<const double2*>(T.win) + 2 * kk;
-    const double2 lo = c[0], hi = c[1];
+    const double2 lo = reinterpret_cast<const double2*>(T.win)[kk];
+    const double2 hi = reinterpret_cast<const double2*>(T.win)[kFWin + kk];
     return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
   }
-  return F64_far(T, r, p);
+  return F64_far(T.g64lo, T.g64hi, T.status, r, p);
 }
 
 __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
   const int k = r >> kRhoCellShift;
   const unsigned kk = static_cast<unsigned>(k - T.kw0);
-  float4 a, b;
+  float4 a;
+  float c3;
   if (kk < static_cast<unsigned>(kFWin)) {
-    const float4* q = reinterpret_cast<const float4*>(T.win) + 2 * kk;
-    a = q[0];
-    b = q[1];
+    a = reinterpret_cast<const float4*>(T.win)[kk];
+    c3 = reinterpret_cast<const float*>(T.win + kFWin * 16)[kk];
   } else {
     int kc = k;
     if (r < 0 || k > kTabN - 2) {
       atomicOr(T.status, kErrRhoRange);
       kc = r < 0 ? 0 : kTabN - 2;
     }
-    const float4* q = reinterpret_cast<const float4*>(T.g32 + kc);
-    a = __ldg(q);
-    b = __ldg(q + 1);
+    a = __ldg(T.g32a + kc);
+    c3 = __ldg(T.g32b + kc);
   }
   FCell32 c;
-  c.hi = a.x; c.lo = a.y; c.c1 = a.z; c.c2 = a.w; c.c3 = b.x;
+  c.hi = a.x; c.lo = a.y; c.c1 = a.z; c.c2 = a.w; c.c3 = c3;
   c.pad0 = c.pad1 = c.pad2 = 0.f;
   return c;
 }
@@ -433,16 +440,24 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const bool need_win = eam && sm.win_pot != win_key;
   __syncthreads();  // every thread has read win_pot; the previous item's readers are done
   if (need_win && tid == kCtl) {
-    const void* src = KIND == kEam32 ? static_cast<const void*>(P.F32 + P.fwin0)
-                                     : static_cast<const void*>(P.Fcoef + 4 * static_cast<int64_t>(P.fwin0));
-    bulk_load(sm.fwin, src, kFWin * 32u, &sm.mbar);
+    if (KIND == kEam32) {
+      bulk_expect(&sm.mbar, kFWin * 20u);
+      bulk_copy(sm.fwin, P.F32a + P.fwin0, kFWin * 16u, &sm.mbar);
+      bulk_copy(sm.fwin + kFWin * 16, P.F32b + P.fwin0, kFWin * 4u, &sm.mbar);
+    } else {
+      bulk_expect(&sm.mbar, kFWin * 32u);
+      bulk_copy(sm.fwin, P.F64lo + P.fwin0, kFWin * 16u, &sm.mbar);
+      bulk_copy(sm.fwin + kFWin * 16, P.F64hi + P.fwin0, kFWin * 16u, &sm.mbar);
+    }
   }
   load_tables(sm, P, *a.geo, R, eam);
   FTab FT;
   FT.win = sm.fwin;
   FT.kw0 = P.fwin0;
-  FT.g64 = P.Fcoef;
-  FT.g32 = P.F32;
+  FT.g64lo = P.F64lo;
+  FT.g64hi = P.F64hi;
+  FT.g32a = P.F32a;
+  FT.g32b = P.F32b;
   FT.status = a.status;
   FT.prof = a.counters + 16;
   FT.fc = fcache_of(rho_s, R.n);
@@ -930,12 +945,30 @@ __device__ void init_cta_smem(uint8_t* smem) {
   __syncthreads();
 }
 
+__device__ __forceinline__ int job_kind(const JobDev& J) {
+  return J.model == AKMC_MODEL_PAIRBOND ? kPairBond : (J.precision == AKMC_FP32C ? kEam32 : kEam64);
+}
+
+// One kernel per energy kind, so each holds only its own hop loop (instruction-cache
+// footprint); items of other kinds are left to their kernel.
+template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
   if (static_cast<int>(blockIdx.x) >= na) return;
   init_cta_smem(smem);
-  for (int item = blockIdx.x; item < na; item += gridDim.x) dispatch_block(a, a.active[item], smem);
+  for (int item = blockIdx.x; item < na; item += gridDim.x) {
+    const int gb = a.active[item];
+    const BlockDev& B = a.blocks[gb];
+    if (job_kind(a.jobs[B.job]) != KIND) continue;
+    Region R;
+    make_region(B, sector_of_round(B.round), R);
+    Smem* sm;
+    uint8_t* occ_s;
+    int32_t* rho_s;
+    carve(smem, R.n, sm, occ_s, rho_s);
+    run_block<KIND>(a, gb, *sm, occ_s, rho_s);
+  }
 }
 
 __global__ void k_finalize(RoundArgs a) {
@@ -1045,7 +1078,9 @@ int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, vo
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a.nvac > 0) k_bucket<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
   if (ev0) cudaEventRecord(static_cast<cudaEvent_t>(ev0), st);
-  k_hop<<<hop_grid, kThreads, smem, st>>>(a);
+  if (a.kind_mask & (1 << kEam64)) k_hop<kEam64><<<hop_grid, kThreads, smem, st>>>(a);
+  if (a.kind_mask & (1 << kEam32)) k_hop<kEam32><<<hop_grid, kThreads, smem, st>>>(a);
+  if (a.kind_mask & (1 << kPairBond)) k_hop<kPairBond><<<hop_grid, kThreads, smem, st>>>(a);
   if (ev1) cudaEventRecord(static_cast<cudaEvent_t>(ev1), st);
   k_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
@@ -1060,7 +1095,12 @@ int launch_api(const RoundArgs& a, size_t smem, void* stream) {
 }
 
 int configure_hop_smem(size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(k_hop, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaError_t e = cudaFuncSetAttribute(k_hop<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_hop<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_hop<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
   e = cudaFuncSetAttribute(k_api_block, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   return static_cast<int>(e);

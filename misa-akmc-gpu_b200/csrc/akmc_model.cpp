@@ -196,7 +196,8 @@ int build_potential(const akmc_eam_tables* t, Potential& P, std::vector<double>&
   int64_t rbulk = 0;
   for (int i = 0; i < nsh; ++i) rbulk += static_cast<int64_t>(counts[i]) * P.fq[0][i + 1];
   const int kb = static_cast<int>(rbulk >> kRhoCellShift);
-  P.fwin0 = std::max(1, std::min(kb - (3 * kFWin) / 4, kTabN - 2 - kFWin));
+  // window start a multiple of 4 cells: the bulk copies of its planes start 16-byte aligned
+  P.fwin0 = std::max(0, std::min(kb - (3 * kFWin) / 4, kTabN - 2 - kFWin)) & ~3;
   for (int k = 0; k + 1 < kTabN; ++k) {
     double c[4];
     cell_coefs(t->F, kTabN, k, c);
