@@ -836,6 +836,76 @@ struct Job {
     ++round;
     return 0;
   }
+
+  // Asynchronous order: each (block, round) runs as soon as, for every neighbour offset
+  // d in {-1,0,1}^3, the neighbour has completed its latest earlier round whose staged
+  // region (sector plus a 2-cell halo) overlaps this round's region.  Items are taken in
+  // a random order among the ready ones; the result must equal run_round's.
+  static int flow_lag(int phase, const int d[3]) {
+    const int now = kSectorOrder[phase];
+    for (int k = 1; k <= 8; ++k) {
+      const int then = kSectorOrder[(phase - k + 8) % 8];
+      bool ov = true;
+      for (int a = 0; a < 3 && ov; ++a) {
+        const int hn = (now >> a) & 1, ht = (then >> a) & 1;
+        if (d[a] == 1) ov = hn == 1 && ht == 0;    // the +1 neighbour's low half meets our high half
+        if (d[a] == -1) ov = hn == 0 && ht == 1;   // the -1 neighbour's high half meets our low half
+      }
+      if (ov) return k;
+    }
+    return 0;  // no region of that neighbour ever meets this one
+  }
+  int run_rounds_flow(int64_t n_rounds, uint64_t order_seed) {
+    if (small_blocks) return -3;
+    const int64_t r0 = round;
+    std::vector<int64_t> done(static_cast<size_t>(nblocks), r0);  // rounds completed
+    Xoshiro pick = make_stream(order_seed, 99, 0);
+    std::vector<int> ready;
+    for (;;) {
+      ready.clear();
+      bool all = true;
+      for (int b = 0; b < nblocks; ++b) {
+        const int64_t r = done[static_cast<size_t>(b)];
+        if (r >= r0 + n_rounds) continue;
+        all = false;
+        const int bi[3] = {b % nb[0], (b / nb[0]) % nb[1], b / (nb[0] * nb[1])};
+        bool ok = true;
+        for (int dz = -1; dz <= 1 && ok; ++dz)
+          for (int dy = -1; dy <= 1 && ok; ++dy)
+            for (int dx = -1; dx <= 1 && ok; ++dx) {
+              const int d[3] = {dx, dy, dz};
+              const int k = flow_lag(static_cast<int>(r % 8), d);
+              if (!k) continue;
+              int yi[3];
+              for (int a = 0; a < 3; ++a) yi[a] = (bi[a] + d[a] + nb[a]) % nb[a];
+              const int y = yi[0] + nb[0] * (yi[1] + nb[1] * yi[2]);
+              if (done[static_cast<size_t>(y)] < r - k + 1) ok = false;
+            }
+        if (ok) ready.push_back(b);
+      }
+      if (all) break;
+      if (ready.empty()) return -11;  // no item ready: the rule would deadlock
+      int b = ready[0];
+      if (order_seed) {
+        b = ready[static_cast<size_t>(pick.below(ready.size()))];
+      } else {  // seed 0: the ready block furthest ahead, to stretch the skew between blocks
+        for (int c2 : ready)
+          if (done[static_cast<size_t>(c2)] > done[static_cast<size_t>(b)]) b = c2;
+      }
+      std::vector<ao_event> ev;
+      int64_t st[4] = {0, 0, 0, 0};
+      const int rc = run_block(b, done[static_cast<size_t>(b)], ev, st);
+      if (rc) return rc;
+      hops += st[0];
+      st_nact += st[1];
+      st_dirty += st[2];
+      st_start += st[3];
+      if (c.log_events) events.insert(events.end(), ev.begin(), ev.end());
+      ++done[static_cast<size_t>(b)];
+    }
+    round = r0 + n_rounds;
+    return 0;
+  }
 };
 
 int64_t ratio_total(const ao_config& c) {
@@ -993,6 +1063,10 @@ int ao_get_rho(void* h, int32_t* out) {
   std::memcpy(out, J->rho.data(), static_cast<size_t>(J->ns) * 4);
   return 0;
 }
+int ao_run_rounds_flow(void* h, int64_t n_rounds, uint64_t order_seed) {
+  return static_cast<Job*>(h)->run_rounds_flow(n_rounds, order_seed);
+}
+
 int ao_run_rounds(void* h, int64_t n_rounds) {
   Job* J = static_cast<Job*>(h);
   for (int64_t i = 0; i < n_rounds; ++i) {

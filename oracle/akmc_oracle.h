@@ -85,6 +85,11 @@ int ao_get_rho(void* h, int32_t* out);
  * max_rounds rounds. Returns 0 on success, negative on error. */
 int ao_run_rounds(void* h, int64_t n_rounds);
 int ao_run(void* h, int64_t hop_budget, int64_t max_rounds);
+/* n_rounds rounds of every block in a random dependency-respecting order instead of
+ * round by round (a block's round waits only for the neighbour rounds whose staged
+ * regions overlap it).  order_seed 0 always runs the ready block furthest ahead.
+ * Must leave the same state and events as ao_run_rounds. */
+int ao_run_rounds_flow(void* h, int64_t n_rounds, uint64_t order_seed);
 
 int64_t ao_round(void* h);
 int64_t ao_total_hops(void* h);

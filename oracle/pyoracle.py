@@ -106,6 +106,7 @@ def lib():
             ("ao_get_occupancy", [vp, dp]),
             ("ao_get_rho", [vp, dp]),
             ("ao_run_rounds", [vp, i64]),
+            ("ao_run_rounds_flow", [vp, i64, C.c_uint64]),
             ("ao_run", [vp, i64, i64]),
             ("ao_get_events", [vp, dp, i64, i64]),
             ("ao_get_block_state", [vp, dp, dp]),
@@ -227,6 +228,11 @@ class Oracle:
 
     def run_rounds(self, n):
         rc = lib().ao_run_rounds(self.h, n)
+        if rc:
+            raise RuntimeError("oracle run failed %d" % rc)
+
+    def run_rounds_flow(self, n, order_seed):
+        rc = lib().ao_run_rounds_flow(self.h, n, order_seed)
         if rc:
             raise RuntimeError("oracle run failed %d" % rc)
 
