@@ -162,6 +162,15 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds);
  * contexts of a device: calls whose rounds overlap on the device race.  Kernel
  * timing mode is not applied. */
 AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
+/* Order in which akmc_run_rounds runs the rounds of different domain blocks.
+ * ROUNDS: every block finishes round r before any starts r+1 (SubLattice::startTimeLoop,
+ * sublattice.inl:61-179, with the blocks as MPI ranks).  FLOW: a block's round waits only
+ * for the neighbour rounds whose staged regions (sector plus a 2-cell halo) overlap it, so
+ * blocks with few hops run ahead; results are identical to ROUNDS.  FLOW serves no hop
+ * budget.  AUTO (default): FLOW when the context holds more than one domain block, no job
+ * has a hop budget and every block area starts with at most 32 vacancies, else ROUNDS.  akmc_run_rounds_noalloc always runs ROUNDS. */
+enum { AKMC_SCHEDULE_AUTO = 0, AKMC_SCHEDULE_ROUNDS = 1, AKMC_SCHEDULE_FLOW = 2 };
+AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule);
 /* Runs until every job is done (hop budget or max_rounds) or max_rounds pass. */
 AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds);
 AKMC_API akmc_status akmc_sync(akmc_ctx* ctx);

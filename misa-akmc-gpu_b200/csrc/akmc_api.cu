@@ -78,6 +78,16 @@ struct akmc_ctx {
   cudaGraph_t graph_def = nullptr;
   int graph_rounds = 0;
   int32_t* d_vac_count = nullptr;
+  // asynchronous round schedule
+  int32_t schedule = AKMC_SCHEDULE_AUTO;
+  bool flow_ok = false;  // no hop budget, and every block area starts with few enough vacancies
+  int flow_grid = 0;
+  int32_t* d_lease = nullptr;
+  unsigned long long* d_vclaim = nullptr;
+  unsigned long long* d_vvalid = nullptr;
+  int32_t* d_vslot = nullptr;
+  int32_t* d_vcount = nullptr;
+  int32_t* d_flow = nullptr;  // flow_need[3], flow_done[3]
   // kernel timing mode: rounds launched one by one with events around the hop kernel
   bool timing = false;
   std::vector<cudaEvent_t> ev;
@@ -111,7 +121,8 @@ akmc_status check_status(akmc_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
   if (!st) return AKMC_OK;
   CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned int), ctx->stream));
-  if (st & kErrVacOverflow) return fail(ctx, AKMC_EOVERFLOW, "more than AKMC_MAX_SECTOR_VACANCIES vacancies in one sector");
+  if (st & kErrVacOverflow)
+    return fail(ctx, AKMC_EOVERFLOW, "more than 64 vacancies in one sector (or, under AKMC_SCHEDULE_FLOW, one block area)");
   if (st & kErrRhoRange) return fail(ctx, AKMC_ERANGE, "a density left the F table");
   if (st & kErrHopCap) return fail(ctx, AKMC_ERANGE, "a block exceeded the hop cap of one round");
   if (st & kErrLogOverflow) return fail(ctx, AKMC_EOVERFLOW, "event log full");
@@ -123,6 +134,11 @@ void free_device(akmc_ctx* ctx) {
   ctx->ev.clear();
   cudaFree(ctx->d_vac_count);
   ctx->d_vac_count = nullptr;
+  void* flow_ptrs[] = {ctx->d_lease, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vcount, ctx->d_flow};
+  for (void* p : flow_ptrs) cudaFree(p);
+  ctx->d_lease = nullptr;
+  ctx->d_vclaim = ctx->d_vvalid = nullptr;
+  ctx->d_vslot = ctx->d_vcount = ctx->d_flow = nullptr;
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->graph_def) cudaGraphDestroy(ctx->graph_def);
   ctx->graph = nullptr;
@@ -344,6 +360,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   // 256-thread CTAs at <= 128 registers: at most two per SM
   int per_sm = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
   ctx->hop_grid = std::max(1, std::min(nb, sms * per_sm));
+  ctx->flow_grid = std::max(1, std::min(nb, sms));
 
   // geometry and potentials
   Geometry geo;
@@ -448,6 +465,38 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(&ctx->d_status, 1));
   CK(dalloc(&ctx->d_counters, 24));
   CK(dalloc(&ctx->d_vac_count, 1));
+  CK(dalloc(&ctx->d_lease, static_cast<size_t>(nb)));
+  CK(dalloc(&ctx->d_vclaim, static_cast<size_t>(nb)));
+  CK(dalloc(&ctx->d_vvalid, static_cast<size_t>(nb)));
+  CK(dalloc(&ctx->d_vslot, static_cast<size_t>(nb) * kFlowSlots));
+  CK(dalloc(&ctx->d_vcount, static_cast<size_t>(nb)));
+  CK(dalloc(&ctx->d_flow, 6));
+  {
+    // the asynchronous schedule keeps each block area's vacancies in kFlowSlots slots;
+    // it is chosen only with room left for vacancies to gather
+    std::vector<int32_t> per_block(static_cast<size_t>(nb), 0);
+    bool budget = false;
+    for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
+      const HostJob& j = ctx->jobs[ji];
+      budget = budget || j.cfg.hop_budget > 0;
+      const int nbx = static_cast<int>(j.split[0].size()) - 1, nby = static_cast<int>(j.split[1].size()) - 1;
+      for (int32_t k = j.vac0; k < j.vac0 + static_cast<int32_t>(j.nvac); ++k) {
+        const int64_t s = vsite[static_cast<size_t>(k)];
+        const int64_t X = s % (2 * j.cfg.box[0]), t = s / (2 * j.cfg.box[0]);
+        const int64_t c[3] = {X >> 1, t % j.cfg.box[1], t / j.cfg.box[1]};
+        int bi[3];
+        for (int d = 0; d < 3; ++d) {
+          const auto& sp = j.split[d];
+          bi[d] = static_cast<int>(std::upper_bound(sp.begin(), sp.end(), static_cast<int32_t>(c[d])) - sp.begin()) - 1;
+        }
+        per_block[static_cast<size_t>(j.block0 + bi[0] + nbx * (bi[1] + nby * bi[2]))] += 1;
+      }
+    }
+    int32_t mx = 0;
+    for (int32_t v : per_block) mx = std::max(mx, v);
+    // one block gains nothing from running rounds apart
+    ctx->flow_ok = !budget && mx <= kFlowSlots / 2 && nb > 1;
+  }
   CK(dalloc(&ctx->d_log_count, 1));
   CK(dalloc(&ctx->d_api_total, 1));
   CK(dalloc(&ctx->d_api_event, 1));
@@ -497,6 +546,13 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.api_sector = -1;
   a.api_total = ctx->d_api_total;
   a.api_event = ctx->d_api_event;
+  a.lease = ctx->d_lease;
+  a.vclaim = ctx->d_vclaim;
+  a.vvalid = ctx->d_vvalid;
+  a.vslot = ctx->d_vslot;
+  a.vcount = ctx->d_vcount;
+  a.flow_need = ctx->d_flow;
+  a.flow_done = ctx->d_flow + 3;
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->h_jobs = hj;
   ctx->h_blocks = hb;
@@ -557,6 +613,34 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
   CK(cudaSetDevice(ctx->cfg.device));
   RoundArgs a = ctx->args;
   a.mode = kModeRound;
+  const bool flow = ctx->schedule == AKMC_SCHEDULE_FLOW || (ctx->schedule == AKMC_SCHEDULE_AUTO && ctx->flow_ok);
+  if (flow) {
+    // up to 1024 rounds per launch of the persistent flow kernels
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing) {
+      while (ctx->ev.size() < 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ctx->ev.push_back(e);
+      }
+      e0 = ctx->ev[0];
+      e1 = ctx->ev[1];
+    }
+    for (int64_t left = n_rounds; left > 0;) {
+      a.flow_rounds = std::min<int64_t>(left, 1024);
+      left -= a.flow_rounds;
+      const int e = launch_flow(a, ctx->flow_grid, ctx->smem, ctx->stream, e0, e1);
+      if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+      if (ctx->timing) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        ctx->hop_ms += ms;
+        ctx->hop_launches += 1;
+      }
+    }
+    return AKMC_OK;
+  }
   if (ctx->timing) {
     // one launch sequence per round, events around every hop kernel
     const size_t pool = 512;
@@ -654,6 +738,17 @@ AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds) {
     const int e = launch_round(a, ctx->hop_grid, ctx->smem, ctx->stream, nullptr, nullptr);
     if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
   }
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule) {
+  if (!ctx) return AKMC_EINVAL;
+  if (schedule < AKMC_SCHEDULE_AUTO || schedule > AKMC_SCHEDULE_FLOW)
+    return fail(ctx, AKMC_EINVAL, "schedule: AKMC_SCHEDULE_AUTO, _ROUNDS or _FLOW");
+  for (const auto& j : ctx->jobs)
+    if (schedule == AKMC_SCHEDULE_FLOW && j.cfg.hop_budget > 0)
+      return fail(ctx, AKMC_EINVAL, "the asynchronous schedule does not serve hop budgets");
+  ctx->schedule = schedule;
   return AKMC_OK;
 }
 

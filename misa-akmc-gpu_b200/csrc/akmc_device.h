@@ -14,6 +14,7 @@ constexpr int kNoAllocMaxBlocks = AKMC_NOALLOC_MAX_BLOCKS;
 constexpr int kJumpN = 76;                        // |N(s) u N(t)| - 2 sites per jump
 constexpr int kRefreshN = 78;                     // density refresh sites per jump
 constexpr int kShellNb = 58;                      // neighbours within the 5-shell cutoff
+constexpr int kFlowSlots = 64;                    // vacancies held in one domain block's area
 
 // Packed neighbour entry: int8 dX | int8 dy << 8 | int8 dz << 16 | (sh_s | sh_t << 4) << 24,
 // dX in doubled-x site units; shell codes 0 = outside the cutoff, 1..5 shells, 6 = the site itself.
@@ -83,6 +84,7 @@ struct BlockDev {
   uint64_t xs[4], xt[4]; // selection / residence-time streams
   int32_t cnt;           // vacancies bucketed into the active sector this round
   int32_t done;          // the job finished at or before this block's last round
+  int64_t target;        // asynchronous schedule: round this launch runs the block up to
 };
 
 enum : uint32_t {
@@ -117,6 +119,15 @@ struct RoundArgs {
   unsigned int* status;
   unsigned long long* counters;  // hops, evaluations, rounds, blocks, n_act sum, staged sites, written sites, -
   int64_t hop_cap;
+  // asynchronous round schedule (k_flow)
+  int32_t* lease;               // per block: 0 free, 1 held by a thread or CTA
+  unsigned long long* vclaim;   // per block: slots of vslot taken
+  unsigned long long* vvalid;   // per block: slots of vslot holding a vacancy id
+  int32_t* vslot;               // per block: kFlowSlots ids of the vacancies in its area
+  int32_t* vcount;              // per block: fill counter while the slots are rebuilt
+  int32_t* flow_need;           // per energy kind: blocks with rounds to run in this launch
+  int32_t* flow_done;           // per energy kind: blocks that reached their target
+  int64_t flow_rounds;          // rounds this launch adds to every unfinished block
   // per-hop entry points
   int32_t api_job, api_sector;
   double api_u;
@@ -135,6 +146,9 @@ int launch_api(const RoundArgs& a, size_t smem, void* stream);
 int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, const Potential* pot,
                     const Geometry* geo, unsigned int* status, void* stream);
 int launch_device_math(const double* x, int64_t n, double* e, double* l, void* stream);
+// n rounds of every unfinished block under the asynchronous schedule (no job may have a
+// hop budget); grid = persistent CTAs of the flow kernels.
+int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1);
 // Device address of the fixed round scratch (current device): kNoAllocMaxBlocks * kMaxV
 // block-list slots, then kNoAllocMaxBlocks active-list slots, then the active count.
 int noalloc_scratch(int32_t** base);

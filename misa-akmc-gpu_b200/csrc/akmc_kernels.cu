@@ -93,6 +93,11 @@ struct Smem {
   int32_t ctl_ksel, ctl_bsel, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop, ctl_hop, ctl_n8;
   int32_t ctl_gx, ctl_gy, ctl_gz, ctl_qx, ctl_qy, ctl_qz, ctl_pos;
   uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
+  // asynchronous schedule (k_flow)
+  int8_t flow_lag[8][27];
+  int32_t flow_cand[kThreads];
+  int32_t flow_ncand, flow_stop, flow_progress;
+  int32_t fv[kFlowSlots], fslot[kFlowSlots], fnv;  // the sector's vacancies and their slots
   uint64_t xsn[4];        // selection stream after the uniform drawn ahead
 };
 
@@ -406,8 +411,12 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
 // The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
 // Warps 0..7 evaluate rates (warp b = jump b) and refresh densities; warp 8 keeps the
 // ordered vacancy list, selects, performs the occupancy swap and runs the clock.
+// vlist holds the ids of the cnt_in vacancies inside the sector (any order).  Returns
+// false, uniformly, when the sector's clock is already past its window: nothing ran and
+// the vacancy arrays of sm were not filled.
 template <int KIND>
-__device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s) {
+__device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s,
+                          const int32_t* vlist, int cnt_in) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const bool evaluator = warp < 8;
@@ -418,12 +427,15 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const JobDev& J = a.jobs[B.job];
   const Potential& P = a.pots[J.pot];
   const bool eam = KIND != kPairBond;
-  const int sec = a.mode == kModeRound ? sector_of_round(B.round) : a.api_sector;
+  // the block record, the lattice and the vacancy table are read at L2 (__ldcg): under the
+  // asynchronous schedule another SM may have written them since this SM last looked
+  const int64_t round_now = __ldcg(&B.round);
+  const int sec = a.mode == kModeRound ? sector_of_round(round_now) : a.api_sector;
   double thr = 0.0;
   if (a.mode == kModeRound) {
-    const int64_t step = B.round >> 3;
-    thr = static_cast<double>(step + 1) * J.window - B.evo[sec];
-    if (!(0.0 < thr)) return;  // sector_time stays 0 (sublattice.inl:82)
+    const int64_t step = round_now >> 3;
+    thr = static_cast<double>(step + 1) * J.window - __ldcg(&B.evo[sec]);
+    if (!(0.0 < thr)) return false;  // sector_time stays 0 (sublattice.inl:82)
   }
   JobC jc;
   jc.occ = J.occ;
@@ -480,12 +492,12 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
           const int64_t base = static_cast<int64_t>(jc.sx) * (gy + static_cast<int64_t>(jc.sy) * gz);
           if (has0) {
-            ov[k][0] = jc.occ[base + gx0];
-            if (eam) rv[k][0] = jc.rho[base + gx0];
+            ov[k][0] = __ldcg(jc.occ + base + gx0);
+            if (eam) rv[k][0] = __ldcg(jc.rho + base + gx0);
           }
           if (has1) {
-            ov[k][1] = jc.occ[base + gx1];
-            if (eam) rv[k][1] = jc.rho[base + gx1];
+            ov[k][1] = __ldcg(jc.occ + base + gx1);
+            if (eam) rv[k][1] = __ldcg(jc.rho + base + gx1);
           }
         }
       }
@@ -506,10 +518,10 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
   }
-  const int cnt = min(B.cnt, kMaxV);
+  const int cnt = cnt_in;
   if (tid < cnt) {
-    const int v = a.blk_list[static_cast<int64_t>(gb) * kMaxV + tid];
-    const int s = a.vac_site[v];
+    const int v = vlist[tid];
+    const int s = __ldcg(&a.vac_site[v]);
     const int X = s % jc.sx;
     const int t = s / jc.sx;
     const int y = t % jc.sy;
@@ -539,8 +551,8 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       sm.ord[j] = i;
     }
     for (int i = 0; i < 4; ++i) {
-      sm.xs[i] = B.xs[i];
-      sm.xt[i] = B.xt[i];
+      sm.xs[i] = __ldcg(&B.xs[i]);
+      sm.xt[i] = __ldcg(&B.xt[i]);
     }
     sm.ctl_next_stop = 0;
     sm.ctl_hop = 0;
@@ -559,7 +571,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   __syncthreads();
   AKMC_PHASE(1);
-  if (!sm.ctl_ok) return;
+  if (!sm.ctl_ok) return true;
   if (KIND == kEam64) {  // F(rho) of every staged site, reused by all jumps that touch it
     for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
     __syncthreads();
@@ -598,7 +610,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   //  (S) the control warp forms the ordered total, selects the next hop and performs it
   //      on the occupancy and the vacancy record.
   // Clock and counters live in the control thread's registers.
-  const int64_t hop0 = B.hops;
+  const int64_t hop0 = __ldcg(&B.hops);
   int64_t nh = 0, nact_sum = 0, evals = cnt;
   int nord = cnt, nact_last = 0;
   double sector_time = 0.0, total_last = 0.0;
@@ -668,7 +680,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
             const unsigned long long slot = atomicAdd(a.log_count, 1ull);
             if (slot < static_cast<unsigned long long>(a.log_cap)) {
               akmc_event* e = a.log + slot;
-              e->round = B.round;
+              e->round = round_now;
               e->hop = hop0 + nh - 1;
               e->from_site = sm.ctl_from;
               e->to_site = sm.ctl_to;
@@ -858,16 +870,16 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   __syncthreads();
   AKMC_PHASE(6);
-  if (a.mode == kModeCalc) return;
+  if (a.mode == kModeCalc) return true;
   if (tid == kCtl) {
     if (a.mode == kModeRound) {
-      B.evo[sec] += sector_time;
+      B.evo[sec] = __ldcg(&B.evo[sec]) + sector_time;
       for (int i = 0; i < 4; ++i) {
         B.xs[i] = sm.xs[i];
         B.xt[i] = sm.xt[i];
       }
     }
-    B.hops += nh;
+    B.hops = hop0 + nh;
     if (nh) atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[B.job].hops), static_cast<unsigned long long>(nh));
     atomicAdd(a.counters + 0, static_cast<unsigned long long>(nh));
     atomicAdd(a.counters + 1, static_cast<unsigned long long>(evals));
@@ -878,6 +890,7 @@ __device__ void run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   }
   // the lattice was written through at every hop; only the vacancy positions remain
   if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[tid];
+  return true;
 }
 
 __device__ __forceinline__ void carve(uint8_t* smem, int nreg, Smem*& sm, uint8_t*& occ_s, int32_t*& rho_s) {
@@ -897,9 +910,11 @@ __device__ void dispatch_block(const RoundArgs& a, int gb, uint8_t* smem) {
   uint8_t* occ_s;
   int32_t* rho_s;
   carve(smem, R.n, sm, occ_s, rho_s);
-  if (J.model == AKMC_MODEL_PAIRBOND) run_block<kPairBond>(a, gb, *sm, occ_s, rho_s);
-  else if (J.precision == AKMC_FP32C) run_block<kEam32>(a, gb, *sm, occ_s, rho_s);
-  else run_block<kEam64>(a, gb, *sm, occ_s, rho_s);
+  const int32_t* vl = a.blk_list + static_cast<int64_t>(gb) * kMaxV;
+  const int cnt = min(B.cnt, kMaxV);
+  if (J.model == AKMC_MODEL_PAIRBOND) run_block<kPairBond>(a, gb, *sm, occ_s, rho_s, vl, cnt);
+  else if (J.precision == AKMC_FP32C) run_block<kEam32>(a, gb, *sm, occ_s, rho_s, vl, cnt);
+  else run_block<kEam64>(a, gb, *sm, occ_s, rho_s, vl, cnt);
 }
 
 __global__ void k_bucket(RoundArgs a) {
@@ -967,7 +982,323 @@ __global__ void __launch_bounds__(kThreads, 1) k_hop(RoundArgs a) {
     uint8_t* occ_s;
     int32_t* rho_s;
     carve(smem, R.n, sm, occ_s, rho_s);
-    run_block<KIND>(a, gb, *sm, occ_s, rho_s);
+    run_block<KIND>(a, gb, *sm, occ_s, rho_s, a.blk_list + static_cast<int64_t>(gb) * kMaxV, min(B.cnt, kMaxV));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous round schedule.  A block's round r may run once, for every neighbour
+// offset d in {-1,0,1}^3, the neighbour block has completed its latest earlier round
+// whose staged region (sector plus a 2-cell halo) meets region r (flow_lag); rounds of
+// different blocks then run in any order and the result equals the round-by-round
+// schedule (sublattice.inl:61-179): a round reads and writes only its region, every
+// write that a region can see comes from an earlier round that it waits for, and rounds
+// that run at the same time have disjoint regions.  Each block keeps the ids of the
+// vacancies in its area in kFlowSlots slots; a hop that carries a vacancy into a
+// neighbour's area moves the id there.
+//
+// k_flow is persistent.  Each sweep a thread takes one block: while the block's next
+// round is ready and its sector holds no vacancy, the thread runs that round alone (the
+// clock jumps to the window, sublattice.inl:108-112); a ready round with vacancies is
+// handed to the CTA, which runs the hop loop for it.  A block is held with a lease (an
+// atomic flag) while anything works on it, and nothing waits while holding a lease.
+
+__device__ __forceinline__ int64_t ld_acquire64(const int64_t* p) {
+  int64_t v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int64_t ld_relaxed64(const int64_t* p) {
+  int64_t v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release64(int64_t* p, int64_t v) {
+  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Rounds back to the latest earlier round of the neighbour at offset (dx, dy, dz) whose
+// region meets this round's (phase = round mod 8), 0 if none ever does.  Per dimension a
+// +1 neighbour's regions meet ours only between our high half and its low half (block
+// edges >= 8 cells, halos of 2), a -1 neighbour's only between our low half and its high.
+__device__ int flow_lag(int phase, int dx, int dy, int dz) {
+  const int now = sector_of_round(phase);
+  const int d[3] = {dx, dy, dz};
+  for (int k = 1; k <= 8; ++k) {
+    const int then = sector_of_round(phase + 8 - k);
+    bool meet = true;
+    for (int a = 0; a < 3; ++a) {
+      const int hn = (now >> a) & 1, ht = (then >> a) & 1;
+      if (d[a] == 1) meet = meet && hn == 1 && ht == 0;
+      if (d[a] == -1) meet = meet && hn == 0 && ht == 1;
+    }
+    if (meet) return k;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ int wrapb(int v, int m) { return v < 0 ? v + m : (v >= m ? v - m : v); }
+
+// Global index of the neighbour of block local_id at offset o (o = (dz+1)*9 + (dy+1)*3 + dx+1).
+__device__ __forceinline__ int flow_neighbour(const JobDev& J, int local_id, int o) {
+  const int bx = local_id % J.nb[0], by = (local_id / J.nb[0]) % J.nb[1], bz = local_id / (J.nb[0] * J.nb[1]);
+  return J.block0 + wrapb(bx + o % 3 - 1, J.nb[0]) +
+         J.nb[0] * (wrapb(by + (o / 3) % 3 - 1, J.nb[1]) + J.nb[1] * wrapb(bz + o / 9 - 1, J.nb[2]));
+}
+
+// Whether round r of the block may run.  The neighbours' round counters are read with
+// relaxed loads, all in flight at once, and a fence follows a positive answer (the acquire
+// pattern): the writes of the rounds waited for become visible to this thread.
+__device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, int64_t r, const int8_t (*lag)[27]) {
+  const int ph = static_cast<int>(r & 7);
+  bool ok = true;
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    const int k = lag[ph][o];
+    if (k) ok &= ld_relaxed64(&a.blocks[flow_neighbour(J, local_id, o)].round) >= r - k + 1;
+  }
+  if (ok) __threadfence();
+  return ok;
+}
+
+__device__ __forceinline__ bool site_in_sector(const BlockDev& B, const JobDev& J, int sec, int32_t s) {
+  const int X = s % J.sx;
+  const int t = s / J.sx;
+  const int c[3] = {X >> 1, t % J.sy, t / J.sy};
+  for (int d = 0; d < 3; ++d) {
+    const int half = (B.c1[d] - B.c0[d]) / 2;
+    const int lo = (sec >> d) & 1 ? B.c0[d] + half : B.c0[d];
+    const int hi = (sec >> d) & 1 ? B.c1[d] : B.c0[d] + half;
+    if (c[d] < lo || c[d] >= hi) return false;
+  }
+  return true;
+}
+
+// Global block whose area holds site s (the reference's rank split, as k_bucket).
+__device__ __forceinline__ int owner_block(const JobDev& J, int32_t s) {
+  const int X = s % J.sx;
+  const int t = s / J.sx;
+  const int c[3] = {X >> 1, t % J.sy, t / J.sy};
+  int k[3];
+  for (int d = 0; d < 3; ++d) k[d] = block_of(c[d], J.n[d], J.nb[d]);
+  return J.block0 + k[0] + J.nb[0] * (k[1] + J.nb[1] * k[2]);
+}
+
+__device__ bool flow_sector_has_vacancy(const RoundArgs& a, const BlockDev& B, const JobDev& J, int gb, int sec) {
+  unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
+  while (m) {
+    const int slot = __ffsll(static_cast<long long>(m)) - 1;
+    m &= m - 1;
+    const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + slot]);
+    if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) return true;
+  }
+  return false;
+}
+
+// Puts vacancy v into block o's slots: claim a free slot, write the id, then mark it valid.
+__device__ void flow_give(const RoundArgs& a, int o, int v) {
+  for (int tries = 0; tries < 4 * kFlowSlots; ++tries) {
+    const unsigned long long m = *reinterpret_cast<volatile unsigned long long*>(&a.vclaim[o]);
+    if (m == ~0ull) break;
+    const int slot = __ffsll(static_cast<long long>(~m)) - 1;
+    const unsigned long long bit = 1ull << slot;
+    if (atomicOr(&a.vclaim[o], bit) & bit) continue;  // taken meanwhile
+    a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
+    __threadfence();
+    atomicOr(&a.vvalid[o], bit);
+    return;
+  }
+  atomicOr(a.status, kErrVacOverflow);
+}
+
+// Publishes round r of block B as complete (after every write of the round).
+__device__ __forceinline__ void flow_publish(const RoundArgs& a, BlockDev& B, int64_t r, int kind) {
+  __threadfence();
+  st_release64(&B.round, r + 1);
+  if (r + 1 == B.target) atomicAdd(&a.flow_done[kind], 1);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  Smem* sm0 = reinterpret_cast<Smem*>(smem);
+  const int tid = threadIdx.x;
+  init_cta_smem(smem);
+  for (int i = tid; i < 8 * 27; i += kThreads) {
+    const int o = i % 27;
+    sm0->flow_lag[i / 27][o] = static_cast<int8_t>(flow_lag(i / 27, o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1));
+  }
+  const int nb = a.nblocks;
+  int cursor = static_cast<int>((static_cast<int64_t>(blockIdx.x) * nb) / gridDim.x);
+  for (int64_t sweep = 0;; ++sweep) {
+    if (tid == 0) {
+      sm0->flow_ncand = 0;
+      sm0->flow_progress = 0;
+      const int need = *reinterpret_cast<volatile int*>(&a.flow_need[KIND]);
+      const int done = *reinterpret_cast<volatile int*>(&a.flow_done[KIND]);
+      const unsigned st = *reinterpret_cast<volatile unsigned*>(a.status);
+      int stop = done >= need || (st & (kErrVacOverflow | kErrRhoRange | kErrHopCap | kErrTimeout)) != 0;
+      if (!stop && sweep >= (1ll << 24)) {  // bounded: no launch of <= 1024 rounds needs this many
+        atomicOr(a.status, kErrTimeout);
+        stop = 1;
+      }
+      sm0->flow_stop = stop;
+    }
+    __syncthreads();
+    if (sm0->flow_stop) break;
+
+    // sweep: thread tid looks after block (cursor + tid) mod nb
+    if (tid < nb) {
+      int gb = cursor + tid;
+      if (gb >= nb) gb -= nb;
+      BlockDev& B = a.blocks[gb];
+      const JobDev& J = a.jobs[B.job];
+      int64_t r = ld_relaxed64(&B.round);
+      if (job_kind(J) == KIND && r < B.target && *reinterpret_cast<volatile int*>(&a.lease[gb]) == 0 &&
+          flow_ready(a, J, B.local_id, r, sm0->flow_lag) && atomicCAS(&a.lease[gb], 0, 1) == 0) {
+        __threadfence();
+        bool keep = false;
+        for (int n = 0; n < 64; ++n) {
+          r = ld_acquire64(&B.round);
+          if (r >= B.target || !flow_ready(a, J, B.local_id, r, sm0->flow_lag)) break;
+          const int sec = sector_of_round(r);
+          if (flow_sector_has_vacancy(a, B, J, gb, sec)) {  // the CTA runs this one
+            sm0->flow_cand[atomicAdd(&sm0->flow_ncand, 1)] = gb;
+            keep = true;
+            break;
+          }
+          // no vacancy in the sector: total = 0, the clock jumps to the window
+          const int64_t step = r >> 3;
+          const double evo = __ldcg(&B.evo[sec]);
+          const double thr = static_cast<double>(step + 1) * J.window - evo;
+          double sector_time = 0.0;
+          if (sector_time < thr) sector_time = thr;
+          B.evo[sec] = evo + sector_time;
+          flow_publish(a, B, r, KIND);
+          sm0->flow_progress = 1;
+        }
+        if (!keep) {
+          __threadfence();
+          atomicExch(&a.lease[gb], 0);
+        }
+      }
+    }
+    __syncthreads();
+
+    // the hop loop for each round handed over
+    const int ncand = sm0->flow_ncand;
+    for (int c = 0; c < ncand; ++c) {
+      const int gb = sm0->flow_cand[c];
+      BlockDev& B = a.blocks[gb];
+      const JobDev& J = a.jobs[B.job];
+      const int64_t r = ld_acquire64(&B.round);
+      // every thread acquires the rounds this one waits for, not only the sweeping thread
+      if (tid < 27 && sm0->flow_lag[r & 7][tid]) (void)ld_acquire64(&a.blocks[flow_neighbour(J, B.local_id, tid)].round);
+      __threadfence();
+      const int sec = sector_of_round(r);
+      Region R;
+      make_region(B, sec, R);
+      Smem* sm;
+      uint8_t* occ_s;
+      int32_t* rho_s;
+      carve(smem, R.n, sm, occ_s, rho_s);
+      if (tid == 0) sm->fnv = 0;
+      __syncthreads();
+      if (tid < kFlowSlots) {
+        const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
+        if ((m >> tid) & 1ull) {
+          const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + tid]);
+          if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) {
+            const int i = atomicAdd(&sm->fnv, 1);
+            sm->fv[i] = v;
+            sm->fslot[i] = tid;
+          }
+        }
+      }
+      __syncthreads();
+      const int cnt = sm->fnv;
+      const bool ran = run_block<KIND>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt);
+      __syncthreads();
+      // vacancies carried into a neighbour's area change owner (only if the round ran:
+      // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
+      if (ran && tid < cnt) {
+        const int o = owner_block(J, sm->vlid[tid]);
+        if (o != gb) {
+          flow_give(a, o, sm->vidx[tid]);
+          const unsigned long long bit = 1ull << sm->fslot[tid];
+          atomicAnd(&a.vvalid[gb], ~bit);
+          __threadfence();
+          atomicAnd(&a.vclaim[gb], ~bit);
+        }
+      }
+      __threadfence();  // every thread's lattice, record and slot writes before the round is published
+      __syncthreads();
+      if (tid == 0) {
+        flow_publish(a, B, r, KIND);
+        __threadfence();
+        atomicExch(&a.lease[gb], 0);
+        sm->flow_progress = 1;
+      }
+      __syncthreads();
+    }
+    if (!sm0->flow_progress) __nanosleep(256);
+    cursor += kThreads;
+    if (cursor >= nb) cursor %= nb;
+  }
+}
+
+// Per block: target round of this launch, lease and slots cleared; counts the blocks with
+// rounds to run per energy kind.
+__global__ void k_flow_prep(RoundArgs a) {
+  const int gb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gb >= a.nblocks) return;
+  BlockDev& B = a.blocks[gb];
+  const JobDev& J = a.jobs[B.job];
+  int64_t t = B.done ? B.round : B.round + a.flow_rounds;
+  if (J.max_rounds > 0 && t > J.max_rounds) t = J.max_rounds > B.round ? J.max_rounds : B.round;
+  B.target = t;
+  B.cnt = 0;
+  a.lease[gb] = 0;
+  a.vclaim[gb] = 0;
+  a.vvalid[gb] = 0;
+  a.vcount[gb] = 0;
+  if (t > B.round) atomicAdd(&a.flow_need[job_kind(J)], 1);
+}
+
+// Per vacancy: into the slots of the block whose area holds it.
+__global__ void k_flow_slots(RoundArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.nvac) return;
+  const JobDev& J = a.jobs[a.vac_job[v]];
+  const int o = owner_block(J, a.vac_site[v]);
+  const int slot = atomicAdd(&a.vcount[o], 1);
+  if (slot >= kFlowSlots) {
+    atomicOr(a.status, kErrVacOverflow);
+    return;
+  }
+  a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
+  atomicOr(&a.vclaim[o], 1ull << slot);
+  atomicOr(&a.vvalid[o], 1ull << slot);
+}
+
+// After the flow kernels: job round and done flags as k_finalize leaves them.
+__global__ void k_flow_finalize(RoundArgs a) {
+  const int gb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gb == 0) atomicAdd(a.counters + 2, static_cast<unsigned long long>(a.flow_rounds));
+  if (gb >= a.nblocks) return;
+  BlockDev& B = a.blocks[gb];
+  JobDev& J = a.jobs[B.job];
+  B.cnt = 0;
+  const int done = J.max_rounds > 0 && B.round >= J.max_rounds;
+  B.done = done;
+  if (B.local_id == 0) {
+    J.round = B.round;
+    J.done = done;
   }
 }
 
@@ -1094,6 +1425,21 @@ int launch_api(const RoundArgs& a, size_t smem, void* stream) {
   return static_cast<int>(cudaGetLastError());
 }
 
+int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(a.flow_need, 0, 3 * sizeof(int32_t), st);
+  cudaMemsetAsync(a.flow_done, 0, 3 * sizeof(int32_t), st);
+  k_flow_prep<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
+  if (a.nvac > 0) k_flow_slots<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
+  if (ev0) cudaEventRecord(static_cast<cudaEvent_t>(ev0), st);
+  if (a.kind_mask & (1 << kEam64)) k_flow<kEam64><<<grid, kThreads, smem, st>>>(a);
+  if (a.kind_mask & (1 << kEam32)) k_flow<kEam32><<<grid, kThreads, smem, st>>>(a);
+  if (a.kind_mask & (1 << kPairBond)) k_flow<kPairBond><<<grid, kThreads, smem, st>>>(a);
+  if (ev1) cudaEventRecord(static_cast<cudaEvent_t>(ev1), st);
+  k_flow_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
+  return static_cast<int>(cudaGetLastError());
+}
+
 int configure_hop_smem(size_t smem) {
   cudaError_t e = cudaFuncSetAttribute(k_hop<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -1101,6 +1447,12 @@ int configure_hop_smem(size_t smem) {
     e = cudaFuncSetAttribute(k_hop<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_hop<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_flow<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_flow<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_flow<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
   e = cudaFuncSetAttribute(k_api_block, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   return static_cast<int>(e);

@@ -20,6 +20,7 @@ RNG_XOSHIRO = 0
 V, FE, CU, NI, MN = 0, 1, 2, 4, 8
 MAX_SECTOR_VACANCIES = 64
 NOALLOC_MAX_BLOCKS = 8192
+SCHEDULE_AUTO, SCHEDULE_ROUNDS, SCHEDULE_FLOW = 0, 1, 2
 SECTOR_ORDER = (0, 7, 2, 5, 3, 4, 1, 6)
 
 STATUS = {
@@ -178,6 +179,7 @@ SIGNATURES = {
     "akmc_prepare": (C.c_int, [_vp]),
     "akmc_run_rounds": (C.c_int, [_vp, _i64]),
     "akmc_run_rounds_noalloc": (C.c_int, [_vp, _i64]),
+    "akmc_set_round_schedule": (C.c_int, [_vp, _i32]),
     "akmc_run": (C.c_int, [_vp, _i64]),
     "akmc_sync": (C.c_int, [_vp]),
     "akmc_stream": (_vp, [_vp]),
@@ -382,6 +384,10 @@ class Engine:
         """akmc_run_rounds without allocation: round scratch in a fixed device array
         (at most NOALLOC_MAX_BLOCKS domain blocks; calls on one device must not overlap)."""
         self._ck(lib().akmc_run_rounds_noalloc(self.h, n))
+
+    def set_round_schedule(self, schedule):
+        """SCHEDULE_AUTO, SCHEDULE_ROUNDS (round by round) or SCHEDULE_FLOW (dependency-driven)."""
+        self._ck(lib().akmc_set_round_schedule(self.h, schedule))
 
     def run(self, max_rounds=0):
         self._ck(lib().akmc_run(self.h, max_rounds))

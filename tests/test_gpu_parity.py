@@ -30,9 +30,10 @@ def ak():
     return akmc_b200
 
 
-def run_pair(ak, rounds, jobs):
+def run_pair(ak, rounds, jobs, schedule=0):
     """jobs: list of dicts of oracle_job/device_job kwargs; returns (engine, oracles)."""
     eng = ak.Engine(event_log_capacity=1 << 21)
+    eng.set_round_schedule(schedule)
     oracles = []
     for kw in jobs:
         o = oracle_job(**kw)
@@ -84,10 +85,11 @@ def test_single_domain_20_cubed(ak, model, prec):
     eng.close()
 
 
-def test_domain_blocks_quaternary(ak):
+@pytest.mark.parametrize("schedule", [1, 2])  # round by round; dependency-driven
+def test_domain_blocks_quaternary(ak, schedule):
     kw = dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=60,
               temperature=563.0, seed=7)
-    eng, (o,) = run_pair(ak, 160, [kw])
+    eng, (o,) = run_pair(ak, 160, [kw], schedule)
     assert o.hops > 500
     check_job(eng, o, 0, eng.events())
     assert np.array_equal(eng.rho(0), o.rho())
@@ -247,3 +249,16 @@ def test_load_occupancy_restarts_the_trajectory(ak):
         bad[np.nonzero(bad == 0)[0][0]] = 1  # one vacancy fewer than the job holds
         with pytest.raises(ak.AkmcError):
             eng.load_occupancy(0, bad)
+
+
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_many_blocks_both_schedules(ak, schedule):
+    # 5 x 5 x 5 blocks of 8 cells: under the dependency-driven schedule blocks run
+    # rounds apart; both schedules must give the oracle's trajectory
+    kw = dict(box=(40, 40, 40), blocks=(5, 5, 5), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=150,
+              temperature=563.0, seed=5)
+    eng, (o,) = run_pair(ak, 96, [kw], schedule)
+    assert o.hops > 1000
+    check_job(eng, o, 0, eng.events())
+    assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
