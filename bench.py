@@ -11,6 +11,7 @@ read back every step.  N > 1 runs independent replicas (one per GPU, seed 42 +
 rank): the path has no exchange step between jobs.
 """
 import argparse
+import datetime
 import json
 import math
 import os
@@ -93,6 +94,71 @@ def workload_jobs(name, rank=0):
     raise SystemExit("unknown workload %s" % name)
 
 
+def serve_jobs(rate, seconds, rank=0):
+    """Job stream of the serving workload: Poisson arrivals at `rate` per second for `seconds`,
+    box edge log-uniform in [16, 96] cells, hop budget log-uniform in [1e4, 1e6], the batched
+    workload's composition ranges, vacancy fraction 1e-4, seed 42 + job index."""
+    draw = _xoshiro(42 + rank, 11)
+    t, out, i = 0.0, [], 0
+    while True:
+        t += -math.log(1.0 - draw()) / rate
+        if t >= seconds:
+            return out
+        edge = int(round(math.exp(math.log(16) + (math.log(96) - math.log(16)) * draw())))
+        budget = int(round(math.exp(math.log(1e4) + (math.log(1e6) - math.log(1e4)) * draw())))
+        cu = 50 + int(round(100 * draw()))
+        ni = int(round(100 * draw()))
+        mn = int(round(50 * draw()))
+        nb = -(-edge // 24)  # blocks of at most 24 cells: the staged sector region fits in shared memory
+        out.append(dict(t=t, box=(edge, edge, edge), blocks=(nb, nb, nb),
+                        alloy=((FE, 10000 - cu - ni - mn), (CU, cu), (NI, ni), (MN, mn)),
+                        n_vacancies=max(2, int(round(1e-4 * 2 * edge ** 3))), temperature=473.0 + 200.0 * draw(),
+                        precision=1, seed=42 + i + 100000 * rank, hop_budget=budget))
+        i += 1
+
+
+def run_serve(args, ak, device):
+    """Serving workload through akmc_server: arrivals replayed in real time, every job waited
+    for; latency = result published - submitted."""
+    jobs = serve_jobs(args.serve_rate, args.serve_seconds)
+    eam = ak.eam_johnson(42)
+    prepared = []
+    for j in jobs:
+        occ = ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"])
+        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=j["precision"],
+                            temperature=j["temperature"], seed=j["seed"], eam=eam, hop_budget=j["hop_budget"])
+        prepared.append((j["t"], cfg, occ))
+    srv = ak.Server(device=device, lanes=args.serve_lanes)
+    t0 = time.perf_counter()
+    tickets = []
+    for t, cfg, occ in prepared:
+        while time.perf_counter() - t0 < t:
+            time.sleep(0.0005)
+        tickets.append(srv.submit(cfg, occ))
+    lat, hops = [], 0
+    for tk in tickets:
+        res, _ = srv.wait(tk, timeout=3600.0)
+        if res["status"] != 0:
+            raise SystemExit("serving job failed with status %d: %s" % (res["status"], res["error"]))
+        lat.append(res["finish_s"] - res["submit_s"])
+        hops += res["hops"]
+    wall = time.perf_counter() - t0
+    srv.close()
+    lat = np.array(lat)
+    line = {
+        "metric": METRIC, "value": hops / wall, "unit": "hops/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+        "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals %.0f/s for %.0f s, edge log-uniform 16-96 cells, hop "
+                               "budget log-uniform 1e4-1e6, EAM FP32-compensated" % (args.serve_rate, args.serve_seconds),
+                   "jobs": len(jobs), "lanes": args.serve_lanes,
+                   "offered_hops_per_s": sum(j["hop_budget"] for j in jobs) / args.serve_seconds},
+        "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+        "latency_max_s": float(lat.max()), "wall_s": wall,
+    }
+    print(json.dumps(line))
+
+
 def algorithmic_bytes(hops, evals, nact_sum, eam=True):
     """Canonical bytes of the path: per vacancy evaluation the 145-site footprint
     (occupancy byte + int32 density) and 8 FP64 rates; per hop the 78-site density
@@ -105,15 +171,18 @@ def algorithmic_bytes(hops, evals, nact_sum, eam=True):
 
 # ---------------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples (every 200 ms) around the timed region.  The sampler starts before
+    the warm-up, so short timed regions still get samples; samples taken between mark_start
+    and mark_stop (plus 250 ms either side) are kept, else the two nearest."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.p = None
+        self.t0 = self.t1 = None
         self.path = os.path.join("/tmp", "akmc_clocks_%d_%d.csv" % (os.getpid(), device))
 
     def start(self):
@@ -125,32 +194,46 @@ class Clocks:
         except Exception:
             self.p = None
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_stop(self):
+        self.t1 = time.time()
+
     def stop(self):
         if self.p is None:
             return None
+        time.sleep(0.3)  # one more sample after the timed region
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
         self.f.close()
-        sm, mx, reasons = [], None, set()
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+        if not rows:
+            return None
+        t0, t1 = (self.t0 or rows[0][0]), (self.t1 or rows[-1][0])
+        sel = [r for r in rows if t0 - 0.25 <= r[0] <= t1 + 0.25]
+        if not sel:
+            sel = sorted(rows, key=lambda r: min(abs(r[0] - t0), abs(r[0] - t1)))[:2]
+        reasons = set()
+        for r in sel:
+            for n, v in zip(names, r[3]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median([r[1] for r in sel]), "sm_max_mhz": sel[-1][2],
+                "reasons": sorted(reasons), "samples": len(sel)}
 
 
 def peaks():
@@ -161,11 +244,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(workload):
-    """DRAM bytes per hop-kernel launch from the committed ncu summary, if any."""
+def traffic_per_launch(workload, schedule, rounds):
+    """DRAM bytes per hop-kernel launch from the committed ncu summary, if any: per launch
+    of one round (round by round) or per round of a flow launch, scaled to its rounds."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "k_hop_traffic.json")))
-        return d.get(workload)
+        v = d.get(schedule, {}).get(workload)
+        if v is None:
+            return None
+        return v * rounds if schedule == "flow" else v
     except Exception:
         return None
 
@@ -263,7 +350,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="scale", choices=["scale", "scale32", "batched", "serial"])
+    ap.add_argument("--workload", default="scale", choices=["scale", "scale32", "batched", "serial", "serve"])
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--rounds-per-step", type=int, default=256)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -272,6 +362,16 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "serve":
+        if rank == 0 and args.impl != "reference":
+            import build as akbuild
+            import akmc_b200 as ak
+
+            akbuild.build()
+            run_serve(args, ak, local)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the serving workload has no CPU reference arm"}))
+        return
     jobs = workload_jobs(args.workload, rank)
 
     if args.impl == "reference":
@@ -307,23 +407,25 @@ def main():
         if dist:
             dist.barrier()
 
+    clocks = Clocks(local)
+    clocks.start()
     # warm-up
     for _ in range(args.warmup):
         eng.run_rounds(R)
     eng.sync()
     sync_all()
     c0 = eng.counters()
-    clocks = Clocks(local)
-    clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     sync_all()
+    clocks.mark_start()
     ev0.record(stream)
     for _ in range(args.steps):
         eng.run_rounds(R)
     ev1.record(stream)
     eng.sync()
     sync_all()
+    clocks.mark_stop()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     c1 = eng.counters()
@@ -336,6 +438,13 @@ def main():
         t = tmax
     ms_all, hops_all = float(t[0]), float(t[1])
     value = hops_all / (ms_all / 1e3)
+
+    # kernels launched per timed step: round by round, k_bucket + k_hop + k_finalize per round
+    # (captured in CUDA graphs); dependency-driven, per launch of up to 1024 rounds k_flow_prep,
+    # k_flow_slots, k_flow and k_flow_finalize (plus two memsets)
+    sched = eng.round_schedule()
+    sched_name = "flow" if sched == ak.SCHEDULE_FLOW else "rounds"
+    launches_per_step = 4 * ((R + 1023) // 1024) if sched == ak.SCHEDULE_FLOW else 3 * R
 
     # roofline pass: same workload continued, hop kernel timed with events around every launch
     eng.set_kernel_timing(True)
@@ -350,9 +459,9 @@ def main():
     bytes_alg = algorithmic_bytes(rh, r1["evaluations"] - r0["evaluations"], r1["n_act_sum"] - r0["n_act_sum"], eam)
     peak, peak_kind = peaks()
     achieved = bytes_alg / (hop_ms / 1e3) / 1e9 if hop_ms > 0 else 0.0
-    traffic = traffic_per_launch(args.workload)
+    traffic = traffic_per_launch(args.workload, sched_name, R)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_hop",
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_flow" if sched_name == "flow" else "k_hop",
                 "bytes_per_launch": bytes_alg / max(1, launches), "avg_launch_us": 1e3 * hop_ms / max(1, launches),
                 "hops_per_launch": rh / max(1, launches),
                 "e_hop": (r1["evaluations"] - r0["evaluations"]) / max(1, rh),
@@ -391,7 +500,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if jobs[0]["precision"] == 0 else "f32c", "data": "synthetic",
             "config": config_of(args, jobs), "roofline": roofline, "e2e": e2e,
-            "gpu_launches": 3 * R * args.steps, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps, "schedule": sched_name, "clocks": clk,
             "hops_timed": int(hops_all),
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -171,6 +171,8 @@ AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
  * has a hop budget and every block area starts with at most 32 vacancies, else ROUNDS.  akmc_run_rounds_noalloc always runs ROUNDS. */
 enum { AKMC_SCHEDULE_AUTO = 0, AKMC_SCHEDULE_ROUNDS = 1, AKMC_SCHEDULE_FLOW = 2 };
 AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule);
+/* The schedule akmc_run_rounds uses (ROUNDS or FLOW), AUTO resolved; after akmc_prepare. */
+AKMC_API akmc_status akmc_get_round_schedule(akmc_ctx* ctx, int32_t* effective);
 /* Runs until every job is done (hop budget or max_rounds) or max_rounds pass. */
 AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds);
 AKMC_API akmc_status akmc_sync(akmc_ctx* ctx);
@@ -218,6 +220,14 @@ AKMC_API akmc_status akmc_get_kernel_timing(akmc_ctx* ctx, double* hop_kernel_ms
 /* calculate_GPU / first_calculate_GPU (gpu_simulate.h:33-35, gpu_simulate.hip:1211-1716):
  * rates of every vacancy in sector sector_id; returns their ordered sum. */
 AKMC_API akmc_status akmc_calculate(akmc_ctx* ctx, int32_t job, int32_t sector_id, double* total);
+/* The jumps behind the last akmc_calculate, as the device vacancy records hold
+ * them (d_vacancy_adv[].rates, gpu_simulate.hip:476-480): for each of the n_out
+ * vacancies of the sector, in list order, its site (-1 if it has left the
+ * sector), the 8 jumps' ΔE in eV (0 for a jump onto a vacancy) and rates in Hz
+ * (0 likewise).  delta_e and rates hold 8 * capacity values.  AKMC_EINVAL with
+ * n_out set when capacity is too small; n_out = 0 before any akmc_calculate. */
+AKMC_API akmc_status akmc_get_calculated_rates(akmc_ctx* ctx, int32_t* sites, double* delta_e, double* rates,
+                                               int64_t capacity, int64_t* n_out);
 /* selectAndPerformEventGPU (gpu_simulate.h:37-41, gpu_simulate.hip:1388-1449):
  * selects the first event whose cumulative rate exceeds u * total in z-y-x
  * order and performs it.  ev->from_site < 0 when no event is selected. */
@@ -232,9 +242,16 @@ AKMC_API akmc_status akmc_eam_johnson(uint64_t seed, double lattice_const, doubl
  * xoshiro256** streams: one draw per site in site-id order, then vacancies. */
 AKMC_API akmc_status akmc_create_lattice(const int64_t box[3], const int32_t type_codes[4], const int64_t ratio[4],
                                          int64_t n_vacancies, uint64_t seed, uint8_t* occ, int64_t n_sites);
-/* Isolated-Cu count (profiles/m_event_hook.cpp:17-55) and Cu cluster-size histogram (1nn). */
+/* Isolated-Cu count (profiles/m_event_hook.cpp:17-55) and Cu cluster-size histogram (1nn):
+ * hist[k] = clusters of k atoms, the last bin holding all larger ones.  Host code. */
 AKMC_API akmc_status akmc_cluster_stats(const uint8_t* occ, const int64_t box[3], int64_t* isolated_cu, int64_t* hist,
                                         int64_t hist_len);
+/* The same statistics of a job's resident lattice, computed on the device (the reference
+ * computes them on the host from its hash sets, m_event_hook.cpp:17-55).  hist_len <=
+ * AKMC_CLUSTER_MAX_BINS.  The first call for a job size allocates 12 bytes per site. */
+#define AKMC_CLUSTER_MAX_BINS 4096
+AKMC_API akmc_status akmc_job_cluster_stats(akmc_ctx* ctx, int32_t job, int64_t* isolated_cu, int64_t* hist,
+                                            int64_t hist_len);
 
 /*
  * config.yaml of the reference (profiles/config/config_parsing.cpp:54-230, keys of
@@ -281,6 +298,52 @@ AKMC_API akmc_status akmc_dump_lattice(const uint8_t* occ, const int64_t box[3],
 
 /* Device checks of the shared arithmetic: port_exp/port_log of x[i] on the GPU. */
 AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out);
+
+/*
+ * Job server: many independent jobs (parameter sweeps, ensembles, requests) on one GPU.
+ * Submitted jobs queue; worker lanes (one host thread and one CUDA stream each) take the
+ * queued jobs in arrival order as a batch that fits the memory budget, run them together
+ * in one context (akmc_add_job per job, then akmc_run_rounds in chunks), and publish each
+ * job's result as soon as that job is done.  The server is internally synchronised: any
+ * host thread may submit and poll.  This replaces running one MPI job per box.
+ */
+typedef struct akmc_server akmc_server;
+typedef struct akmc_server_config {
+  int32_t device;           /* CUDA device ordinal */
+  int32_t lanes;            /* concurrent batches (0: 2) */
+  int64_t budget_bytes;     /* device memory the jobs of all running batches may hold (0: 8 GiB) */
+  int32_t max_batch_jobs;   /* jobs per batch (0: 512) */
+  int32_t chunk_rounds;     /* rounds between checks for finished jobs (0: 16) */
+} akmc_server_config;
+typedef struct akmc_job_result {
+  int64_t hops;
+  int64_t rounds;
+  double submit_s;          /* server clock (seconds since akmc_server_create) */
+  double start_s;           /* its batch started */
+  double finish_s;          /* the result was published */
+  int32_t status;           /* akmc_status of the job */
+  int32_t n_blocks;
+  char error[128];          /* akmc_last_error of its batch when status != AKMC_OK */
+} akmc_job_result;
+AKMC_API akmc_status akmc_server_create(const akmc_server_config* cfg, akmc_server** out);
+/* Queues a job (cfg, its EAM tables and occ are copied).  The job must end by itself: a hop
+ * budget or max_rounds.  EINVAL for a job no batch could run (bad config, or more device
+ * memory than the whole budget). */
+AKMC_API akmc_status akmc_server_submit(akmc_server* s, const akmc_job_config* cfg, const uint8_t* occ,
+                                        int64_t n_sites, int64_t* ticket);
+/* ready = 1 once the job is done: res is filled and, when occ_out is not NULL, the final
+ * lattice copied (n_sites bytes); the job's record is then released.  ready = 0 while it
+ * queues or runs.  ENOTFOUND for an unknown or already collected ticket. */
+AKMC_API akmc_status akmc_server_poll(akmc_server* s, int64_t ticket, akmc_job_result* res, uint8_t* occ_out,
+                                      int64_t n_sites, int32_t* ready);
+/* akmc_server_poll that blocks up to timeout_s seconds (ETIMEOUT if the job is not done). */
+AKMC_API akmc_status akmc_server_wait(akmc_server* s, int64_t ticket, double timeout_s, akmc_job_result* res,
+                                      uint8_t* occ_out, int64_t n_sites);
+/* Jobs queued or running, and jobs done but not collected. */
+AKMC_API akmc_status akmc_server_stats(akmc_server* s, int64_t* queued, int64_t* running, int64_t* done);
+/* Finishes the running batches, fails the queued jobs (status AKMC_ESTATE) and frees the
+ * server. */
+AKMC_API akmc_status akmc_server_shutdown(akmc_server* s);
 
 #ifdef __cplusplus
 }

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libakmc_b200.so")
-SOURCES = ["akmc_kernels.cu", "akmc_api.cu", "akmc_model.cpp", "akmc_host.cpp", "akmc_server.cpp"]
+SOURCES = ["akmc_kernels.cu", "akmc_cluster.cu", "akmc_api.cu", "akmc_model.cpp", "akmc_host.cpp", "akmc_server.cpp"]
 HEADERS = ["akmc_common.cuh", "akmc_device.h", "akmc_model.h", "akmc_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

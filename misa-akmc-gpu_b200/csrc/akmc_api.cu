@@ -71,6 +71,10 @@ struct akmc_ctx {
   unsigned long long* d_counters = nullptr;
   double* d_api_total = nullptr;
   akmc_event* d_api_event = nullptr;
+  double* d_api_de = nullptr;
+  double* d_api_rates = nullptr;
+  int32_t* d_api_sites = nullptr;
+  int32_t* d_api_count = nullptr;
   size_t smem = 0;
   int hop_grid = 0;
   RoundArgs args{};
@@ -88,6 +92,11 @@ struct akmc_ctx {
   int32_t* d_vslot = nullptr;
   int32_t* d_vcount = nullptr;
   int32_t* d_flow = nullptr;  // flow_need[3], flow_done[3]
+  // cluster statistics scratch: list, parent, size (one int32 per site of the largest job
+  // measured so far), then n_list, the isolated count and the histogram
+  int32_t* d_cl = nullptr;
+  int64_t cl_sites = 0;
+  unsigned long long* d_cl_misc = nullptr;
   // kernel timing mode: rounds launched one by one with events around the hop kernel
   bool timing = false;
   std::vector<cudaEvent_t> ev;
@@ -126,6 +135,7 @@ akmc_status check_status(akmc_ctx* ctx) {
   if (st & kErrRhoRange) return fail(ctx, AKMC_ERANGE, "a density left the F table");
   if (st & kErrHopCap) return fail(ctx, AKMC_ERANGE, "a block exceeded the hop cap of one round");
   if (st & kErrLogOverflow) return fail(ctx, AKMC_EOVERFLOW, "event log full");
+  if (st & kErrTimeout) return fail(ctx, AKMC_ETIMEOUT, "a bounded device wait or loop gave up");
   return fail(ctx, AKMC_ESTATE, "device reported status " + std::to_string(st));
 }
 
@@ -139,6 +149,11 @@ void free_device(akmc_ctx* ctx) {
   ctx->d_lease = nullptr;
   ctx->d_vclaim = ctx->d_vvalid = nullptr;
   ctx->d_vslot = ctx->d_vcount = ctx->d_flow = nullptr;
+  cudaFree(ctx->d_cl);
+  cudaFree(ctx->d_cl_misc);
+  ctx->d_cl = nullptr;
+  ctx->d_cl_misc = nullptr;
+  ctx->cl_sites = 0;
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->graph_def) cudaGraphDestroy(ctx->graph_def);
   ctx->graph = nullptr;
@@ -157,7 +172,8 @@ void free_device(akmc_ctx* ctx) {
   }
   void* ptrs[] = {ctx->d_jobs, ctx->d_blocks, ctx->d_vac_site, ctx->d_vac_job, ctx->d_blk_list, ctx->d_active,
                   ctx->d_n_active, ctx->d_pots, ctx->d_geo, ctx->d_log, ctx->d_log_count, ctx->d_status,
-                  ctx->d_counters, ctx->d_api_total, ctx->d_api_event};
+                  ctx->d_counters, ctx->d_api_total, ctx->d_api_event, ctx->d_api_de, ctx->d_api_rates,
+                  ctx->d_api_sites, ctx->d_api_count};
   for (void* p : ptrs) cudaFree(p);
   ctx->d_jobs = nullptr;
   ctx->d_blocks = nullptr;
@@ -170,6 +186,8 @@ void free_device(akmc_ctx* ctx) {
   ctx->d_counters = nullptr;
   ctx->d_api_total = nullptr;
   ctx->d_api_event = nullptr;
+  ctx->d_api_de = ctx->d_api_rates = nullptr;
+  ctx->d_api_sites = ctx->d_api_count = nullptr;
   ctx->prepared = false;
 }
 
@@ -350,7 +368,9 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   if (ctx->smem > static_cast<size_t>(dev_smem))
     return fail(ctx, AKMC_EINVAL, "sector region does not fit in shared memory; use more domain blocks");
   {
-    const int e = configure_hop_smem(ctx->smem);
+    // The attribute belongs to the kernel, not to this context: set it to the device's
+    // limit, so that another context with smaller regions cannot lower it under this one.
+    const int e = configure_hop_smem(static_cast<size_t>(dev_smem));
     if (e) return fail(ctx, AKMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cuda_name(e));
   }
   int sms = 148;
@@ -500,6 +520,11 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(&ctx->d_log_count, 1));
   CK(dalloc(&ctx->d_api_total, 1));
   CK(dalloc(&ctx->d_api_event, 1));
+  CK(dalloc(&ctx->d_api_de, static_cast<size_t>(kMaxV) * 8));
+  CK(dalloc(&ctx->d_api_rates, static_cast<size_t>(kMaxV) * 8));
+  CK(dalloc(&ctx->d_api_sites, static_cast<size_t>(kMaxV)));
+  CK(dalloc(&ctx->d_api_count, 1));
+  CK(cudaMemsetAsync(ctx->d_api_count, 0, sizeof(int32_t), ctx->stream));
   if (ctx->cfg.event_log_capacity > 0) CK(dalloc(&ctx->d_log, static_cast<size_t>(ctx->cfg.event_log_capacity)));
   CK(cudaMemcpyAsync(ctx->d_jobs, hj.data(), hj.size() * sizeof(JobDev), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_blocks, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
@@ -546,6 +571,10 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.api_sector = -1;
   a.api_total = ctx->d_api_total;
   a.api_event = ctx->d_api_event;
+  a.api_de = ctx->d_api_de;
+  a.api_rates = ctx->d_api_rates;
+  a.api_sites = ctx->d_api_sites;
+  a.api_count = ctx->d_api_count;
   a.lease = ctx->d_lease;
   a.vclaim = ctx->d_vclaim;
   a.vvalid = ctx->d_vvalid;
@@ -752,6 +781,14 @@ AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule) {
   return AKMC_OK;
 }
 
+AKMC_API akmc_status akmc_get_round_schedule(akmc_ctx* ctx, int32_t* effective) {
+  if (!ctx || !effective) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  const bool flow = ctx->schedule == AKMC_SCHEDULE_FLOW || (ctx->schedule == AKMC_SCHEDULE_AUTO && ctx->flow_ok);
+  *effective = flow ? AKMC_SCHEDULE_FLOW : AKMC_SCHEDULE_ROUNDS;
+  return AKMC_OK;
+}
+
 AKMC_API akmc_status akmc_sync(akmc_ctx* ctx) {
   if (!ctx) return AKMC_EINVAL;
   if (!ctx->prepared) return AKMC_OK;
@@ -911,6 +948,24 @@ AKMC_API akmc_status akmc_calculate(akmc_ctx* ctx, int32_t job, int32_t sector_i
   return akmc_sync(ctx);
 }
 
+AKMC_API akmc_status akmc_get_calculated_rates(akmc_ctx* ctx, int32_t* sites, double* delta_e, double* rates,
+                                               int64_t capacity, int64_t* n_out) {
+  if (!ctx || !n_out || capacity < 0 || (capacity > 0 && (!sites || !delta_e || !rates))) return AKMC_EINVAL;
+  *n_out = 0;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  int32_t n = 0;
+  CK(cudaMemcpyAsync(&n, ctx->d_api_count, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_out = n;
+  if (n > capacity) return fail(ctx, AKMC_EINVAL, "capacity below the sector's vacancy count");
+  if (n == 0) return AKMC_OK;
+  CK(cudaMemcpyAsync(sites, ctx->d_api_sites, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(delta_e, ctx->d_api_de, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(rates, ctx->d_api_rates, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return akmc_sync(ctx);
+}
+
 AKMC_API akmc_status akmc_select_and_perform(akmc_ctx* ctx, int32_t job, int32_t sector_id, double u,
                                              akmc_event* ev) {
   if (!ctx || !ev) return AKMC_EINVAL;
@@ -936,6 +991,48 @@ AKMC_API akmc_status akmc_cluster_stats(const uint8_t* occ, const int64_t box[3]
                                         int64_t hist_len) {
   if (!occ || !box || !isolated_cu || (!hist && hist_len > 0)) return AKMC_EINVAL;
   return cluster_stats(occ, box, isolated_cu, hist, hist_len) ? AKMC_EINVAL : AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_job_cluster_stats(akmc_ctx* ctx, int32_t job, int64_t* isolated_cu, int64_t* hist,
+                                            int64_t hist_len) {
+  if (!ctx || !isolated_cu || hist_len < 0 || hist_len > AKMC_CLUSTER_MAX_BINS || (hist_len > 0 && !hist))
+    return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  CK(cudaSetDevice(ctx->cfg.device));
+  if (ctx->cl_sites < j.nsites) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_cl);
+    ctx->d_cl = nullptr;
+    ctx->cl_sites = 0;
+    CK(dalloc(&ctx->d_cl, static_cast<size_t>(3 * j.nsites)));
+    ctx->cl_sites = j.nsites;
+  }
+  if (!ctx->d_cl_misc) CK(dalloc(&ctx->d_cl_misc, 2 + AKMC_CLUSTER_MAX_BINS));
+  ClusterArgs c{};
+  c.occ = j.d_occ;
+  c.ns = j.nsites;
+  c.sx = 2 * static_cast<int32_t>(j.cfg.box[0]);
+  c.sy = static_cast<int32_t>(j.cfg.box[1]);
+  c.sz = static_cast<int32_t>(j.cfg.box[2]);
+  c.bins = hist_len > 0 ? static_cast<int32_t>(hist_len) : 1;
+  c.list = ctx->d_cl;
+  c.parent = ctx->d_cl + j.nsites;
+  c.size = ctx->d_cl + 2 * j.nsites;
+  c.n_list = reinterpret_cast<unsigned int*>(ctx->d_cl_misc);
+  c.iso = ctx->d_cl_misc + 1;
+  c.hist = ctx->d_cl_misc + 2;
+  c.status = ctx->d_status;
+  const int e = launch_cluster_stats(c, ctx->stream);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+  std::vector<unsigned long long> h(static_cast<size_t>(1 + c.bins));
+  CK(cudaMemcpyAsync(h.data(), c.iso, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  const akmc_status st = akmc_sync(ctx);
+  if (st != AKMC_OK) return st;
+  *isolated_cu = static_cast<int64_t>(h[0]);
+  for (int64_t k = 0; k < hist_len; ++k) hist[k] = static_cast<int64_t>(h[static_cast<size_t>(1 + k)]);
+  return AKMC_OK;
 }
 
 AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out) {

@@ -1,0 +1,188 @@
+// akmc_cluster.cu -- Cu cluster statistics of a job's resident lattice.
+//
+// The isolated-Cu count of MEventHook::onStepFinished (profiles/m_event_hook.cpp:17-55: a Cu
+// atom none of whose 8 first neighbours is Cu) and the Cu cluster-size histogram by 1nn
+// connectivity, on the device, so that a run can sample them every few rounds without
+// copying the lattice out.
+//
+//   k_cu_collect  one pass over the occupancy bytes (16 per thread, vector loads): every Cu
+//                 site is appended to a list, starts as its own root and is tested for a Cu
+//                 neighbour.  The only pass over the whole lattice: HBM-bound.
+//   k_cu_union    per listed site, each 1nn Cu bond to a higher site id is merged into one
+//                 set (lock-free union-find: the larger root is hooked under the smaller with
+//                 a CAS, finds halve their paths).
+//   k_cu_size     per listed site, +1 on its root's size.
+//   k_cu_hist     per root, +1 on the bin of its size (min(size, bins - 1)).
+// The partition, hence every count, does not depend on the order the threads run in.
+#include <algorithm>
+#include <cstdint>
+
+#include "akmc_device.h"
+
+namespace akmc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCuCode = AKMC_CU;
+constexpr int kFindLimit = 1 << 24;   // a find walks at most the set's size; the bound only guards
+constexpr int kUnionLimit = 1 << 20;  // CAS retries; each failure means another hook succeeded
+
+__device__ __forceinline__ int64_t nn1_site(int64_t s, int b, int sx, int sy, int sz) {
+  const int X = static_cast<int>(s % sx);
+  const int64_t t = s / sx;
+  const int y = static_cast<int>(t % sy), z = static_cast<int>(t / sy);
+  const int p = X & 1;
+  int gx = X + ((b & 4) ? 1 : -1);
+  int gy = y + ((b >> 1) & 1) - 1 + p;
+  int gz = z + (b & 1) - 1 + p;
+  gx = gx < 0 ? gx + sx : (gx >= sx ? gx - sx : gx);
+  gy = gy < 0 ? gy + sy : (gy >= sy ? gy - sy : gy);
+  gz = gz < 0 ? gz + sz : (gz >= sz ? gz - sz : gz);
+  return gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz);
+}
+
+// Mask with bit 7 of every byte of w that equals the Cu code (exact per byte: no borrow
+// crosses a byte boundary).
+__device__ __forceinline__ uint32_t cu_bytes(uint32_t w) {
+  const uint32_t x = w ^ (0x01010101u * kCuCode);
+  return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
+}
+
+// Thread t of the grid reads the 16 sites [16 t, 16 t + 16); the warp takes list slots with one
+// atomic and counts its isolated atoms with one more.
+__global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int sx, int sy, int sz, int32_t* list,
+                             unsigned int* n_list, int32_t* parent, int32_t* size, unsigned long long* iso) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nvec = (ns + 15) / 16;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  const uint4* v = reinterpret_cast<const uint4*>(occ);
+  for (int64_t w0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x - lane); w0 < nvec;
+       w0 += warps * 32) {
+    const int64_t i = w0 + lane;
+    uint32_t m[4] = {0, 0, 0, 0};
+    if (i * 16 + 16 <= ns) {
+      const uint4 w = __ldg(v + i);
+      m[0] = cu_bytes(w.x);
+      m[1] = cu_bytes(w.y);
+      m[2] = cu_bytes(w.z);
+      m[3] = cu_bytes(w.w);
+    } else if (i < nvec) {  // the last ns % 16 sites, byte by byte
+      for (int k = 0; i * 16 + k < ns; ++k)
+        if (occ[i * 16 + k] == kCuCode) m[k >> 2] |= 0x80u << (8 * (k & 3));
+    }
+    const int cnt = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+    int pre = cnt;  // inclusive prefix over the warp
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int o = __shfl_up_sync(kFull, pre, d);
+      if (lane >= d) pre += o;
+    }
+    unsigned int base = 0;
+    if (lane == 31 && pre) base = atomicAdd(n_list, static_cast<unsigned int>(pre));
+    base = __shfl_sync(kFull, base, 31) + static_cast<unsigned int>(pre - cnt);
+    int isolated = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      uint32_t z = m[k];
+      while (z) {
+        const int64_t s = i * 16 + k * 4 + ((__ffs(static_cast<int>(z)) - 1) >> 3);
+        z &= z - 1;
+        parent[s] = static_cast<int32_t>(s);
+        size[s] = 0;
+        bool has = false;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) has |= __ldg(occ + nn1_site(s, b, sx, sy, sz)) == kCuCode;
+        isolated += has ? 0 : 1;
+        list[base++] = static_cast<int32_t>(s);
+      }
+    }
+    isolated = __reduce_add_sync(kFull, isolated);
+    if (lane == 0 && isolated) atomicAdd(iso, static_cast<unsigned long long>(isolated));
+  }
+}
+
+__device__ __forceinline__ int32_t find_root(int32_t* parent, int32_t x, unsigned int* status) {
+  for (int it = 0; it < kFindLimit; ++it) {
+    const int32_t p = __ldcg(parent + x);
+    if (p == x) return x;
+    const int32_t gp = __ldcg(parent + p);
+    if (gp != p) atomicCAS(parent + x, p, gp);  // path halving; losing the race is harmless
+    x = gp;
+  }
+  atomicOr(status, kErrTimeout);
+  return x;
+}
+
+__global__ void k_cu_union(const uint8_t* __restrict__ occ, int sx, int sy, int sz, const int32_t* list,
+                           const unsigned int* n_list, int32_t* parent, unsigned int* status) {
+  const int64_t n = *n_list;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s = list[i];
+#pragma unroll 1
+    for (int b = 0; b < 8; ++b) {
+      const int64_t r = nn1_site(s, b, sx, sy, sz);
+      if (r <= s || __ldg(occ + r) != kCuCode) continue;
+      int32_t a = s, c = static_cast<int32_t>(r);
+      int it = 0;
+      for (; it < kUnionLimit; ++it) {
+        a = find_root(parent, a, status);
+        c = find_root(parent, c, status);
+        if (a == c) break;
+        if (a < c) {
+          const int32_t t = a;
+          a = c;
+          c = t;
+        }
+        if (atomicCAS(parent + a, a, c) == a) break;  // root a now hangs under c
+      }
+      if (it == kUnionLimit) atomicOr(status, kErrTimeout);
+    }
+  }
+}
+
+__global__ void k_cu_size(const int32_t* list, const unsigned int* n_list, int32_t* parent, int32_t* size,
+                          unsigned int* status) {
+  const int64_t n = *n_list;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    atomicAdd(size + find_root(parent, list[i], status), 1);
+}
+
+__global__ void k_cu_hist(const int32_t* list, const unsigned int* n_list, const int32_t* parent,
+                          const int32_t* size, unsigned long long* hist, int bins) {
+  extern __shared__ unsigned long long h_s[];
+  for (int k = threadIdx.x; k < bins; k += blockDim.x) h_s[k] = 0;
+  __syncthreads();
+  const int64_t n = *n_list;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t s = list[i];
+    if (parent[s] == s) atomicAdd(h_s + min(size[s], bins - 1), 1ull);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < bins; k += blockDim.x)
+    if (h_s[k]) atomicAdd(hist + k, h_s[k]);
+}
+
+}  // namespace
+
+int launch_cluster_stats(const ClusterArgs& c, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(c.n_list, 0, sizeof(unsigned int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.iso, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.hist, 0, sizeof(unsigned long long) * c.bins, st);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  const int64_t nvec = (c.ns + 15) / 16;
+  int grid = static_cast<int>(std::min<int64_t>((nvec + 255) / 256, 148 * 16));
+  if (grid < 1) grid = 1;
+  k_cu_collect<<<grid, 256, 0, st>>>(c.occ, c.ns, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.size, c.iso);
+  const int g2 = 148 * 8;
+  k_cu_union<<<g2, 256, 0, st>>>(c.occ, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.status);
+  k_cu_size<<<g2, 256, 0, st>>>(c.list, c.n_list, c.parent, c.size, c.status);
+  k_cu_hist<<<g2, 256, sizeof(unsigned long long) * c.bins, st>>>(c.list, c.n_list, c.parent, c.size, c.hist,
+                                                                   c.bins);
+  return static_cast<int>(cudaGetLastError());
+}
+
+}  // namespace akmc

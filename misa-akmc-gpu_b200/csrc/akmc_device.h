@@ -133,6 +133,10 @@ struct RoundArgs {
   double api_u;
   double* api_total;
   akmc_event* api_event;
+  double* api_de;         // kMaxV * 8: ΔE of each jump of the last akmc_calculate
+  double* api_rates;      // kMaxV * 8: its rates
+  int32_t* api_sites;     // kMaxV: vacancy sites (-1: left the sector)
+  int32_t* api_count;
 };
 
 // Kernel launchers (akmc_kernels.cu).
@@ -149,6 +153,22 @@ int launch_device_math(const double* x, int64_t n, double* e, double* l, void* s
 // n rounds of every unfinished block under the asynchronous schedule (no job may have a
 // hop budget); grid = persistent CTAs of the flow kernels.
 int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1);
+
+// Cu cluster statistics of one job's occupancy (akmc_cluster.cu).  list, parent and size hold
+// one int32 per site; iso and hist are cleared by the launch.
+struct ClusterArgs {
+  const uint8_t* occ;
+  int64_t ns;
+  int32_t sx, sy, sz, bins;
+  int32_t* list;
+  unsigned int* n_list;
+  int32_t* parent;
+  int32_t* size;
+  unsigned long long* iso;
+  unsigned long long* hist;
+  unsigned int* status;
+};
+int launch_cluster_stats(const ClusterArgs& c, void* stream);
 // Device address of the fixed round scratch (current device): kNoAllocMaxBlocks * kMaxV
 // block-list slots, then kNoAllocMaxBlocks active-list slots, then the active count.
 int noalloc_scratch(int32_t** base);

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <cstdint>
 
 #include "akmc_device.h"
 
@@ -96,8 +97,13 @@ struct Smem {
   // asynchronous schedule (k_flow)
   int8_t flow_lag[8][27];
   int32_t flow_cand[kThreads];
-  int32_t flow_ncand, flow_stop, flow_progress;
+  int32_t flow_ncand, flow_stop, flow_progress, flow_more;
   int32_t fv[kFlowSlots], fslot[kFlowSlots], fnv;  // the sector's vacancies and their slots
+  // device counters summed per CTA and added once when the kernel ends (per-round atomics on
+  // the same addresses from every CTA queue up); hops of the current job likewise
+  unsigned long long acc[6];  // counters 0 (hops), 1, 3, 4, 5, 6
+  int32_t acc_job;
+  unsigned long long acc_job_hops;
   uint64_t xsn[4];        // selection stream after the uniform drawn ahead
 };
 
@@ -157,7 +163,7 @@ struct JobC {
   double nu, kT;
 };
 
-#ifdef AKMC_PHASE_PROFILE
+#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE)
 #define EVAL_T(i)                                                                       \
   do {                                                                                  \
     if (threadIdx.x == 0) {                                                             \
@@ -279,7 +285,7 @@ enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };
 //             embedding change is added.
 template <int KIND>
 __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const FTab& FT,
-                             const JobC& jc, const int32_t (&jr)[2][3]) {
+                             const JobC& jc, const int32_t (&jr)[2][3], double* de_out) {
   const int lane = threadIdx.x & 31;
   const int b = threadIdx.x >> 5;
   const int q = lane;
@@ -387,6 +393,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
   if (q == 0) {
     sm.rates[k][b] = avail ? arrhenius(jc.nu, jc.kT, Xc, dE) : 0.0;
     sm.vavb[k][b] = avail ? 1 : 0;
+    if (de_out) de_out[k * 8 + b] = avail ? dE : 0.0;  // akmc_calculate only
   }
   if (KIND == kEam64) EVAL_T(3);
 }
@@ -617,6 +624,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   bool clock_due = false;  // a selection with a positive total happened since the last clock
   const int D = eam ? 4 : 3;
   bool first = true;
+  double* const de_out = a.mode == kModeCalc ? a.api_de : nullptr;
   // vacancies to evaluate: all active ones on the first pass, then those within D cells
   // of the last hop's origin (every warp derives the same set)
   auto dirty_mask = [&](int base) -> unsigned {
@@ -641,7 +649,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           while (m) {
             const int k = base + __ffs(m) - 1;
             m &= m - 1;
-            eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr);
+            eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr, de_out);
           }
         }
       }
@@ -736,6 +744,12 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         double u = 0.0, expected = 0.0;
         if (a.mode == kModeCalc) {
           *a.api_total = total;
+          // the sector's vacancies with their jump rates (ΔE is written by the evaluators)
+          for (int i = 0; i < cnt; ++i) {
+            a.api_sites[i] = sm.vact[i] ? sm.vlid[i] : -1;
+            for (int bb = 0; bb < 8; ++bb) a.api_rates[i * 8 + bb] = sm.rates[i][bb];
+          }
+          *a.api_count = cnt;
           stop = 1;
         } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
           if (a.mode == kModeSelectPerform) {
@@ -880,13 +894,19 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
     B.hops = hop0 + nh;
-    if (nh) atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[B.job].hops), static_cast<unsigned long long>(nh));
-    atomicAdd(a.counters + 0, static_cast<unsigned long long>(nh));
-    atomicAdd(a.counters + 1, static_cast<unsigned long long>(evals));
-    atomicAdd(a.counters + 3, 1ull);
-    atomicAdd(a.counters + 4, static_cast<unsigned long long>(nact_sum));
-    atomicAdd(a.counters + 5, static_cast<unsigned long long>(R.n));
-    if (nh) atomicAdd(a.counters + 6, static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2)));
+    if (sm.acc_job != B.job) {
+      if (sm.acc_job >= 0 && sm.acc_job_hops)
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[sm.acc_job].hops), sm.acc_job_hops);
+      sm.acc_job = B.job;
+      sm.acc_job_hops = 0;
+    }
+    sm.acc_job_hops += static_cast<unsigned long long>(nh);
+    sm.acc[0] += static_cast<unsigned long long>(nh);
+    sm.acc[1] += static_cast<unsigned long long>(evals);
+    sm.acc[2] += 1ull;
+    sm.acc[3] += static_cast<unsigned long long>(nact_sum);
+    sm.acc[4] += static_cast<unsigned long long>(R.n);
+    sm.acc[5] += static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2));
   }
   // the lattice was written through at every hop; only the vacancy positions remain
   if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[tid];
@@ -956,8 +976,24 @@ __device__ void init_cta_smem(uint8_t* smem) {
     sm->win_pot = -1;
     sm->mbar_phase = 0;
     mbar_init(&sm->mbar);
+    for (int i = 0; i < 6; ++i) sm->acc[i] = 0;
+    sm->acc_job = -1;
+    sm->acc_job_hops = 0;
   }
   __syncthreads();
+}
+
+// Adds the CTA's counters (summed by the control thread) to the device counters; CTA-wide.
+__device__ void cta_flush(const RoundArgs& a, uint8_t* smem) {
+  Smem* sm = reinterpret_cast<Smem*>(smem);
+  __syncthreads();
+  if (threadIdx.x == kCtl) {
+    const int idx[6] = {0, 1, 3, 4, 5, 6};
+    for (int i = 0; i < 6; ++i)
+      if (sm->acc[i]) atomicAdd(a.counters + idx[i], sm->acc[i]);
+    if (sm->acc_job >= 0 && sm->acc_job_hops)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[sm->acc_job].hops), sm->acc_job_hops);
+  }
 }
 
 __device__ __forceinline__ int job_kind(const JobDev& J) {
@@ -984,6 +1020,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_hop(RoundArgs a) {
     carve(smem, R.n, sm, occ_s, rho_s);
     run_block<KIND>(a, gb, *sm, occ_s, rho_s, a.blk_list + static_cast<int64_t>(gb) * kMaxV, min(B.cnt, kMaxV));
   }
+  cta_flush(a, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1015,9 +1052,12 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 __device__ __forceinline__ int64_t ld_relaxed64(const int64_t* p) {
   int64_t v;
-  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  // no memory clobber: a relaxed load orders nothing; the fence after it does
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
   return v;
 }
+// Release/acquire fence at GPU scope (lighter than the sequentially consistent __threadfence).
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release64(int64_t* p, int64_t v) {
   asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -1062,7 +1102,7 @@ __device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, in
     const int k = lag[ph][o];
     if (k) ok &= ld_relaxed64(&a.blocks[flow_neighbour(J, local_id, o)].round) >= r - k + 1;
   }
-  if (ok) __threadfence();
+  if (ok) fence_acq_rel();
   return ok;
 }
 
@@ -1089,17 +1129,6 @@ __device__ __forceinline__ int owner_block(const JobDev& J, int32_t s) {
   return J.block0 + k[0] + J.nb[0] * (k[1] + J.nb[1] * k[2]);
 }
 
-__device__ bool flow_sector_has_vacancy(const RoundArgs& a, const BlockDev& B, const JobDev& J, int gb, int sec) {
-  unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
-  while (m) {
-    const int slot = __ffsll(static_cast<long long>(m)) - 1;
-    m &= m - 1;
-    const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + slot]);
-    if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) return true;
-  }
-  return false;
-}
-
 // Puts vacancy v into block o's slots: claim a free slot, write the id, then mark it valid.
 __device__ void flow_give(const RoundArgs& a, int o, int v) {
   for (int tries = 0; tries < 4 * kFlowSlots; ++tries) {
@@ -1109,19 +1138,101 @@ __device__ void flow_give(const RoundArgs& a, int o, int v) {
     const unsigned long long bit = 1ull << slot;
     if (atomicOr(&a.vclaim[o], bit) & bit) continue;  // taken meanwhile
     a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
-    __threadfence();
+    fence_acq_rel();
     atomicOr(&a.vvalid[o], bit);
     return;
   }
   atomicOr(a.status, kErrVacOverflow);
 }
 
-// Publishes round r of block B as complete (after every write of the round).
+// Publishes round r of block B as complete.  The release is cumulative: writes of other
+// threads of the CTA that a barrier ordered before this call are released too.
 __device__ __forceinline__ void flow_publish(const RoundArgs& a, BlockDev& B, int64_t r, int kind) {
-  __threadfence();
+  fence_acq_rel();
   st_release64(&B.round, r + 1);
   if (r + 1 == B.target) atomicAdd(&a.flow_done[kind], 1);
 }
+
+// Lease held, one thread: runs the block's ready rounds whose sectors hold no vacancy (the
+// clock jumps to the window, sublattice.inl:108-112), up to 64 in one batch.  The neighbours'
+// round counters are read once, all 27 loads in flight together: a round is ready when that
+// snapshot already covers it, and the vacancy slots read after the snapshot hold every vacancy
+// those rounds can see (a round that could bring one into such a sector overlaps it, so it is
+// in the snapshot).  Returns true when it stops at a ready round with vacancies, false when the
+// next round is not ready or the target is reached.
+__device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, int gb, const int8_t (*lag)[27],
+                             int kind, int* progress) {
+  const int64_t r0 = ld_relaxed64(&B.round);
+  const int64_t target = B.target;
+  if (r0 >= target) return false;
+  const int n0 = J.nb[0], n1 = J.nb[1], n2 = J.nb[2], block0 = J.block0, lid = B.local_id;
+  const int bx = lid % n0, by = (lid / n0) % n1, bz = lid / (n0 * n1);
+  int64_t P[27];
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    const int y = block0 + wrapb(bx + o % 3 - 1, n0) + n0 * (wrapb(by + (o / 3) % 3 - 1, n1) + n1 * wrapb(bz + o / 9 - 1, n2));
+    P[o] = y == gb ? INT64_MAX : ld_relaxed64(&a.blocks[y].round);  // the block itself never holds it back
+  }
+  fence_acq_rel();
+  double evo[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) evo[k] = __ldcg(&B.evo[k]);
+  // sectors holding a vacancy
+  unsigned occ_sec = 0;
+  unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
+  const int hx = B.c0[0] + (B.c1[0] - B.c0[0]) / 2, hy = B.c0[1] + (B.c1[1] - B.c0[1]) / 2,
+            hz = B.c0[2] + (B.c1[2] - B.c0[2]) / 2;
+  while (m) {
+    const int slot = __ffsll(static_cast<long long>(m)) - 1;
+    m &= m - 1;
+    const int32_t st = __ldcg(&a.vac_site[__ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + slot])]);
+    const int X = st % J.sx, t = st / J.sx;
+    occ_sec |= 1u << (((X >> 1) >= hx ? 1 : 0) | ((t % J.sy) >= hy ? 2 : 0) | ((t / J.sy) >= hz ? 4 : 0));
+  }
+  const int64_t last = min(target, r0 + 64);
+  const double window = J.window;
+  int64_t r = r0;
+  bool stop_full = false;
+  while (r < last) {
+    const int ph = static_cast<int>(r & 7);
+    bool ok = true;
+#pragma unroll
+    for (int o = 0; o < 27; ++o) {
+      const int k = lag[ph][o];
+      if (k && P[o] < r - k + 1) ok = false;
+    }
+    if (!ok) break;
+    const int sec = sector_of_round(r);
+    if ((occ_sec >> sec) & 1u) {
+      stop_full = true;
+      break;
+    }
+    double e = evo[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) e = k == sec ? evo[k] : e;
+    const double thr = static_cast<double>((r >> 3) + 1) * window - e;
+    double sector_time = 0.0;
+    if (sector_time < thr) sector_time = thr;
+    const double ne = e + sector_time;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) evo[k] = k == sec ? ne : evo[k];
+    ++r;
+  }
+  if (r > r0) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) B.evo[k] = evo[k];
+    flow_publish(a, B, r - 1, kind);
+    *progress = 1;
+  }
+  return stop_full;
+}
+
+// Rounds with vacancies a CTA takes per sweep, and rounds of one block it runs back to back
+// while the next one is ready.  Measured on the 256^3 lattice and the 512 batched boxes: taking
+// every ready round found, one round per block at a time, beats taking one per sweep (others
+// left to idle CTAs) and beats chaining up to 8 rounds of one block.
+constexpr int kFlowTake = kThreads;
+constexpr int kFlowChain = 1;
 
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
@@ -1135,7 +1246,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
   }
   const int nb = a.nblocks;
   int cursor = static_cast<int>((static_cast<int64_t>(blockIdx.x) * nb) / gridDim.x);
+#ifdef AKMC_PHASE_PROFILE
+  long long t_sweep = 0, t_hop = 0, n_sweep = 0, n_full = 0, t0 = 0;
+#endif
   for (int64_t sweep = 0;; ++sweep) {
+#ifdef AKMC_PHASE_PROFILE
+    if (tid == 0) t0 = clock64();
+#endif
     if (tid == 0) {
       sm0->flow_ncand = 0;
       sm0->flow_progress = 0;
@@ -1158,98 +1275,147 @@ __global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
       if (gb >= nb) gb -= nb;
       BlockDev& B = a.blocks[gb];
       const JobDev& J = a.jobs[B.job];
-      int64_t r = ld_relaxed64(&B.round);
+      const int64_t r = ld_relaxed64(&B.round);
       if (job_kind(J) == KIND && r < B.target && *reinterpret_cast<volatile int*>(&a.lease[gb]) == 0 &&
           flow_ready(a, J, B.local_id, r, sm0->flow_lag) && atomicCAS(&a.lease[gb], 0, 1) == 0) {
-        __threadfence();
+        fence_acq_rel();
         bool keep = false;
-        for (int n = 0; n < 64; ++n) {
-          r = ld_acquire64(&B.round);
-          if (r >= B.target || !flow_ready(a, J, B.local_id, r, sm0->flow_lag)) break;
-          const int sec = sector_of_round(r);
-          if (flow_sector_has_vacancy(a, B, J, gb, sec)) {  // the CTA runs this one
-            sm0->flow_cand[atomicAdd(&sm0->flow_ncand, 1)] = gb;
+        if (flow_advance(a, B, J, gb, sm0->flow_lag, KIND, &sm0->flow_progress)) {
+          const int i = atomicAdd(&sm0->flow_ncand, 1);
+          if (i < kFlowTake) {
+            sm0->flow_cand[i] = gb;
             keep = true;
-            break;
           }
-          // no vacancy in the sector: total = 0, the clock jumps to the window
-          const int64_t step = r >> 3;
-          const double evo = __ldcg(&B.evo[sec]);
-          const double thr = static_cast<double>(step + 1) * J.window - evo;
-          double sector_time = 0.0;
-          if (sector_time < thr) sector_time = thr;
-          B.evo[sec] = evo + sector_time;
-          flow_publish(a, B, r, KIND);
-          sm0->flow_progress = 1;
         }
         if (!keep) {
-          __threadfence();
+          fence_acq_rel();
           atomicExch(&a.lease[gb], 0);
         }
       }
     }
     __syncthreads();
+#ifdef AKMC_PHASE_PROFILE
+    if (tid == 0) {
+      const long long t1 = clock64();
+      t_sweep += t1 - t0;
+      t0 = t1;
+      ++n_sweep;
+    }
+#endif
 
-    // the hop loop for each round handed over
-    const int ncand = sm0->flow_ncand;
+    // the hop loop for each round handed over, then for the block's next rounds while they
+    // are ready (empty ones in between run on thread 0)
+    const int ncand = min(sm0->flow_ncand, kFlowTake);
     for (int c = 0; c < ncand; ++c) {
       const int gb = sm0->flow_cand[c];
-      BlockDev& B = a.blocks[gb];
-      const JobDev& J = a.jobs[B.job];
-      const int64_t r = ld_acquire64(&B.round);
-      // every thread acquires the rounds this one waits for, not only the sweeping thread
-      if (tid < 27 && sm0->flow_lag[r & 7][tid]) (void)ld_acquire64(&a.blocks[flow_neighbour(J, B.local_id, tid)].round);
-      __threadfence();
-      const int sec = sector_of_round(r);
-      Region R;
-      make_region(B, sec, R);
-      Smem* sm;
-      uint8_t* occ_s;
-      int32_t* rho_s;
-      carve(smem, R.n, sm, occ_s, rho_s);
-      if (tid == 0) sm->fnv = 0;
-      __syncthreads();
-      if (tid < kFlowSlots) {
-        const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
-        if ((m >> tid) & 1ull) {
-          const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + tid]);
-          if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) {
-            const int i = atomicAdd(&sm->fnv, 1);
-            sm->fv[i] = v;
-            sm->fslot[i] = tid;
+      for (int link = 0;; ++link) {
+#ifdef AKMC_PHASE_PROFILE
+        long long tw = clock64();
+#endif
+        BlockDev& B = a.blocks[gb];
+        const JobDev& J = a.jobs[B.job];
+        const int64_t r = ld_acquire64(&B.round);
+        // the rounds this one waits for are acquired again here; the barrier below orders
+        // every thread's reads after these acquires (shared data is read at L2)
+        if (tid < 27 && sm0->flow_lag[r & 7][tid]) (void)ld_acquire64(&a.blocks[flow_neighbour(J, B.local_id, tid)].round);
+        const int sec = sector_of_round(r);
+        Region R;
+        make_region(B, sec, R);
+        Smem* sm;
+        uint8_t* occ_s;
+        int32_t* rho_s;
+        carve(smem, R.n, sm, occ_s, rho_s);
+        if (tid == 0) sm->fnv = 0;
+        __syncthreads();
+        if (tid < kFlowSlots) {
+          const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
+          if ((m >> tid) & 1ull) {
+            const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + tid]);
+            if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) {
+              const int i = atomicAdd(&sm->fnv, 1);
+              sm->fv[i] = v;
+              sm->fslot[i] = tid;
+            }
           }
         }
-      }
-      __syncthreads();
-      const int cnt = sm->fnv;
-      const bool ran = run_block<KIND>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt);
-      __syncthreads();
-      // vacancies carried into a neighbour's area change owner (only if the round ran:
-      // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
-      if (ran && tid < cnt) {
-        const int o = owner_block(J, sm->vlid[tid]);
-        if (o != gb) {
-          flow_give(a, o, sm->vidx[tid]);
-          const unsigned long long bit = 1ull << sm->fslot[tid];
-          atomicAnd(&a.vvalid[gb], ~bit);
-          __threadfence();
-          atomicAnd(&a.vclaim[gb], ~bit);
+        __syncthreads();
+        const int cnt = sm->fnv;
+#ifdef AKMC_PHASE_PROFILE
+        if (tid == 0) {
+          atomicAdd(a.counters + 12, static_cast<unsigned long long>(clock64() - tw));  // [4] before the hop loop
+          tw = clock64();
         }
+#endif
+        const bool ran = run_block<KIND>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt);
+#ifdef AKMC_PHASE_PROFILE
+        if (tid == 0) tw = clock64();
+#endif
+        __syncthreads();
+        // vacancies carried into a neighbour's area change owner (only if the round ran:
+        // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
+        if (ran && tid < cnt) {
+          const int o = owner_block(J, sm->vlid[tid]);
+          if (o != gb) {
+            flow_give(a, o, sm->vidx[tid]);
+            const unsigned long long bit = 1ull << sm->fslot[tid];
+            atomicAnd(&a.vvalid[gb], ~bit);
+            fence_acq_rel();
+            atomicAnd(&a.vclaim[gb], ~bit);
+          }
+        }
+        __syncthreads();
+        if (tid == 0) {
+#ifdef AKMC_FLOW_PROFILE
+          const long long q0 = clock64();
+#endif
+          flow_publish(a, B, r, KIND);
+          sm->flow_progress = 1;
+#ifdef AKMC_FLOW_PROFILE
+          const long long q1 = clock64();
+#endif
+          // keep the lease for the block's next round with vacancies, if it is ready now
+          const bool more = link + 1 < kFlowChain && flow_advance(a, B, J, gb, sm0->flow_lag, KIND, &sm->flow_progress);
+#ifdef AKMC_FLOW_PROFILE
+          const long long q2 = clock64();
+#endif
+          sm->flow_more = more;
+          if (!more) {
+            fence_acq_rel();
+            atomicExch(&a.lease[gb], 0);
+          }
+#ifdef AKMC_FLOW_PROFILE
+          atomicAdd(a.counters + 20, static_cast<unsigned long long>(q1 - q0));
+          atomicAdd(a.counters + 21, static_cast<unsigned long long>(q2 - q1));
+          atomicAdd(a.counters + 22, static_cast<unsigned long long>(clock64() - q2));
+          atomicAdd(a.counters + 23, static_cast<unsigned long long>(q0 - tw));
+#endif
+        }
+        __syncthreads();
+#ifdef AKMC_PHASE_PROFILE
+        if (tid == 0) {
+          ++n_full;
+          atomicAdd(a.counters + 15, static_cast<unsigned long long>(clock64() - tw));  // [7] after the hop loop
+        }
+#endif
+        if (!sm0->flow_more) break;
       }
-      __threadfence();  // every thread's lattice, record and slot writes before the round is published
-      __syncthreads();
-      if (tid == 0) {
-        flow_publish(a, B, r, KIND);
-        __threadfence();
-        atomicExch(&a.lease[gb], 0);
-        sm->flow_progress = 1;
-      }
-      __syncthreads();
     }
+#ifdef AKMC_PHASE_PROFILE
+    if (tid == 0) t_hop += clock64() - t0;
+#endif
     if (!sm0->flow_progress) __nanosleep(256);
     cursor += kThreads;
     if (cursor >= nb) cursor %= nb;
   }
+  cta_flush(a, smem);
+#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE)
+  if (tid == 0) {  // scheduler profile: [12] sweep cycles, [13] hop-loop cycles, [14] sweeps, [15] full rounds
+    atomicAdd(a.counters + 20, static_cast<unsigned long long>(t_sweep));
+    atomicAdd(a.counters + 21, static_cast<unsigned long long>(t_hop));
+    atomicAdd(a.counters + 22, static_cast<unsigned long long>(n_sweep));
+    atomicAdd(a.counters + 23, static_cast<unsigned long long>(n_full));
+  }
+#endif
 }
 
 // Per block: target round of this launch, lease and slots cleared; counts the blocks with
@@ -1337,8 +1503,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_api_block(RoundArgs a) {
   const JobDev& J = a.jobs[a.api_job];
   if (*a.n_active == 0) {  // no vacancy in the sector
     if (threadIdx.x == 0) {
-      if (a.mode == kModeCalc) *a.api_total = 0.0;
-      else {
+      if (a.mode == kModeCalc) {
+        *a.api_total = 0.0;
+        *a.api_count = 0;
+      } else {
         a.api_event->from_site = -1;
         a.api_event->total = 0.0;
       }
@@ -1347,6 +1515,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_api_block(RoundArgs a) {
   }
   init_cta_smem(smem);
   dispatch_block(a, J.block0, smem);
+  cta_flush(a, smem);
 }
 __global__ void k_api_reset(RoundArgs a) {
   const JobDev& J = a.jobs[a.api_job];

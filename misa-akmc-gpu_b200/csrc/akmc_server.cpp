@@ -1,0 +1,282 @@
+// akmc_server.cpp -- job server over the context API of include/akmc.h.
+//
+// Jobs queue in arrival order.  Each lane (a host thread with its own context, hence its
+// own CUDA stream) takes the queued jobs that fit the device-memory budget as one batch,
+// runs them together in chunks of rounds and publishes every job's result the moment that
+// job is done, so short jobs do not wait for the long ones of their batch.  Lanes overlap
+// on the GPU.  All shared state is under one mutex; the device work runs outside it.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/akmc.h"
+
+namespace {
+
+struct SJob {
+  int64_t ticket = 0;
+  akmc_job_config cfg{};
+  bool has_eam = false;
+  akmc_eam_tables eam{};
+  std::vector<uint8_t> occ;
+  int64_t bytes = 0;
+  int state = 0;  // 0 queued, 1 running, 2 done
+  akmc_job_result res{};
+  std::vector<uint8_t> out;
+};
+
+// Device bytes a job holds: occupancy, density cache, block records and lists, vacancies.
+int64_t job_bytes(const akmc_job_config& c, int64_t nsites, int64_t nvac) {
+  const int64_t nb = static_cast<int64_t>(std::max(1, c.blocks[0])) * std::max(1, c.blocks[1]) * std::max(1, c.blocks[2]);
+  const int64_t per_site = c.energy_model == AKMC_MODEL_EAM ? 5 : 1;
+  return nsites * per_site + nb * 1024 + nvac * 16 + (c.energy_model == AKMC_MODEL_EAM ? 400000 : 0);
+}
+
+}  // namespace
+
+struct akmc_server {
+  akmc_server_config cfg{};
+  std::mutex m;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<SJob>> queue;
+  std::unordered_map<int64_t, std::shared_ptr<SJob>> jobs;  // queued, running or done, not collected
+  int64_t next_ticket = 1;
+  int64_t held = 0;     // bytes of the jobs in running batches
+  int64_t running = 0;  // jobs in running batches
+  bool stopping = false;
+  std::vector<std::thread> lanes;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  void publish(const std::shared_ptr<SJob>& j, int32_t status, akmc_ctx* ctx = nullptr) {
+    char msg[sizeof(j->res.error)] = {0};
+    if (status != AKMC_OK && ctx) akmc_last_error(ctx, msg, static_cast<int32_t>(sizeof(msg)));
+    std::lock_guard<std::mutex> lk(m);
+    j->res.status = status;
+    std::memcpy(j->res.error, msg, sizeof(msg));
+    j->res.finish_s = now();
+    j->state = 2;
+    --running;
+    cv_done.notify_all();
+  }
+
+  void run_batch(std::vector<std::shared_ptr<SJob>>& batch) {
+    akmc_context_config cc{};
+    cc.device = cfg.device;
+    cc.graph_rounds = cfg.chunk_rounds;
+    akmc_ctx* ctx = nullptr;
+    akmc_status st = akmc_create(&cc, &ctx);
+    if (st != AKMC_OK) {
+      for (auto& j : batch) publish(j, st);
+      return;
+    }
+    std::vector<std::pair<std::shared_ptr<SJob>, int32_t>> live;
+    for (auto& j : batch) {
+      akmc_job_config c = j->cfg;
+      c.eam = j->has_eam ? &j->eam : nullptr;
+      int32_t id = -1;
+      const akmc_status s = akmc_add_job(ctx, &c, j->occ.data(), static_cast<int64_t>(j->occ.size()), &id);
+      if (s != AKMC_OK) publish(j, s, ctx);
+      else live.emplace_back(j, id);
+    }
+    if (!live.empty()) st = akmc_prepare(ctx);
+    while (st == AKMC_OK && !live.empty()) {
+      st = akmc_run_rounds(ctx, cfg.chunk_rounds);
+      if (st == AKMC_OK) st = akmc_sync(ctx);
+      if (st != AKMC_OK) break;
+      for (size_t i = 0; i < live.size();) {
+        akmc_job_state js{};
+        st = akmc_get_job_state(ctx, live[i].second, &js);
+        if (st != AKMC_OK) break;
+        if (!js.done) {
+          ++i;
+          continue;
+        }
+        auto& j = live[i].first;
+        j->out.resize(j->occ.size());
+        st = akmc_get_occupancy(ctx, live[i].second, j->out.data(), static_cast<int64_t>(j->out.size()));
+        if (st != AKMC_OK) break;
+        j->res.hops = js.hops;
+        j->res.rounds = js.round;
+        j->res.n_blocks = js.n_blocks;
+        publish(j, AKMC_OK);
+        live.erase(live.begin() + static_cast<long>(i));
+      }
+    }
+    for (auto& p : live) publish(p.first, st == AKMC_OK ? AKMC_ESTATE : st, ctx);
+    if (ctx) akmc_destroy(ctx);
+  }
+
+  void lane() {
+    for (;;) {
+      std::vector<std::shared_ptr<SJob>> batch;
+      int64_t bytes = 0;
+      {
+        std::unique_lock<std::mutex> lk(m);
+        cv_work.wait(lk, [&] {
+          return stopping || (!queue.empty() && held + queue.front()->bytes <= cfg.budget_bytes);
+        });
+        if (stopping) return;
+        while (!queue.empty() && static_cast<int32_t>(batch.size()) < cfg.max_batch_jobs &&
+               held + bytes + queue.front()->bytes <= cfg.budget_bytes) {
+          auto j = queue.front();
+          queue.pop_front();
+          j->state = 1;
+          j->res.start_s = now();
+          bytes += j->bytes;
+          batch.push_back(j);
+        }
+        held += bytes;
+        running += static_cast<int64_t>(batch.size());
+      }
+      run_batch(batch);
+      {
+        std::lock_guard<std::mutex> lk(m);
+        held -= bytes;
+      }
+      cv_work.notify_all();
+    }
+  }
+};
+
+namespace {
+
+bool collect(akmc_server* s, const std::shared_ptr<SJob>& j, akmc_job_result* res, uint8_t* occ_out, int64_t n) {
+  if (res) *res = j->res;
+  if (occ_out && !j->out.empty()) std::memcpy(occ_out, j->out.data(), static_cast<size_t>(std::min<int64_t>(n, static_cast<int64_t>(j->out.size()))));
+  s->jobs.erase(j->ticket);
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+AKMC_API akmc_status akmc_server_create(const akmc_server_config* cfg, akmc_server** out) {
+  if (!out) return AKMC_EINVAL;
+  *out = nullptr;
+  akmc_server* s = new (std::nothrow) akmc_server();
+  if (!s) return AKMC_ENOMEM;
+  if (cfg) s->cfg = *cfg;
+  if (s->cfg.lanes <= 0) s->cfg.lanes = 2;
+  if (s->cfg.budget_bytes <= 0) s->cfg.budget_bytes = int64_t(8) << 30;
+  if (s->cfg.max_batch_jobs <= 0) s->cfg.max_batch_jobs = 512;
+  if (s->cfg.chunk_rounds <= 0) s->cfg.chunk_rounds = 16;
+  try {
+    for (int i = 0; i < s->cfg.lanes; ++i) s->lanes.emplace_back([s] { s->lane(); });
+  } catch (...) {
+    {
+      std::lock_guard<std::mutex> lk(s->m);
+      s->stopping = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->lanes) t.join();
+    delete s;
+    return AKMC_ENOMEM;
+  }
+  *out = s;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_submit(akmc_server* s, const akmc_job_config* cfg, const uint8_t* occ,
+                                        int64_t n_sites, int64_t* ticket) {
+  if (!s || !cfg || !occ || !ticket) return AKMC_EINVAL;
+  *ticket = 0;
+  if (cfg->hop_budget <= 0 && cfg->max_rounds <= 0) return AKMC_EINVAL;  // the job would never end
+  for (int d = 0; d < 3; ++d)
+    if (cfg->box[d] < 8 || cfg->box[d] > (1 << 20)) return AKMC_EINVAL;
+  if (n_sites != 2 * cfg->box[0] * cfg->box[1] * cfg->box[2]) return AKMC_EINVAL;
+  if (cfg->energy_model == AKMC_MODEL_EAM && !cfg->eam) return AKMC_EINVAL;
+  auto j = std::make_shared<SJob>();
+  j->cfg = *cfg;
+  j->has_eam = cfg->eam != nullptr;
+  if (j->has_eam) j->eam = *cfg->eam;
+  j->cfg.eam = nullptr;
+  j->occ.assign(occ, occ + n_sites);
+  const int64_t nvac = std::count(j->occ.begin(), j->occ.end(), static_cast<uint8_t>(AKMC_V));
+  j->bytes = job_bytes(*cfg, n_sites, nvac);
+  {
+    std::lock_guard<std::mutex> lk(s->m);
+    if (s->stopping) return AKMC_ESTATE;
+    if (j->bytes > s->cfg.budget_bytes) return AKMC_EINVAL;
+    j->ticket = s->next_ticket++;
+    j->res.submit_s = s->now();
+    s->jobs[j->ticket] = j;
+    s->queue.push_back(j);
+    *ticket = j->ticket;
+  }
+  s->cv_work.notify_one();
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_poll(akmc_server* s, int64_t ticket, akmc_job_result* res, uint8_t* occ_out,
+                                      int64_t n_sites, int32_t* ready) {
+  if (!s || !ready) return AKMC_EINVAL;
+  *ready = 0;
+  std::lock_guard<std::mutex> lk(s->m);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return AKMC_ENOTFOUND;
+  auto j = it->second;
+  if (j->state != 2) return AKMC_OK;
+  if (occ_out && n_sites != static_cast<int64_t>(j->occ.size())) return AKMC_EINVAL;
+  collect(s, j, res, occ_out, n_sites);
+  *ready = 1;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_wait(akmc_server* s, int64_t ticket, double timeout_s, akmc_job_result* res,
+                                      uint8_t* occ_out, int64_t n_sites) {
+  if (!s) return AKMC_EINVAL;
+  std::unique_lock<std::mutex> lk(s->m);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return AKMC_ENOTFOUND;
+  auto j = it->second;
+  if (occ_out && n_sites != static_cast<int64_t>(j->occ.size())) return AKMC_EINVAL;
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(std::max(0.0, timeout_s)),
+                                      [&] { return j->state == 2; });
+  if (!ok) return AKMC_ETIMEOUT;
+  collect(s, j, res, occ_out, n_sites);
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_stats(akmc_server* s, int64_t* queued, int64_t* running, int64_t* done) {
+  if (!s) return AKMC_EINVAL;
+  std::lock_guard<std::mutex> lk(s->m);
+  int64_t d = 0;
+  for (auto& kv : s->jobs) d += kv.second->state == 2 ? 1 : 0;
+  if (queued) *queued = static_cast<int64_t>(s->queue.size());
+  if (running) *running = s->running;
+  if (done) *done = d;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_shutdown(akmc_server* s) {
+  if (!s) return AKMC_EINVAL;
+  {
+    std::lock_guard<std::mutex> lk(s->m);
+    s->stopping = true;
+    for (auto& j : s->queue) {
+      j->state = 2;
+      j->res.status = AKMC_ESTATE;
+    }
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->lanes) t.join();  // running batches finish first
+  delete s;
+  return AKMC_OK;
+}
+
+}  // extern "C"

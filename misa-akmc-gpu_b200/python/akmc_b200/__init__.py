@@ -131,6 +131,29 @@ class ContextConfig(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("lanes", C.c_int32),
+        ("budget_bytes", C.c_int64),
+        ("max_batch_jobs", C.c_int32),
+        ("chunk_rounds", C.c_int32),
+    ]
+
+
+class JobResult(C.Structure):
+    _fields_ = [
+        ("hops", C.c_int64),
+        ("rounds", C.c_int64),
+        ("submit_s", C.c_double),
+        ("start_s", C.c_double),
+        ("finish_s", C.c_double),
+        ("status", C.c_int32),
+        ("n_blocks", C.c_int32),
+        ("error", C.c_char * 128),
+    ]
+
+
 class RunConfig(C.Structure):
     _fields_ = [
         ("box", C.c_int64 * 3),
@@ -180,6 +203,7 @@ SIGNATURES = {
     "akmc_run_rounds": (C.c_int, [_vp, _i64]),
     "akmc_run_rounds_noalloc": (C.c_int, [_vp, _i64]),
     "akmc_set_round_schedule": (C.c_int, [_vp, _i32]),
+    "akmc_get_round_schedule": (C.c_int, [_vp, C.POINTER(_i32)]),
     "akmc_run": (C.c_int, [_vp, _i64]),
     "akmc_sync": (C.c_int, [_vp]),
     "akmc_stream": (_vp, [_vp]),
@@ -192,10 +216,18 @@ SIGNATURES = {
     "akmc_get_counters": (C.c_int, [_vp, _vp]),
     "akmc_calculate": (C.c_int, [_vp, _i32, _i32, C.POINTER(_d)]),
     "akmc_select_and_perform": (C.c_int, [_vp, _i32, _i32, _d, C.POINTER(Event)]),
+    "akmc_get_calculated_rates": (C.c_int, [_vp, _vp, _vp, _vp, _i64, C.POINTER(_i64)]),
     "akmc_eam_johnson": (C.c_int, [_u64, _d, _d, C.POINTER(EamTables)]),
     "akmc_create_lattice": (C.c_int, [_vp, _vp, _vp, _i64, _u64, _vp, _i64]),
     "akmc_cluster_stats": (C.c_int, [_vp, _vp, C.POINTER(_i64), _vp, _i64]),
+    "akmc_job_cluster_stats": (C.c_int, [_vp, _i32, C.POINTER(_i64), _vp, _i64]),
     "akmc_device_math": (C.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "akmc_server_create": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "akmc_server_submit": (C.c_int, [_vp, _vp, _vp, _i64, C.POINTER(_i64)]),
+    "akmc_server_poll": (C.c_int, [_vp, _i64, _vp, _vp, _i64, C.POINTER(_i32)]),
+    "akmc_server_wait": (C.c_int, [_vp, _i64, _d, _vp, _vp, _i64]),
+    "akmc_server_stats": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "akmc_server_shutdown": (C.c_int, [_vp]),
     "akmc_load_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_get_phase_cycles": (C.c_int, [_vp, _vp]),
     "akmc_set_kernel_timing": (C.c_int, [_vp, _i32]),
@@ -389,6 +421,12 @@ class Engine:
         """SCHEDULE_AUTO, SCHEDULE_ROUNDS (round by round) or SCHEDULE_FLOW (dependency-driven)."""
         self._ck(lib().akmc_set_round_schedule(self.h, schedule))
 
+    def round_schedule(self):
+        """The schedule run_rounds uses: SCHEDULE_ROUNDS or SCHEDULE_FLOW."""
+        v = _i32(0)
+        self._ck(lib().akmc_get_round_schedule(self.h, C.byref(v)))
+        return v.value
+
     def run(self, max_rounds=0):
         self._ck(lib().akmc_run(self.h, max_rounds))
 
@@ -454,10 +492,28 @@ class Engine:
         self._ck(lib().akmc_get_kernel_timing(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def cluster_stats(self, job=0, hist_len=64):
+        """(isolated-Cu count, Cu cluster-size histogram) of the job's lattice, on the device."""
+        iso = C.c_int64(0)
+        hist = np.zeros(hist_len, np.int64)
+        self._ck(lib().akmc_job_cluster_stats(self.h, job, C.byref(iso), _ptr(hist), hist_len))
+        return int(iso.value), hist
+
     def calculate(self, job, sector_id):
         t = C.c_double(0.0)
         self._ck(lib().akmc_calculate(self.h, job, sector_id, C.byref(t)))
         return t.value
+
+    def calculated_rates(self, capacity=MAX_SECTOR_VACANCIES):
+        """(sites int32[n], delta_e float64[n, 8] in eV, rates float64[n, 8] in Hz) of the
+        jumps behind the last calculate(), in the sector's list order."""
+        sites = np.empty(capacity, np.int32)
+        de = np.empty((capacity, 8), np.float64)
+        rates = np.empty((capacity, 8), np.float64)
+        n = C.c_int64(0)
+        self._ck(lib().akmc_get_calculated_rates(self.h, _ptr(sites), _ptr(de), _ptr(rates), capacity, C.byref(n)))
+        k = n.value
+        return sites[:k].copy(), de[:k].copy(), rates[:k].copy()
 
     def select_and_perform(self, job, sector_id, u):
         ev = Event()
@@ -478,3 +534,62 @@ class Engine:
         l = np.empty_like(x)
         self._ck(lib().akmc_device_math(self.h, _ptr(x), x.size, _ptr(e), _ptr(l)))
         return e, l
+
+
+def _result(r):
+    return dict(hops=r.hops, rounds=r.rounds, submit_s=r.submit_s, start_s=r.start_s, finish_s=r.finish_s,
+                status=r.status, n_blocks=r.n_blocks, error=r.error.decode(errors="replace"))
+
+
+class Server:
+    """akmc_server: queued jobs run in batches by worker lanes, results as each job ends."""
+
+    def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0):
+        cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds)
+        h = C.c_void_p()
+        _check(lib().akmc_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.sizes = {}
+
+    def submit(self, cfg, occ):
+        occ = np.ascontiguousarray(occ, np.uint8)
+        t = C.c_int64(0)
+        _check(lib().akmc_server_submit(self.h, C.byref(cfg), _ptr(occ), occ.size, C.byref(t)))
+        self.sizes[t.value] = occ.size
+        return t.value
+
+    def poll(self, ticket):
+        """(result, final lattice) once the job is done, else None."""
+        n = self.sizes.get(ticket, 0)
+        out = np.empty(n, np.uint8)
+        r = JobResult()
+        ready = C.c_int32(0)
+        _check(lib().akmc_server_poll(self.h, ticket, C.byref(r), _ptr(out), n, C.byref(ready)))
+        if not ready.value:
+            return None
+        self.sizes.pop(ticket, None)
+        return _result(r), out
+
+    def wait(self, ticket, timeout=60.0):
+        n = self.sizes.get(ticket, 0)
+        out = np.empty(n, np.uint8)
+        r = JobResult()
+        _check(lib().akmc_server_wait(self.h, ticket, timeout, C.byref(r), _ptr(out), n))
+        self.sizes.pop(ticket, None)
+        return _result(r), out
+
+    def stats(self):
+        q, r, d = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        _check(lib().akmc_server_stats(self.h, C.byref(q), C.byref(r), C.byref(d)))
+        return dict(queued=q.value, running=r.value, done=d.value)
+
+    def close(self):
+        if self.h:
+            lib().akmc_server_shutdown(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

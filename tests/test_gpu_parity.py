@@ -197,6 +197,37 @@ def test_per_hop_entry_points_follow_the_reference_loop(ak, model):
         assert np.array_equal(eng.occupancy(0), o.occupancy())
 
 
+@pytest.mark.parametrize("model,precision", [(po.MODEL_PAIRBOND, po.FP64), (po.MODEL_EAM, po.FP64),
+                                             (po.MODEL_EAM, po.FP32C)])
+def test_calculated_rates_match_oracle_jump_by_jump(ak, model, precision):
+    # every sector of a quaternary 20^3 box with 40 vacancies: each vacancy's 8 jumps
+    o = oracle_job(model=model, precision=precision, alloy=QUATERNARY, n_vacancies=40, seed=5)
+    with ak.Engine() as eng:
+        device_job(eng, o, (20, 20, 20), model=model, precision=precision, seed=5)
+        eng.prepare()
+        seen = 0
+        for sector in range(8):
+            total = eng.calculate(0, sector)
+            sites, de, rates = eng.calculated_rates()
+            want_total = 0.0
+            for i in np.argsort(sites, kind="stable"):  # the ordered total runs in site order
+                for b in range(8):
+                    want_total += float(rates[i, b])
+            assert total == want_total
+            for i, s in enumerate(sites):
+                assert s >= 0
+                avail, r, d = o.vacancy_rates(int(s))
+                assert np.array_equal(rates[i].view(np.uint64), r.view(np.uint64))
+                for b in range(8):
+                    if (avail >> b) & 1:
+                        assert de[i, b].view(np.uint64) == d[b].view(np.uint64)
+                    else:
+                        assert rates[i, b] == 0.0 and de[i, b] == 0.0
+                seen += 1
+            assert (total > 0.0) == (len(sites) > 0)
+        assert seen == 40
+
+
 def test_sector_overflow_is_reported(ak):
     # 200 vacancies in a 16^3 box: more than 64 in one sector
     o = oracle_job(box=(16, 16, 16), n_vacancies=600, model=po.MODEL_PAIRBOND, alloy=((po.FE, 1),))
