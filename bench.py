@@ -479,8 +479,7 @@ def main():
         eng.run_rounds(R)
         eng.sync()
         for j, o in enumerate(outs):
-            lib_occ = eng.occupancy(j)
-            o.numpy()[:] = lib_occ
+            eng.occupancy(j, out=o.numpy())
     sync_all()
     e_dt = time.perf_counter() - t0
     e1 = eng.counters()

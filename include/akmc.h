@@ -120,6 +120,9 @@ typedef struct akmc_context_config {
   void* stream;                /* cudaStream_t to run on; NULL: the context creates one */
   int64_t event_log_capacity;  /* 0: no event log */
   int64_t hop_cap_per_round;   /* per block and round; 0: 1e7 */
+  int64_t flow_sweep_limit;    /* AKMC_SCHEDULE_FLOW watchdog: sweeps per CTA and launch before
+                                  the launch gives up with AKMC_ETIMEOUT; 0: 2^24.  Rounds
+                                  already published stay complete; recover from a snapshot. */
 } akmc_context_config;
 
 typedef struct akmc_ctx akmc_ctx;
@@ -183,6 +186,8 @@ AKMC_API void* akmc_stream(akmc_ctx* ctx);
 AKMC_API akmc_status akmc_gpu_final(akmc_ctx* ctx);
 
 AKMC_API akmc_status akmc_get_job_state(akmc_ctx* ctx, int32_t job, akmc_job_state* st);
+/* Every job's state with one device read; n_jobs must be the context's job count. */
+AKMC_API akmc_status akmc_get_job_states(akmc_ctx* ctx, akmc_job_state* out, int32_t n_jobs);
 AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out, int64_t n_sites);
 AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int64_t n_sites);
 /* evo[nblocks][8]: per-sector evolution time (SectorMeta, sublattice.h:17-33); hops[nblocks]. */
@@ -204,8 +209,20 @@ AKMC_API akmc_status akmc_get_phase_cycles(akmc_ctx* ctx, int64_t* out16);
 /* Replaces the lattice of a prepared job (same box and vacancy count) and
  * restarts it: density cache rebuilt on the device, clocks, rounds and RNG
  * streams reset as after akmc_prepare.  gpu_prepare's lattice upload
- * (gpu_simulate.hip:1771-1831) for a new box. */
+ * (gpu_simulate.hip:1771-1831) for a new box.  Asynchronous on the context's
+ * stream: from pinned memory, occ must stay unchanged until the stream is
+ * synchronised, and a lattice with another vacancy count is reported
+ * (AKMC_EINVAL) by the next synchronising call. */
 AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8_t* occ, int64_t n_sites);
+
+/* Restart snapshots.  The reference's restart is a stub (pkmc.cpp:183-184); this one holds
+ * a job's lattice, its rounds, hop counts, sector clocks and random streams per block, in a
+ * versioned byte buffer with a checksum.  Restored into a job added with the same
+ * configuration and potential (checked) and prepared, the run continues exactly as the
+ * uninterrupted one: same events, clocks and lattice.  Save between runs; it synchronises. */
+AKMC_API akmc_status akmc_snapshot_size(akmc_ctx* ctx, int32_t job, int64_t* bytes);
+AKMC_API akmc_status akmc_save_snapshot(akmc_ctx* ctx, int32_t job, uint8_t* buf, int64_t capacity, int64_t* written);
+AKMC_API akmc_status akmc_restore_snapshot(akmc_ctx* ctx, int32_t job, const uint8_t* buf, int64_t n);
 
 /* Kernel timing mode: while enabled, akmc_run_rounds launches each round on its
  * own (no CUDA graph) with CUDA events around the hop kernel on the context

@@ -136,6 +136,8 @@ akmc_status check_status(akmc_ctx* ctx) {
   if (st & kErrHopCap) return fail(ctx, AKMC_ERANGE, "a block exceeded the hop cap of one round");
   if (st & kErrLogOverflow) return fail(ctx, AKMC_EOVERFLOW, "event log full");
   if (st & kErrTimeout) return fail(ctx, AKMC_ETIMEOUT, "a bounded device wait or loop gave up");
+  if (st & kErrVacCount)
+    return fail(ctx, AKMC_EINVAL, "a lattice given to akmc_load_occupancy does not hold its job's vacancy count");
   return fail(ctx, AKMC_ESTATE, "device reported status " + std::to_string(st));
 }
 
@@ -204,6 +206,42 @@ int region_sites(const HostJob& j) {
   return static_cast<int>(mx);
 }
 
+// Restart snapshot layout: SnapHeader, then one SnapBlock per domain block, then the
+// occupancy bytes.  All fields little-endian, as the host writes them.
+struct SnapHeader {
+  char magic[8];  // "AKMCSNAP"
+  uint32_t version, header_bytes;
+  int64_t box[3];
+  int32_t blocks[3];
+  int32_t model, precision, rng;
+  double lattice_const, cutoff, attempt_freq, temperature, window;
+  uint64_t seed, eam_hash;
+  int64_t round, hops;
+  int32_t done, nblocks;
+  int64_t nsites, nvac;
+  uint64_t checksum;  // FNV-1a 64 of every byte after the header
+};
+struct SnapBlock {
+  int64_t round, hops;
+  double evo[8];
+  uint64_t xs[4], xt[4];
+  int32_t done, pad;
+};
+constexpr uint32_t kSnapVersion = 1;
+
+uint64_t fnv1a(const uint8_t* p, size_t n, uint64_t h = 1469598103934665603ull) {
+  for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
+  return h;
+}
+
+uint64_t eam_hash(const HostJob& j) {
+  return j.has_eam ? fnv1a(reinterpret_cast<const uint8_t*>(&j.eam), sizeof(j.eam)) : 0;
+}
+
+int64_t snapshot_bytes(const HostJob& j) {
+  return static_cast<int64_t>(sizeof(SnapHeader)) + j.nblocks * static_cast<int64_t>(sizeof(SnapBlock)) + j.nsites;
+}
+
 }  // namespace
 
 extern "C" {
@@ -247,6 +285,7 @@ AKMC_API akmc_status akmc_create(const akmc_context_config* cfg, akmc_ctx** out)
   if (cfg) ctx->cfg = *cfg;
   if (ctx->cfg.graph_rounds <= 0) ctx->cfg.graph_rounds = 32;
   if (ctx->cfg.hop_cap_per_round <= 0) ctx->cfg.hop_cap_per_round = 10000000;
+  if (ctx->cfg.flow_sweep_limit <= 0) ctx->cfg.flow_sweep_limit = int64_t(1) << 24;
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) {
     delete ctx;
     return AKMC_ECUDA;
@@ -377,8 +416,10 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device));
   int smem_sm = 0;
   CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
-  // 256-thread CTAs at <= 128 registers: at most two per SM
-  int per_sm = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
+  // k_hop: one CTA resident per SM (its register use); a second wave where two staged regions
+  // (plus the 1 KB the SM reserves per CTA) fit takes over as CTAs finish.  k_flow is
+  // persistent: one CTA per SM.  (Two per SM, at 96 registers, measured slower.)
+  const int per_sm = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
   ctx->hop_grid = std::max(1, std::min(nb, sms * per_sm));
   ctx->flow_grid = std::max(1, std::min(nb, sms));
 
@@ -567,6 +608,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.status = ctx->d_status;
   a.counters = ctx->d_counters;
   a.hop_cap = ctx->cfg.hop_cap_per_round;
+  a.flow_sweep_limit = ctx->cfg.flow_sweep_limit;
   a.api_job = -1;
   a.api_sector = -1;
   a.api_total = ctx->d_api_total;
@@ -597,9 +639,8 @@ AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8
   if (n_sites != j.nsites) return fail(ctx, AKMC_EINVAL, "n_sites does not match the job");
   CK(cudaSetDevice(ctx->cfg.device));
   CK(cudaMemcpyAsync(j.d_occ, occ, static_cast<size_t>(n_sites), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_vac_count, 0, 4, ctx->stream));
   int e = launch_collect_vacancies(j.d_occ, n_sites, ctx->d_vac_site + j.vac0, ctx->d_vac_job + j.vac0, job,
-                                   static_cast<int32_t>(j.nvac), ctx->d_vac_count, ctx->stream);
+                                   static_cast<int32_t>(j.nvac), ctx->d_vac_count, ctx->d_status, ctx->stream);
   if (e) return fail(ctx, AKMC_ECUDA, std::string("collect vacancies: ") + cuda_name(e));
   if (j.has_eam) {
     e = launch_init_rho(j.d_occ, j.d_rho, 2 * static_cast<int32_t>(j.cfg.box[0]), static_cast<int32_t>(j.cfg.box[1]),
@@ -611,13 +652,126 @@ AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8
                      ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_blocks + j.block0, &ctx->h_blocks[static_cast<size_t>(j.block0)],
                      static_cast<size_t>(j.nblocks) * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
-  int32_t count = 0;
-  CK(cudaMemcpyAsync(&count, ctx->d_vac_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  if (count != j.nvac)
-    return fail(ctx, AKMC_EINVAL, "the lattice must hold the job's " + std::to_string(j.nvac) + " vacancies, found " +
-                                      std::to_string(count));
+  return AKMC_OK;  // a wrong vacancy count is reported by the next synchronising call
+}
+
+AKMC_API akmc_status akmc_snapshot_size(akmc_ctx* ctx, int32_t job, int64_t* bytes) {
+  if (!ctx || !bytes) return AKMC_EINVAL;
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  *bytes = snapshot_bytes(ctx->jobs[static_cast<size_t>(job)]);
   return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_save_snapshot(akmc_ctx* ctx, int32_t job, uint8_t* buf, int64_t capacity, int64_t* written) {
+  if (!ctx || !buf || !written) return AKMC_EINVAL;
+  *written = 0;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  const int64_t need = snapshot_bytes(j);
+  if (capacity < need) return fail(ctx, AKMC_EINVAL, "snapshot needs " + std::to_string(need) + " bytes");
+  CK(cudaSetDevice(ctx->cfg.device));
+  JobDev J;
+  std::vector<BlockDev> B(static_cast<size_t>(j.nblocks));
+  uint8_t* occ = buf + sizeof(SnapHeader) + j.nblocks * sizeof(SnapBlock);
+  CK(cudaMemcpyAsync(&J, ctx->d_jobs + job, sizeof(J), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(B.data(), ctx->d_blocks + j.block0, B.size() * sizeof(BlockDev), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(occ, j.d_occ, static_cast<size_t>(j.nsites), cudaMemcpyDeviceToHost, ctx->stream));
+  const akmc_status st = akmc_sync(ctx);  // also the last run's errors
+  if (st != AKMC_OK) return st;
+  for (int32_t b = 0; b < j.nblocks; ++b) {
+    SnapBlock r{};
+    r.round = B[static_cast<size_t>(b)].round;
+    r.hops = B[static_cast<size_t>(b)].hops;
+    for (int k = 0; k < 8; ++k) r.evo[k] = B[static_cast<size_t>(b)].evo[k];
+    for (int k = 0; k < 4; ++k) {
+      r.xs[k] = B[static_cast<size_t>(b)].xs[k];
+      r.xt[k] = B[static_cast<size_t>(b)].xt[k];
+    }
+    r.done = B[static_cast<size_t>(b)].done;
+    std::memcpy(buf + sizeof(SnapHeader) + b * sizeof(SnapBlock), &r, sizeof(r));
+  }
+  SnapHeader h{};
+  std::memcpy(h.magic, "AKMCSNAP", 8);
+  h.version = kSnapVersion;
+  h.header_bytes = sizeof(SnapHeader);
+  for (int d = 0; d < 3; ++d) {
+    h.box[d] = j.cfg.box[d];
+    h.blocks[d] = j.cfg.blocks[d] > 0 ? j.cfg.blocks[d] : 1;
+  }
+  h.model = j.cfg.energy_model;
+  h.precision = j.cfg.precision;
+  h.rng = j.cfg.rng;
+  h.lattice_const = j.cfg.lattice_const;
+  h.cutoff = j.cfg.cutoff_radius;
+  h.attempt_freq = j.cfg.attempt_freq;
+  h.temperature = j.cfg.temperature;
+  h.window = j.cfg.sector_window;
+  h.seed = j.cfg.seed;
+  h.eam_hash = eam_hash(j);
+  h.round = J.round;
+  h.hops = J.hops;
+  h.done = J.done;
+  h.nblocks = j.nblocks;
+  h.nsites = j.nsites;
+  h.nvac = j.nvac;
+  h.checksum = fnv1a(buf + sizeof(SnapHeader), static_cast<size_t>(need) - sizeof(SnapHeader));
+  std::memcpy(buf, &h, sizeof(h));
+  *written = need;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_restore_snapshot(akmc_ctx* ctx, int32_t job, const uint8_t* buf, int64_t n) {
+  if (!ctx || !buf) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
+  SnapHeader h{};
+  if (n < static_cast<int64_t>(sizeof(h))) return fail(ctx, AKMC_EINVAL, "not a snapshot: too short");
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, "AKMCSNAP", 8) != 0 || h.header_bytes != sizeof(SnapHeader))
+    return fail(ctx, AKMC_EINVAL, "not a snapshot");
+  if (h.version != kSnapVersion) return fail(ctx, AKMC_EINVAL, "snapshot version " + std::to_string(h.version));
+  if (n != snapshot_bytes(j) || h.nsites != j.nsites || h.nblocks != j.nblocks || h.nvac != j.nvac)
+    return fail(ctx, AKMC_EINVAL, "snapshot of a job of another size");
+  bool same = h.model == j.cfg.energy_model && h.precision == j.cfg.precision && h.rng == j.cfg.rng &&
+              h.lattice_const == j.cfg.lattice_const && h.cutoff == j.cfg.cutoff_radius &&
+              h.attempt_freq == j.cfg.attempt_freq && h.temperature == j.cfg.temperature &&
+              h.window == j.cfg.sector_window && h.eam_hash == eam_hash(j);
+  for (int d = 0; d < 3; ++d)
+    same = same && h.box[d] == j.cfg.box[d] && h.blocks[d] == (j.cfg.blocks[d] > 0 ? j.cfg.blocks[d] : 1);
+  if (!same) return fail(ctx, AKMC_EINVAL, "snapshot of another job configuration or potential");
+  if (fnv1a(buf + sizeof(h), static_cast<size_t>(n) - sizeof(h)) != h.checksum)
+    return fail(ctx, AKMC_EINVAL, "snapshot checksum mismatch");
+  const uint8_t* occ = buf + sizeof(h) + j.nblocks * sizeof(SnapBlock);
+  // the lattice, its vacancy table and density cache, and the initial records ...
+  akmc_status st = akmc_load_occupancy(ctx, job, occ, j.nsites);
+  if (st != AKMC_OK) return st;
+  // ... then the saved counters, clocks and random streams over them
+  JobDev J = ctx->h_jobs[static_cast<size_t>(job)];
+  J.round = h.round;
+  J.hops = h.hops;
+  J.done = h.done;
+  std::vector<BlockDev> B(ctx->h_blocks.begin() + j.block0, ctx->h_blocks.begin() + j.block0 + j.nblocks);
+  for (int32_t b = 0; b < j.nblocks; ++b) {
+    SnapBlock r;
+    std::memcpy(&r, buf + sizeof(h) + b * sizeof(SnapBlock), sizeof(r));
+    BlockDev& d = B[static_cast<size_t>(b)];
+    d.round = r.round;
+    d.hops = r.hops;
+    for (int k = 0; k < 8; ++k) d.evo[k] = r.evo[k];
+    for (int k = 0; k < 4; ++k) {
+      d.xs[k] = r.xs[k];
+      d.xt[k] = r.xt[k];
+    }
+    d.done = r.done;
+    d.cnt = 0;
+  }
+  CK(cudaMemcpyAsync(ctx->d_jobs + job, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks + j.block0, B.data(), B.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  return akmc_sync(ctx);  // B and J leave scope; also reports a lattice with a wrong vacancy count
 }
 
 AKMC_API akmc_status akmc_set_kernel_timing(akmc_ctx* ctx, int32_t enable) {
@@ -834,6 +988,33 @@ AKMC_API akmc_status akmc_get_job_state(akmc_ctx* ctx, int32_t job, akmc_job_sta
   st->round = J.round;
   st->hops = J.hops;
   st->done = J.done;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_get_job_states(akmc_ctx* ctx, akmc_job_state* out, int32_t n_jobs) {
+  if (!ctx || (!out && n_jobs > 0)) return AKMC_EINVAL;
+  if (n_jobs != static_cast<int32_t>(ctx->jobs.size()))
+    return fail(ctx, AKMC_EINVAL, "n_jobs must equal the context's job count");
+  if (n_jobs == 0) return AKMC_OK;
+  std::vector<JobDev> J(static_cast<size_t>(n_jobs));
+  if (ctx->prepared) {
+    CK(cudaSetDevice(ctx->cfg.device));
+    CK(cudaMemcpyAsync(J.data(), ctx->d_jobs, J.size() * sizeof(JobDev), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  for (int32_t k = 0; k < n_jobs; ++k) {
+    const HostJob& j = ctx->jobs[static_cast<size_t>(k)];
+    akmc_job_state& st = out[k];
+    std::memset(&st, 0, sizeof(st));
+    st.n_blocks = j.nblocks;
+    st.n_sites = j.nsites;
+    st.n_vacancies = j.nvac;
+    if (ctx->prepared) {
+      st.round = J[static_cast<size_t>(k)].round;
+      st.hops = J[static_cast<size_t>(k)].hops;
+      st.done = J[static_cast<size_t>(k)].done;
+    }
+  }
   return AKMC_OK;
 }
 

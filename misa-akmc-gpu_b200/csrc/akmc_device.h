@@ -94,6 +94,7 @@ enum : uint32_t {
   kErrLogOverflow = 8u,
   kErrApiState = 16u,
   kErrTimeout = 32u,
+  kErrVacCount = 64u,  // a loaded lattice does not hold its job's vacancy count
 };
 
 enum : int32_t { kModeRound = 0, kModeCalc = 1, kModeSelectPerform = 2 };
@@ -128,6 +129,7 @@ struct RoundArgs {
   int32_t* flow_need;           // per energy kind: blocks with rounds to run in this launch
   int32_t* flow_done;           // per energy kind: blocks that reached their target
   int64_t flow_rounds;          // rounds this launch adds to every unfinished block
+  int64_t flow_sweep_limit;     // sweeps per CTA before the launch gives up (kErrTimeout)
   // per-hop entry points
   int32_t api_job, api_sector;
   double api_u;
@@ -144,8 +146,10 @@ size_t hop_smem_bytes(int max_region_sites);
 int configure_hop_smem(size_t smem);
 // ev0/ev1 (cudaEvent_t or null) are recorded around the hop kernel.
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1);
+// Collects the vacancies of one job's lattice into its slice of the vacancy table and sets
+// kErrVacCount in *status unless exactly cap were found.
 int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
-                             int32_t cap, int32_t* count, void* stream);
+                             int32_t cap, int32_t* count, unsigned int* status, void* stream);
 int launch_api(const RoundArgs& a, size_t smem, void* stream);
 int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, const Potential* pot,
                     const Geometry* geo, unsigned int* status, void* stream);

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <algorithm>
 #include <cstdint>
 
 #include "akmc_device.h"
@@ -25,6 +26,8 @@ namespace akmc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStageRows = 4;  // rows of the staged region each warp has in flight
+enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };  // energy kinds, one kernel instance each
 constexpr int kThreads = 288;  // warps 0..7 evaluate jump directions 0..7; warp 8 controls
 constexpr int kCtl = 256;      // control thread: first lane of warp 8
 
@@ -66,8 +69,10 @@ __device__ __forceinline__ void make_region(const BlockDev& B, int sec, Region& 
 // Shared-memory working set of one CTA (followed by the staged region).
 struct Smem {
   double b1[25], b2[25];
-  double dphi64[4 * 4 * 64];    // phi_XY(shell s) - phi_XY(shell t), index (X*4+Y)*64 + s*8 + t
-  float dphi32[4 * 4 * 64];
+  union {                       // phi_XY(shell s) - phi_XY(shell t), index (X*4+Y)*64 + s*8 + t,
+    double dphi64[4 * 4 * 64];  // in the precision of the kernel's kind
+    float dphi32[4 * 4 * 64];
+  };
   int32_t dfq[4 * 64];          // f_X(shell s) - f_X(shell t) in Q.24, index X*64 + s*8 + t
   int32_t fq1[4];               // f_X at the first shell
   int32_t d1[2][8];             // 1nn local offsets by x parity
@@ -87,6 +92,7 @@ struct Smem {
   alignas(8) uint64_t mbar;                    // completion barrier of the window's bulk copy
   uint32_t mbar_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
+  int32_t tab_key[2];                          // potential, kind and region strides the tables hold
   // hop-loop control, written by thread 0 between barriers
   double pre[kMaxV * 8];   // running sums of the ordered rates
   double ctl_u, ctl_unext, ctl_expected;
@@ -188,7 +194,8 @@ __device__ __forceinline__ double* fcache_of(int32_t* rho_s, int nreg) {
                                    ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15)));
 }
 
-__device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, const Region& R, bool eam) {
+__device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, const Region& R, int kind) {
+  const bool eam = kind != kPairBond;
   const int tid = threadIdx.x;
   if (tid < 25) {
     sm.b1[tid] = P.b1[tid / 5][tid % 5];
@@ -206,8 +213,8 @@ __device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, con
       const int xy = i >> 6, hs = (i >> 3) & 7, ht = i & 7;
       const double* ph = &P.phi64[0][0][0] + xy * 8;
       const float* pf = &P.phi32[0][0][0] + xy * 8;
-      sm.dphi64[i] = ph[hs] - ph[ht];
-      sm.dphi32[i] = pf[hs] - pf[ht];
+      if (kind == kEam64) sm.dphi64[i] = ph[hs] - ph[ht];
+      else sm.dphi32[i] = pf[hs] - pf[ht];
       if (i < 4 * 64) sm.dfq[i] = P.fq[i >> 6][hs] - P.fq[i >> 6][ht];
     }
     for (int i = tid; i < 2 * 8 * kJumpN; i += kThreads) {
@@ -273,8 +280,6 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
   c.pad0 = c.pad1 = c.pad2 = 0.f;
   return c;
 }
-
-enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };
 
 // Rates of vacancy k, all 8 jumps, CTA-collective (no barrier inside; the caller
 // synchronises before the rates are read).  Warp b evaluates jump b.
@@ -457,7 +462,11 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   // F-table window: one bulk copy issued by the control thread, overlapped with the staging
   const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
   const bool need_win = eam && sm.win_pot != win_key;
-  __syncthreads();  // every thread has read win_pot; the previous item's readers are done
+  // the shell tables and neighbour lists depend on the potential, the kind and the region's
+  // row strides only: kept from the CTA's previous block when those match
+  const int tab0 = J.pot * 4 + KIND, tab1 = R.LX | (R.LY << 16);
+  const bool need_tab = sm.tab_key[0] != tab0 || sm.tab_key[1] != tab1;
+  __syncthreads();  // every thread has read win_pot and tab_key; the previous item's readers are done
   if (need_win && tid == kCtl) {
     if (KIND == kEam32) {
       bulk_expect(&sm.mbar, kFWin * 20u);
@@ -469,7 +478,13 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       bulk_copy(sm.fwin + kFWin * 16, P.F64hi + P.fwin0, kFWin * 16u, &sm.mbar);
     }
   }
-  load_tables(sm, P, *a.geo, R, eam);
+  if (need_tab) {
+    load_tables(sm, P, *a.geo, R, KIND);
+    if (tid == 0) {
+      sm.tab_key[0] = tab0;
+      sm.tab_key[1] = tab1;
+    }
+  }
   FTab FT;
   FT.win = sm.fwin;
   FT.kw0 = P.fwin0;
@@ -481,18 +496,18 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   FT.prof = a.counters + 16;
   FT.fc = fcache_of(rho_s, R.n);
 
-  // stage the region: warp w takes rows w, w+9, ...; four rows of loads are issued
+  // stage the region: warp w takes rows w, w+9, ...; kStageRows rows of loads are issued
   // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
   {
     const int nrows = R.LY * R.LZ;
     const int gx0 = wrap1(R.ox + lane, jc.sx), gx1 = wrap1(R.ox + lane + 32, jc.sx);
     const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
     constexpr int kW = kThreads / 32;
-    for (int row0 = warp; row0 < nrows; row0 += 4 * kW) {
-      uint8_t ov[4][2];
-      int32_t rv[4][2];
+    for (int row0 = warp; row0 < nrows; row0 += kStageRows * kW) {
+      uint8_t ov[kStageRows][2];
+      int32_t rv[kStageRows][2];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < kStageRows; ++k) {
         const int row = row0 + kW * k;
         if (row < nrows) {
           const int ly = row % R.LY, lz = row / R.LY;
@@ -509,7 +524,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         }
       }
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < kStageRows; ++k) {
         const int row = row0 + kW * k;
         if (row < nrows) {
           const int l = lane + R.LX * row;
@@ -974,6 +989,7 @@ __device__ void init_cta_smem(uint8_t* smem) {
   Smem* sm = reinterpret_cast<Smem*>(smem);
   if (threadIdx.x == 0) {
     sm->win_pot = -1;
+    sm->tab_key[0] = sm->tab_key[1] = -1;
     sm->mbar_phase = 0;
     mbar_init(&sm->mbar);
     for (int i = 0; i < 6; ++i) sm->acc[i] = 0;
@@ -1260,7 +1276,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
       const int done = *reinterpret_cast<volatile int*>(&a.flow_done[KIND]);
       const unsigned st = *reinterpret_cast<volatile unsigned*>(a.status);
       int stop = done >= need || (st & (kErrVacOverflow | kErrRhoRange | kErrHopCap | kErrTimeout)) != 0;
-      if (!stop && sweep >= (1ll << 24)) {  // bounded: no launch of <= 1024 rounds needs this many
+      if (!stop && sweep >= a.flow_sweep_limit) {  // watchdog; the default 2^24 no launch of <= 1024 rounds needs
         atomicOr(a.status, kErrTimeout);
         stop = 1;
       }
@@ -1523,27 +1539,57 @@ __global__ void k_api_reset(RoundArgs a) {
   *a.n_active = 0;
 }
 
-__global__ void k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz,
-                           const Potential* pot, const Geometry* geo) {
-  const int64_t n = static_cast<int64_t>(sx) * sy * sz;
-  for (int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; s < n;
-       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int X = static_cast<int>(s % sx);
-    const int64_t t = s / sx;
-    const int y = static_cast<int>(t % sy);
-    const int z = static_cast<int>(t / sy);
-    const int p = X & 1;
-    int32_t acc = 0;
-    for (int i = 0; i < kShellNb; ++i) {
-      const int32_t w = geo->nbr[p][i];
-      int gx = X + unpack_dx(w), gy = y + unpack_dy(w), gz = z + unpack_dz(w);
-      gx = gx < 0 ? gx + sx : (gx >= sx ? gx - sx : gx);
-      gy = gy < 0 ? gy + sy : (gy >= sy ? gy - sy : gy);
-      gz = gz < 0 ? gz + sz : (gz >= sz ? gz - sz : gz);
-      const uint8_t o = occ[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)];
-      if (o != kV) acc += pot->fq[species_index(o)][unpack_sh_s(w)];
+// Density cache of a whole lattice: rho_i = sum over the 58 neighbours j within the cutoff of
+// f_{X_j}(shell) in Q.24.  A CTA takes tiles of 32 x 8 x 4 sites (x doubled), stages each with
+// its halo (4 sites in x, 2 in y and z, periodic) in shared memory together with the shell
+// offsets and the f table by occupancy code, and sums from there.  The sums are exact
+// integers, so the order of the terms does not matter.
+constexpr int kRhoTX = 32, kRhoTY = 8, kRhoTZ = 4, kRhoHX = 4, kRhoHY = 2, kRhoHZ = 2;
+constexpr int kRhoLX = kRhoTX + 2 * kRhoHX, kRhoLY = kRhoTY + 2 * kRhoHY, kRhoLZ = kRhoTZ + 2 * kRhoHZ;
+
+__global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy,
+                                                  int32_t sz, const Potential* pot, const Geometry* geo) {
+  __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
+  __shared__ int32_t nbo[2][kShellNb], nbs[2][kShellNb];  // local offset and shell per x parity
+  __shared__ int32_t fqc[16][8];                           // f in Q.24 by occupancy code; V and others 0
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 16 * 8; i += blockDim.x) {
+    const int code = i >> 3;
+    const bool atom = code == 1 || code == 2 || code == 4 || code == 8;
+    fqc[code][i & 7] = atom ? pot->fq[species_index(static_cast<uint8_t>(code))][i & 7] : 0;
+  }
+  for (int i = tid; i < 2 * kShellNb; i += blockDim.x) {
+    const int32_t w = geo->nbr[i / kShellNb][i % kShellNb];
+    nbo[i / kShellNb][i % kShellNb] = unpack_dx(w) + kRhoLX * (unpack_dy(w) + kRhoLY * unpack_dz(w));
+    nbs[i / kShellNb][i % kShellNb] = unpack_sh_s(w);
+  }
+  const int nx = (sx + kRhoTX - 1) / kRhoTX, ny = (sy + kRhoTY - 1) / kRhoTY, nz = (sz + kRhoTZ - 1) / kRhoTZ;
+  const int64_t ntiles = static_cast<int64_t>(nx) * ny * nz;
+  for (int64_t tix = blockIdx.x; tix < ntiles; tix += gridDim.x) {
+    const int x0 = static_cast<int>(tix % nx) * kRhoTX;
+    const int y0 = static_cast<int>((tix / nx) % ny) * kRhoTY;
+    const int z0 = static_cast<int>(tix / (static_cast<int64_t>(nx) * ny)) * kRhoTZ;
+    __syncthreads();  // tables written; the previous tile's readers are done
+    for (int i = tid; i < kRhoLX * kRhoLY * kRhoLZ; i += blockDim.x) {
+      const int lx = i % kRhoLX, t = i / kRhoLX, ly = t % kRhoLY, lz = t / kRhoLY;
+      int gx = (x0 - kRhoHX + lx) % sx, gy = (y0 - kRhoHY + ly) % sy, gz = (z0 - kRhoHZ + lz) % sz;
+      gx += gx < 0 ? sx : 0;
+      gy += gy < 0 ? sy : 0;
+      gz += gz < 0 ? sz : 0;
+      tile[i] = __ldg(occ + gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz));
     }
-    rho[s] = acc;
+    __syncthreads();
+    for (int k = tid; k < kRhoTX * kRhoTY * kRhoTZ; k += blockDim.x) {
+      const int lx = k % kRhoTX, t = k / kRhoTX, ly = t % kRhoTY, lz = t / kRhoTY;
+      const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+      if (gx >= sx || gy >= sy || gz >= sz) continue;
+      const int p = gx & 1;
+      const int c = (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
+      int32_t acc = 0;
+#pragma unroll 2
+      for (int i = 0; i < kShellNb; ++i) acc += fqc[tile[c + nbo[p][i]]][nbs[p][i]];
+      rho[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)] = acc;
+    }
   }
 }
 
@@ -1616,12 +1662,11 @@ int configure_hop_smem(size_t smem) {
     e = cudaFuncSetAttribute(k_hop<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_hop<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_flow<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_flow<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_flow<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  const void* flows[] = {reinterpret_cast<const void*>(k_flow<kEam64>),
+                         reinterpret_cast<const void*>(k_flow<kEam32>),
+                         reinterpret_cast<const void*>(k_flow<kPairBond>)};
+  for (const void* f : flows)
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
   e = cudaFuncSetAttribute(k_api_block, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   return static_cast<int>(e);
@@ -1631,19 +1676,25 @@ int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t 
                     const Geometry* geo, unsigned int* status, void* stream) {
   (void)status;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int64_t n = static_cast<int64_t>(sx) * sy * sz;
-  int64_t blocks = (n + 255) / 256;
-  if (blocks > 148 * 64) blocks = 148 * 64;
+  const int64_t ntiles = static_cast<int64_t>((sx + kRhoTX - 1) / kRhoTX) * ((sy + kRhoTY - 1) / kRhoTY) *
+                         ((sz + kRhoTZ - 1) / kRhoTZ);
+  const int64_t blocks = std::min<int64_t>(ntiles, 148 * 16);
   k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, pot, geo);
   return static_cast<int>(cudaGetLastError());
 }
 
+__global__ void k_check_vacancy_count(const int32_t* count, int32_t want, unsigned int* status) {
+  if (*count != want) atomicOr(status, kErrVacCount);
+}
+
 int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
-                             int32_t cap, int32_t* count, void* stream) {
+                             int32_t cap, int32_t* count, unsigned int* status, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int64_t blocks = (n + 255) / 256;
   if (blocks > 148 * 64) blocks = 148 * 64;
+  cudaMemsetAsync(count, 0, sizeof(int32_t), st);
   k_collect_vacancies<<<static_cast<int>(blocks), 256, 0, st>>>(occ, n, vac_site, vac_job, job, cap, count);
+  k_check_vacancy_count<<<1, 1, 0, st>>>(count, cap, status);
   return static_cast<int>(cudaGetLastError());
 }
 

@@ -1,10 +1,13 @@
 // akmc_server.cpp -- job server over the context API of include/akmc.h.
 //
-// Jobs queue in arrival order.  Each lane (a host thread with its own context, hence its
-// own CUDA stream) takes the queued jobs that fit the device-memory budget as one batch,
-// runs them together in chunks of rounds and publishes every job's result the moment that
-// job is done, so short jobs do not wait for the long ones of their batch.  Lanes overlap
-// on the GPU.  All shared state is under one mutex; the device work runs outside it.
+// Jobs queue in arrival order.  Each lane (a host thread with its own context, hence its own
+// CUDA stream) takes the queued jobs that fit the device-memory budget as one batch and runs
+// them together in chunks of rounds.  A job's result is published, and its memory returned to
+// the budget, as soon as that job is done.  When an eighth of a batch has finished and queued
+// jobs fit, the lane refills: the running jobs are saved as restart snapshots, the context is
+// rebuilt with them and the newly admitted jobs, and the snapshots are restored, so every
+// job's trajectory is exactly the one it has alone.  Lanes overlap on the GPU.  All shared
+// state is under one mutex; the device work runs outside it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -32,6 +35,7 @@ struct SJob {
   int state = 0;  // 0 queued, 1 running, 2 done
   akmc_job_result res{};
   std::vector<uint8_t> out;
+  std::vector<uint8_t> snap;  // restart snapshot while the job moves to a rebuilt context
 };
 
 // Device bytes a job holds: occupancy, density cache, block records and lists, vacancies.
@@ -60,93 +64,132 @@ struct akmc_server {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
 
+  // Under the lock: the job's result is final and its bytes go back to the budget.
   void publish(const std::shared_ptr<SJob>& j, int32_t status, akmc_ctx* ctx = nullptr) {
     char msg[sizeof(j->res.error)] = {0};
     if (status != AKMC_OK && ctx) akmc_last_error(ctx, msg, static_cast<int32_t>(sizeof(msg)));
-    std::lock_guard<std::mutex> lk(m);
-    j->res.status = status;
-    std::memcpy(j->res.error, msg, sizeof(msg));
-    j->res.finish_s = now();
-    j->state = 2;
-    --running;
+    {
+      std::lock_guard<std::mutex> lk(m);
+      j->res.status = status;
+      std::memcpy(j->res.error, msg, sizeof(msg));
+      j->res.finish_s = now();
+      j->state = 2;
+      j->snap.clear();
+      j->snap.shrink_to_fit();
+      --running;
+      held -= j->bytes;
+    }
     cv_done.notify_all();
+    cv_work.notify_all();
   }
 
-  void run_batch(std::vector<std::shared_ptr<SJob>>& batch) {
-    akmc_context_config cc{};
-    cc.device = cfg.device;
-    cc.graph_rounds = cfg.chunk_rounds;
-    akmc_ctx* ctx = nullptr;
-    akmc_status st = akmc_create(&cc, &ctx);
-    if (st != AKMC_OK) {
-      for (auto& j : batch) publish(j, st);
-      return;
+  bool fits_locked() const {
+    return !queue.empty() && held + queue.front()->bytes <= cfg.budget_bytes;
+  }
+
+  // Under the lock: moves queued jobs that fit into `live`.
+  void take_locked(std::vector<std::shared_ptr<SJob>>& live) {
+    while (fits_locked() && static_cast<int32_t>(live.size()) < cfg.max_batch_jobs) {
+      auto j = queue.front();
+      queue.pop_front();
+      j->state = 1;
+      j->res.start_s = now();
+      held += j->bytes;
+      ++running;
+      live.push_back(j);
     }
-    std::vector<std::pair<std::shared_ptr<SJob>, int32_t>> live;
-    for (auto& j : batch) {
-      akmc_job_config c = j->cfg;
-      c.eam = j->has_eam ? &j->eam : nullptr;
-      int32_t id = -1;
-      const akmc_status s = akmc_add_job(ctx, &c, j->occ.data(), static_cast<int64_t>(j->occ.size()), &id);
-      if (s != AKMC_OK) publish(j, s, ctx);
-      else live.emplace_back(j, id);
-    }
-    if (!live.empty()) st = akmc_prepare(ctx);
-    while (st == AKMC_OK && !live.empty()) {
-      st = akmc_run_rounds(ctx, cfg.chunk_rounds);
-      if (st == AKMC_OK) st = akmc_sync(ctx);
-      if (st != AKMC_OK) break;
-      for (size_t i = 0; i < live.size();) {
-        akmc_job_state js{};
-        st = akmc_get_job_state(ctx, live[i].second, &js);
-        if (st != AKMC_OK) break;
-        if (!js.done) {
-          ++i;
+  }
+
+  // Runs `live` until every job is done, refilling from the queue on the way.
+  void run_batch(std::vector<std::shared_ptr<SJob>>& live) {
+    while (!live.empty()) {
+      akmc_context_config cc{};
+      cc.device = cfg.device;
+      cc.graph_rounds = cfg.chunk_rounds;
+      akmc_ctx* ctx = nullptr;
+      akmc_status st = akmc_create(&cc, &ctx);
+      if (st != AKMC_OK) {
+        for (auto& j : live) publish(j, st);
+        live.clear();
+        return;
+      }
+      std::vector<std::shared_ptr<SJob>> in;  // jobs of this context, by job id
+      for (auto& j : live) {
+        akmc_job_config c = j->cfg;
+        c.eam = j->has_eam ? &j->eam : nullptr;
+        int32_t id = -1;
+        const akmc_status s = akmc_add_job(ctx, &c, j->occ.data(), static_cast<int64_t>(j->occ.size()), &id);
+        if (s != AKMC_OK) publish(j, s, ctx);
+        else in.push_back(j);
+      }
+      if (!in.empty()) st = akmc_prepare(ctx);
+      for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k)
+        if (!in[k]->snap.empty())
+          st = akmc_restore_snapshot(ctx, static_cast<int32_t>(k), in[k]->snap.data(),
+                                     static_cast<int64_t>(in[k]->snap.size()));
+      std::vector<bool> over(in.size(), false);
+      std::vector<akmc_job_state> js(in.size());
+      size_t left = in.size(), finished = 0;
+      const size_t refill_after = std::max<size_t>(1, in.size() / 8);
+      bool refill = false;
+      while (st == AKMC_OK && left > 0 && !refill) {
+        st = akmc_run_rounds(ctx, cfg.chunk_rounds);
+        if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(in.size()));
+        for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k) {
+          if (over[k] || !js[k].done) continue;
+          auto& j = in[k];
+          j->out.resize(j->occ.size());
+          st = akmc_get_occupancy(ctx, static_cast<int32_t>(k), j->out.data(), static_cast<int64_t>(j->out.size()));
+          if (st != AKMC_OK) break;
+          j->res.hops = js[k].hops;
+          j->res.rounds = js[k].round;
+          j->res.n_blocks = js[k].n_blocks;
+          publish(j, AKMC_OK);
+          over[k] = true;
+          --left;
+          ++finished;
+        }
+        if (st == AKMC_OK && left > 0 && finished >= refill_after) {
+          std::lock_guard<std::mutex> lk(m);
+          refill = !stopping && fits_locked() && static_cast<int32_t>(left) < cfg.max_batch_jobs;
+        }
+      }
+      live.clear();
+      for (size_t k = 0; k < in.size(); ++k) {
+        if (over[k]) continue;
+        if (st != AKMC_OK) {
+          publish(in[k], st, ctx);
           continue;
         }
-        auto& j = live[i].first;
-        j->out.resize(j->occ.size());
-        st = akmc_get_occupancy(ctx, live[i].second, j->out.data(), static_cast<int64_t>(j->out.size()));
-        if (st != AKMC_OK) break;
-        j->res.hops = js.hops;
-        j->res.rounds = js.round;
-        j->res.n_blocks = js.n_blocks;
-        publish(j, AKMC_OK);
-        live.erase(live.begin() + static_cast<long>(i));
+        // carried into the next context
+        int64_t n = 0;
+        st = akmc_snapshot_size(ctx, static_cast<int32_t>(k), &n);
+        if (st == AKMC_OK) {
+          in[k]->snap.resize(static_cast<size_t>(n));
+          int64_t w = 0;
+          st = akmc_save_snapshot(ctx, static_cast<int32_t>(k), in[k]->snap.data(), n, &w);
+        }
+        if (st != AKMC_OK) publish(in[k], st, ctx);
+        else live.push_back(in[k]);
+      }
+      akmc_destroy(ctx);
+      if (!live.empty()) {
+        std::lock_guard<std::mutex> lk(m);
+        take_locked(live);
       }
     }
-    for (auto& p : live) publish(p.first, st == AKMC_OK ? AKMC_ESTATE : st, ctx);
-    if (ctx) akmc_destroy(ctx);
   }
 
   void lane() {
     for (;;) {
-      std::vector<std::shared_ptr<SJob>> batch;
-      int64_t bytes = 0;
+      std::vector<std::shared_ptr<SJob>> live;
       {
         std::unique_lock<std::mutex> lk(m);
-        cv_work.wait(lk, [&] {
-          return stopping || (!queue.empty() && held + queue.front()->bytes <= cfg.budget_bytes);
-        });
+        cv_work.wait(lk, [&] { return stopping || fits_locked(); });
         if (stopping) return;
-        while (!queue.empty() && static_cast<int32_t>(batch.size()) < cfg.max_batch_jobs &&
-               held + bytes + queue.front()->bytes <= cfg.budget_bytes) {
-          auto j = queue.front();
-          queue.pop_front();
-          j->state = 1;
-          j->res.start_s = now();
-          bytes += j->bytes;
-          batch.push_back(j);
-        }
-        held += bytes;
-        running += static_cast<int64_t>(batch.size());
+        take_locked(live);
       }
-      run_batch(batch);
-      {
-        std::lock_guard<std::mutex> lk(m);
-        held -= bytes;
-      }
-      cv_work.notify_all();
+      run_batch(live);
     }
   }
 };

@@ -128,6 +128,7 @@ class ContextConfig(C.Structure):
         ("stream", C.c_void_p),
         ("event_log_capacity", C.c_int64),
         ("hop_cap_per_round", C.c_int64),
+        ("flow_sweep_limit", C.c_int64),
     ]
 
 
@@ -209,6 +210,7 @@ SIGNATURES = {
     "akmc_stream": (_vp, [_vp]),
     "akmc_gpu_final": (C.c_int, [_vp]),
     "akmc_get_job_state": (C.c_int, [_vp, _i32, C.POINTER(JobState)]),
+    "akmc_get_job_states": (C.c_int, [_vp, _vp, _i32]),
     "akmc_get_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_get_rho": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_get_block_clocks": (C.c_int, [_vp, _i32, _vp, _vp, _i32]),
@@ -221,6 +223,9 @@ SIGNATURES = {
     "akmc_create_lattice": (C.c_int, [_vp, _vp, _vp, _i64, _u64, _vp, _i64]),
     "akmc_cluster_stats": (C.c_int, [_vp, _vp, C.POINTER(_i64), _vp, _i64]),
     "akmc_job_cluster_stats": (C.c_int, [_vp, _i32, C.POINTER(_i64), _vp, _i64]),
+    "akmc_snapshot_size": (C.c_int, [_vp, _i32, C.POINTER(_i64)]),
+    "akmc_save_snapshot": (C.c_int, [_vp, _i32, _vp, _i64, C.POINTER(_i64)]),
+    "akmc_restore_snapshot": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_device_math": (C.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "akmc_server_create": (C.c_int, [_vp, C.POINTER(_vp)]),
     "akmc_server_submit": (C.c_int, [_vp, _vp, _vp, _i64, C.POINTER(_i64)]),
@@ -367,13 +372,15 @@ def job_config(
 class Engine:
     """One akmc_ctx: a set of jobs advanced together on one GPU."""
 
-    def __init__(self, device=0, stream=None, event_log_capacity=0, graph_rounds=32, hop_cap_per_round=0):
+    def __init__(self, device=0, stream=None, event_log_capacity=0, graph_rounds=32, hop_cap_per_round=0,
+                 flow_sweep_limit=0):
         cfg = ContextConfig()
         cfg.device = device
         cfg.graph_rounds = graph_rounds
         cfg.stream = stream
         cfg.event_log_capacity = event_log_capacity
         cfg.hop_cap_per_round = hop_cap_per_round
+        cfg.flow_sweep_limit = flow_sweep_limit
         h = C.c_void_p()
         _check(lib().akmc_create(C.byref(cfg), C.byref(h)))
         self.h = h
@@ -443,9 +450,21 @@ class Engine:
         return dict(round=st.round, hops=st.hops, done=bool(st.done), n_blocks=st.n_blocks,
                     n_sites=st.n_sites, n_vacancies=st.n_vacancies)
 
-    def occupancy(self, job=0):
+    def job_states(self):
+        """job_state of every job, read from the device at once."""
+        arr = (JobState * len(self.jobs))()
+        self._ck(lib().akmc_get_job_states(self.h, C.cast(arr, C.c_void_p), len(self.jobs)))
+        return [dict(round=st.round, hops=st.hops, done=bool(st.done), n_blocks=st.n_blocks, n_sites=st.n_sites,
+                     n_vacancies=st.n_vacancies) for st in arr]
+
+    def occupancy(self, job=0, out=None):
+        """The job's lattice; into `out` (a contiguous uint8 array, pinned memory for a fast
+        copy) when given."""
         n = self.jobs[job][1]
-        out = np.empty(n, np.uint8)
+        if out is None:
+            out = np.empty(n, np.uint8)
+        elif out.dtype != np.uint8 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous uint8 array of %d sites" % n)
         self._ck(lib().akmc_get_occupancy(self.h, job, _ptr(out), n))
         return out
 
@@ -491,6 +510,19 @@ class Engine:
         n = C.c_int64(0)
         self._ck(lib().akmc_get_kernel_timing(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def save_snapshot(self, job=0):
+        """Restart snapshot of the job (bytes)."""
+        n = C.c_int64(0)
+        self._ck(lib().akmc_snapshot_size(self.h, job, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        w = C.c_int64(0)
+        self._ck(lib().akmc_save_snapshot(self.h, job, _ptr(buf), n.value, C.byref(w)))
+        return buf[: w.value].tobytes()
+
+    def restore_snapshot(self, job, data):
+        buf = np.frombuffer(data, np.uint8)
+        self._ck(lib().akmc_restore_snapshot(self.h, job, _ptr(buf), len(buf)))
 
     def cluster_stats(self, job=0, hist_len=64):
         """(isolated-Cu count, Cu cluster-size histogram) of the job's lattice, on the device."""

@@ -278,15 +278,22 @@ def test_load_occupancy_restarts_the_trajectory(ak):
         assert np.array_equal(eng.occupancy(0), occ1)
         bad = occ0.copy()
         bad[np.nonzero(bad == 0)[0][0]] = 1  # one vacancy fewer than the job holds
-        with pytest.raises(ak.AkmcError):
+        with pytest.raises(ak.AkmcError) as e:  # reported by the next synchronising call
             eng.load_occupancy(0, bad)
+            eng.sync()
+        assert e.value.status == -1
+        eng.load_occupancy(0, occ0)  # the context stays usable
+        eng.sync()
+        assert np.array_equal(eng.occupancy(0), occ0)
 
 
 @pytest.mark.parametrize("schedule", [1, 2])
-def test_many_blocks_both_schedules(ak, schedule):
-    # 5 x 5 x 5 blocks of 8 cells: under the dependency-driven schedule blocks run
-    # rounds apart; both schedules must give the oracle's trajectory
-    kw = dict(box=(40, 40, 40), blocks=(5, 5, 5), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=150,
+@pytest.mark.parametrize("edge,nvac", [(5, 150), (7, 400)])
+def test_many_blocks_both_schedules(ak, schedule, edge, nvac):
+    # edge^3 blocks of 8 cells: under the dependency-driven schedule blocks run rounds apart;
+    # both schedules must give the oracle's trajectory.  343 blocks are more than two per SM,
+    # so the dependency-driven kernel runs two CTAs per SM.
+    kw = dict(box=(8 * edge,) * 3, blocks=(edge,) * 3, model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=nvac,
               temperature=563.0, seed=5)
     eng, (o,) = run_pair(ak, 96, [kw], schedule)
     assert o.hops > 1000
