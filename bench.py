@@ -159,6 +159,50 @@ def run_serve(args, ak, device):
     print(json.dumps(line))
 
 
+def reduce_over_ranks(dist, t, hops, device):
+    """Whole-job figures over the ranks of a replica run: the slowest rank's time and the hops
+    of all ranks (every rank takes the same two collectives in the same order)."""
+    import torch
+
+    v = torch.tensor([float(t), float(hops)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(v[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(v[1:2], op=dist.ReduceOp.SUM)
+    return float(v[0]), float(v[1])
+
+
+def run_one_at_a_time(args, ak, jobs, device, stream, torch):
+    """The plain form of a multi-job workload: the first N jobs in FP64, each alone in its own
+    context, R rounds each after one untimed step; hops/s = all hops / all device time."""
+    eam = ak.eam_johnson(42)
+    hops, ms = 0, 0.0
+    sample = jobs[: args.one_at_a_time]
+    for j in sample:
+        occ = ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"])
+        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=ak.FP64,
+                            temperature=j["temperature"], seed=j["seed"], eam=eam)
+        with ak.Engine(device=device, stream=stream.cuda_stream) as eng:
+            eng.add_job(cfg, occ)
+            eng.prepare()
+            eng.run_rounds(args.rounds_per_step)
+            eng.sync()
+            h0 = eng.counters()["hops"]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.run_rounds(args.rounds_per_step)
+            e1.record(stream)
+            eng.sync()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            hops += eng.counters()["hops"] - h0
+    line = {"metric": METRIC, "impl": "b200 plain FP64, one job at a time", "value": hops / (ms / 1e3),
+            "unit": "hops/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": config_of(args, jobs)["workload"], "jobs_timed": len(sample),
+                       "rounds_per_job": args.rounds_per_step, "note": "each job alone in its own context"},
+            "hops_timed": int(hops), "ms": ms}
+    print(json.dumps(line))
+
+
 def algorithmic_bytes(hops, evals, nact_sum, eam=True):
     """Canonical bytes of the path: per vacancy evaluation the 145-site footprint
     (occupancy byte + int32 density) and 8 FP64 rates; per hop the 78-site density
@@ -355,6 +399,11 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--rounds-per-step", type=int, default=256)
+    ap.add_argument("--one-at-a-time", type=int, default=0, metavar="N",
+                    help="time the first N jobs of the workload in plain FP64, each alone (the baseline of "
+                         "the batched form)")
+    ap.add_argument("--block-edge", type=int, default=0,
+                    help="batched workload: blocks of at most this many cells; 0 = autotune before timing")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -398,6 +447,22 @@ def main():
         dist.barrier()
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
+    if args.one_at_a_time:
+        run_one_at_a_time(args, ak, jobs, local, stream, torch)
+        return
+    tuned = None
+    if args.workload == "batched":
+        import akmc_b200.autotune as at
+
+        edge = args.block_edge
+        if edge <= 0:  # autotune on the actual job set, outside the timed region
+            lats = [ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"]) for j in jobs]
+            edge, table = at.tune_block_edge(jobs, lats, ak.eam_johnson(42), device=local)
+            tuned = {"block_edge": edge, "trial_hops_per_s": {str(k): round(v) for k, v in table.items()}}
+        else:
+            tuned = {"block_edge": edge}
+        for j in jobs:
+            j["blocks"] = tuple(at.blocks_for(e, edge) for e in j["box"])
     eng, lattices = build_engine(ak, jobs, local, stream.cuda_stream)
     R = args.rounds_per_step
     eam = True
@@ -430,13 +495,7 @@ def main():
     clk = clocks.stop()
     c1 = eng.counters()
     hops = c1["hops"] - c0["hops"]
-    t = torch.tensor([ms, float(hops)], dtype=torch.float64, device="cuda")
-    if dist:
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
-        t = tmax
-    ms_all, hops_all = float(t[0]), float(t[1])
+    ms_all, hops_all = reduce_over_ranks(dist, ms, hops, "cuda")
     value = hops_all / (ms_all / 1e3)
 
     # kernels launched per timed step: round by round, k_bucket + k_hop + k_finalize per round
@@ -484,11 +543,8 @@ def main():
     e_dt = time.perf_counter() - t0
     e1 = eng.counters()
     e_hops = e1["hops"] - e0["hops"]
-    et = torch.tensor([e_dt, float(e_hops)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
-    e2e = {"value": float(et[1]) / float(et[0]), "unit": "hops/s",
+    e_dt_all, e_hops_all = reduce_over_ranks(dist, e_dt, e_hops, "cuda")
+    e2e = {"value": e_hops_all / e_dt_all, "unit": "hops/s",
            "h2d_bytes_per_step": int(sum(o.size for o in lattices)), "d2h_bytes_per_step": int(sum(o.size for o in lattices)),
            "note": "each step restarts the jobs from the host lattices (upload, density rebuild), runs R rounds and "
                    "reads the lattices back"}
@@ -502,6 +558,8 @@ def main():
             "gpu_launches": launches_per_step * args.steps, "schedule": sched_name, "clocks": clk,
             "hops_timed": int(hops_all),
         }
+        if tuned:
+            line["config"]["autotune"] = tuned
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(jobs)
         print(json.dumps(line))

@@ -6,11 +6,12 @@
 // copying the lattice out.
 //
 //   k_cu_collect  one pass over the occupancy bytes (16 per thread, vector loads): every Cu
-//                 site is appended to a list, starts as its own root and is tested for a Cu
-//                 neighbour.  The only pass over the whole lattice: HBM-bound.
-//   k_cu_union    per listed site, each 1nn Cu bond to a higher site id is merged into one
-//                 set (lock-free union-find: the larger root is hooked under the smaller with
-//                 a CAS, finds halve their paths).
+//                 site is appended to a list and starts as its own root.  The only pass over
+//                 the whole lattice: HBM-bound.
+//   k_cu_union    per listed site (one per thread), its 8 first neighbours are read once: no
+//                 Cu among them makes it isolated, and each Cu bond to a higher site id is
+//                 merged into one set (lock-free union-find: the larger root is hooked under
+//                 the smaller with a CAS, finds halve their paths).
 //   k_cu_size     per listed site, +1 on its root's size.
 //   k_cu_hist     per root, +1 on the bin of its size (min(size, bins - 1)).
 // The partition, hence every count, does not depend on the order the threads run in.
@@ -49,9 +50,9 @@ __device__ __forceinline__ uint32_t cu_bytes(uint32_t w) {
 }
 
 // Thread t of the grid reads the 16 sites [16 t, 16 t + 16); the warp takes list slots with one
-// atomic and counts its isolated atoms with one more.
-__global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int sx, int sy, int sz, int32_t* list,
-                             unsigned int* n_list, int32_t* parent, int32_t* size, unsigned long long* iso) {
+// atomic.
+__global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int32_t* list, unsigned int* n_list,
+                             int32_t* parent, int32_t* size) {
   const int lane = threadIdx.x & 31;
   const int64_t nvec = (ns + 15) / 16;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
@@ -80,7 +81,6 @@ __global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int sx
     unsigned int base = 0;
     if (lane == 31 && pre) base = atomicAdd(n_list, static_cast<unsigned int>(pre));
     base = __shfl_sync(kFull, base, 31) + static_cast<unsigned int>(pre - cnt);
-    int isolated = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       uint32_t z = m[k];
@@ -89,15 +89,9 @@ __global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int sx
         z &= z - 1;
         parent[s] = static_cast<int32_t>(s);
         size[s] = 0;
-        bool has = false;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) has |= __ldg(occ + nn1_site(s, b, sx, sy, sz)) == kCuCode;
-        isolated += has ? 0 : 1;
         list[base++] = static_cast<int32_t>(s);
       }
     }
-    isolated = __reduce_add_sync(kFull, isolated);
-    if (lane == 0 && isolated) atomicAdd(iso, static_cast<unsigned long long>(isolated));
   }
 }
 
@@ -114,15 +108,26 @@ __device__ __forceinline__ int32_t find_root(int32_t* parent, int32_t x, unsigne
 }
 
 __global__ void k_cu_union(const uint8_t* __restrict__ occ, int sx, int sy, int sz, const int32_t* list,
-                           const unsigned int* n_list, int32_t* parent, unsigned int* status) {
+                           const unsigned int* n_list, int32_t* parent, unsigned long long* iso,
+                           unsigned int* status) {
+  const int lane = threadIdx.x & 31;
   const int64_t n = *n_list;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t s = list[i];
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  // warp-uniform trip count, so that the warp can sum its isolated atoms
+  for (int64_t w0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x - lane; w0 < n; w0 += step) {
+    const int64_t i = w0 + lane;
+    const int32_t s = i < n ? list[i] : -1;
+    unsigned cu = 0;  // bit b: first neighbour b is Cu
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if (s >= 0 && __ldg(occ + nn1_site(s, b, sx, sy, sz)) == kCuCode) cu |= 1u << b;
+    const int isolated = __reduce_add_sync(kFull, s >= 0 && cu == 0 ? 1 : 0);
+    if (lane == 0 && isolated) atomicAdd(iso, static_cast<unsigned long long>(isolated));
 #pragma unroll 1
     for (int b = 0; b < 8; ++b) {
+      if (!((cu >> b) & 1u)) continue;
       const int64_t r = nn1_site(s, b, sx, sy, sz);
-      if (r <= s || __ldg(occ + r) != kCuCode) continue;
+      if (r <= s) continue;
       int32_t a = s, c = static_cast<int32_t>(r);
       int it = 0;
       for (; it < kUnionLimit; ++it) {
@@ -154,11 +159,20 @@ __global__ void k_cu_hist(const int32_t* list, const unsigned int* n_list, const
   extern __shared__ unsigned long long h_s[];
   for (int k = threadIdx.x; k < bins; k += blockDim.x) h_s[k] = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   const int64_t n = *n_list;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t s = list[i];
-    if (parent[s] == s) atomicAdd(h_s + min(size[s], bins - 1), 1ull);
+  // warp-uniform trip count; lanes with the same bin add once through their leader (most
+  // clusters are single atoms: one shared bin would otherwise take every atomic)
+  for (int64_t w0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x - lane; w0 < n;
+       w0 += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = w0 + lane;
+    int bin = -1;
+    if (i < n) {
+      const int32_t s = list[i];
+      if (parent[s] == s) bin = min(size[s], bins - 1);
+    }
+    const unsigned same = __match_any_sync(kFull, bin);
+    if (bin >= 0 && lane == __ffs(static_cast<int>(same)) - 1) atomicAdd(h_s + bin, static_cast<unsigned long long>(__popc(same)));
   }
   __syncthreads();
   for (int k = threadIdx.x; k < bins; k += blockDim.x)
@@ -176,9 +190,9 @@ int launch_cluster_stats(const ClusterArgs& c, void* stream) {
   const int64_t nvec = (c.ns + 15) / 16;
   int grid = static_cast<int>(std::min<int64_t>((nvec + 255) / 256, 148 * 16));
   if (grid < 1) grid = 1;
-  k_cu_collect<<<grid, 256, 0, st>>>(c.occ, c.ns, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.size, c.iso);
+  k_cu_collect<<<grid, 256, 0, st>>>(c.occ, c.ns, c.list, c.n_list, c.parent, c.size);
   const int g2 = 148 * 8;
-  k_cu_union<<<g2, 256, 0, st>>>(c.occ, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.status);
+  k_cu_union<<<g2, 256, 0, st>>>(c.occ, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.iso, c.status);
   k_cu_size<<<g2, 256, 0, st>>>(c.list, c.n_list, c.parent, c.size, c.status);
   k_cu_hist<<<g2, 256, sizeof(unsigned long long) * c.bins, st>>>(c.list, c.n_list, c.parent, c.size, c.hist,
                                                                    c.bins);

@@ -419,6 +419,21 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
   do {              \
   } while (0)
 #endif
+// Staging sub-phases (builds with -DAKMC_FLOW_PROFILE): counters 16..19.
+#ifdef AKMC_FLOW_PROFILE
+#define AKMC_STAGE_T(k)                                                                         \
+  do {                                                                                          \
+    if (threadIdx.x == 0) {                                                                     \
+      const long long t_ = clock64();                                                           \
+      atomicAdd(a.counters + 16 + (k), static_cast<unsigned long long>(t_ - tsub));             \
+      tsub = t_;                                                                                \
+    }                                                                                           \
+  } while (0)
+#else
+#define AKMC_STAGE_T(k) \
+  do {                \
+  } while (0)
+#endif
 
 // The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
 // Warps 0..7 evaluate rates (warp b = jump b) and refresh densities; warp 8 keeps the
@@ -434,6 +449,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const bool evaluator = warp < 8;
 #ifdef AKMC_PHASE_PROFILE
   long long tph = clock64();
+#endif
+#ifdef AKMC_FLOW_PROFILE
+  long long tsub = clock64();
 #endif
   BlockDev& B = a.blocks[gb];
   const JobDev& J = a.jobs[B.job];
@@ -467,6 +485,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const int tab0 = J.pot * 4 + KIND, tab1 = R.LX | (R.LY << 16);
   const bool need_tab = sm.tab_key[0] != tab0 || sm.tab_key[1] != tab1;
   __syncthreads();  // every thread has read win_pot and tab_key; the previous item's readers are done
+  AKMC_STAGE_T(0);
   if (need_win && tid == kCtl) {
     if (KIND == kEam32) {
       bulk_expect(&sm.mbar, kFWin * 20u);
@@ -495,6 +514,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   FT.status = a.status;
   FT.prof = a.counters + 16;
   FT.fc = fcache_of(rho_s, R.n);
+  AKMC_STAGE_T(1);
 
   // stage the region: warp w takes rows w, w+9, ...; kStageRows rows of loads are issued
   // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
@@ -540,6 +560,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
   }
+  AKMC_STAGE_T(2);
   const int cnt = cnt_in;
   if (tid < cnt) {
     const int v = vlist[tid];
@@ -561,6 +582,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.vact[tid] = 1;
   }
   __syncthreads();
+  AKMC_STAGE_T(3);
   AKMC_PHASE(0);
   if (tid == kCtl) {
     // z-y-x scan order of ABVIModel::calcRates = ascending site id inside a sector
@@ -1541,27 +1563,67 @@ __global__ void k_api_reset(RoundArgs a) {
 
 // Density cache of a whole lattice: rho_i = sum over the 58 neighbours j within the cutoff of
 // f_{X_j}(shell) in Q.24.  A CTA takes tiles of 32 x 8 x 4 sites (x doubled), stages each with
-// its halo (4 sites in x, 2 in y and z, periodic) in shared memory together with the shell
-// offsets and the f table by occupancy code, and sums from there.  The sums are exact
-// integers, so the order of the terms does not matter.
+// its halo (4 sites in x, 2 in y and z, periodic) and the f table by occupancy code in shared
+// memory, and sums from there.  The 58 neighbours of the 5 BCC shells are a fixed geometric
+// set, enumerated at compile time: every term is one byte read of the tile and one read of the
+// f table at immediate offsets.  The sums are exact integers, so the term order does not matter.
 constexpr int kRhoTX = 32, kRhoTY = 8, kRhoTZ = 4, kRhoHX = 4, kRhoHY = 2, kRhoHZ = 2;
 constexpr int kRhoLX = kRhoTX + 2 * kRhoHX, kRhoLY = kRhoTY + 2 * kRhoHY, kRhoLZ = kRhoTZ + 2 * kRhoHZ;
 
+struct RhoNb {
+  int off, sh;  // tile offset, shell code 1..5
+};
+// Squared distance of sites (X0, 0, 0) and (X0 + dX, dy, dz) in (a/2)^2 units: corner sites
+// (X even) sit at (X, 2y, 2z), centre sites at (X, 2y + 1, 2z + 1).
+__host__ __device__ constexpr int rho_d2(int p0, int dX, int dy, int dz) {
+  const int p1 = (p0 + dX) & 1;
+  const int hy = 2 * dy + p1 - p0, hz = 2 * dz + p1 - p0;
+  return dX * dX + hy * hy + hz * hz;
+}
+__host__ __device__ constexpr int rho_shell(int d2) {
+  return d2 == 3 ? 1 : d2 == 4 ? 2 : d2 == 8 ? 3 : d2 == 11 ? 4 : d2 == 12 ? 5 : 0;
+}
+// k-th neighbour (k < 58) of a site of x parity p within the 5 shells.
+__host__ __device__ constexpr RhoNb rho_nbr(int p, int k) {
+  int n = 0;
+  for (int dz = -2; dz <= 2; ++dz)
+    for (int dy = -2; dy <= 2; ++dy)
+      for (int dX = -4; dX <= 4; ++dX) {
+        const int sh = (dX || dy || dz) ? rho_shell(rho_d2(p, dX, dy, dz)) : 0;
+        if (!sh) continue;
+        if (n == k) return RhoNb{dX + kRhoLX * (dy + kRhoLY * dz), sh};
+        ++n;
+      }
+  return RhoNb{0, 0};
+}
+__host__ __device__ constexpr int rho_count(int p) {
+  int n = 0;
+  for (int dz = -2; dz <= 2; ++dz)
+    for (int dy = -2; dy <= 2; ++dy)
+      for (int dX = -4; dX <= 4; ++dX) n += (dX || dy || dz) && rho_shell(rho_d2(p, dX, dy, dz)) ? 1 : 0;
+  return n;
+}
+static_assert(rho_count(0) == kShellNb && rho_count(1) == kShellNb, "58 neighbours in the 5 BCC shells");
+
+template <int P, int K>
+__device__ __forceinline__ int32_t rho_terms(const uint8_t* t, const int32_t* fqc) {
+  if constexpr (K == kShellNb) {
+    return 0;
+  } else {
+    constexpr RhoNb e = rho_nbr(P, K);
+    return fqc[t[e.off] * 8 + e.sh] + rho_terms<P, K + 1>(t, fqc);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy,
-                                                  int32_t sz, const Potential* pot, const Geometry* geo) {
+                                                  int32_t sz, const Potential* pot) {
   __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
-  __shared__ int32_t nbo[2][kShellNb], nbs[2][kShellNb];  // local offset and shell per x parity
-  __shared__ int32_t fqc[16][8];                           // f in Q.24 by occupancy code; V and others 0
+  __shared__ int32_t fqc[16 * 8];  // f in Q.24 by occupancy code and shell; V and other codes 0
   const int tid = threadIdx.x;
   for (int i = tid; i < 16 * 8; i += blockDim.x) {
     const int code = i >> 3;
     const bool atom = code == 1 || code == 2 || code == 4 || code == 8;
-    fqc[code][i & 7] = atom ? pot->fq[species_index(static_cast<uint8_t>(code))][i & 7] : 0;
-  }
-  for (int i = tid; i < 2 * kShellNb; i += blockDim.x) {
-    const int32_t w = geo->nbr[i / kShellNb][i % kShellNb];
-    nbo[i / kShellNb][i % kShellNb] = unpack_dx(w) + kRhoLX * (unpack_dy(w) + kRhoLY * unpack_dz(w));
-    nbs[i / kShellNb][i % kShellNb] = unpack_sh_s(w);
+    fqc[i] = atom ? pot->fq[species_index(static_cast<uint8_t>(code))][i & 7] : 0;
   }
   const int nx = (sx + kRhoTX - 1) / kRhoTX, ny = (sy + kRhoTY - 1) / kRhoTY, nz = (sz + kRhoTZ - 1) / kRhoTZ;
   const int64_t ntiles = static_cast<int64_t>(nx) * ny * nz;
@@ -1569,25 +1631,34 @@ __global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* r
     const int x0 = static_cast<int>(tix % nx) * kRhoTX;
     const int y0 = static_cast<int>((tix / nx) % ny) * kRhoTY;
     const int z0 = static_cast<int>(tix / (static_cast<int64_t>(nx) * ny)) * kRhoTZ;
-    __syncthreads();  // tables written; the previous tile's readers are done
+    __syncthreads();  // table written; the previous tile's readers are done
     for (int i = tid; i < kRhoLX * kRhoLY * kRhoLZ; i += blockDim.x) {
       const int lx = i % kRhoLX, t = i / kRhoLX, ly = t % kRhoLY, lz = t / kRhoLY;
-      int gx = (x0 - kRhoHX + lx) % sx, gy = (y0 - kRhoHY + ly) % sy, gz = (z0 - kRhoHZ + lz) % sz;
+      // periodic wrap without division: coordinates start at most one halo below 0 and end
+      // below 3 box lengths (sx >= 16 sites, sy, sz >= 8 cells)
+      int gx = x0 - kRhoHX + lx, gy = y0 - kRhoHY + ly, gz = z0 - kRhoHZ + lz;
       gx += gx < 0 ? sx : 0;
       gy += gy < 0 ? sy : 0;
       gz += gz < 0 ? sz : 0;
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        gx -= gx >= sx ? sx : 0;
+        gy -= gy >= sy ? sy : 0;
+        gz -= gz >= sz ? sz : 0;
+      }
       tile[i] = __ldg(occ + gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz));
     }
     __syncthreads();
+    // each warp takes sites of one x parity (both parities' sums are unrolled code): warp w
+    // covers rows 2 (w / 2) and 2 (w / 2) + 1, the 16 sites of parity w % 2 of each
     for (int k = tid; k < kRhoTX * kRhoTY * kRhoTZ; k += blockDim.x) {
-      const int lx = k % kRhoTX, t = k / kRhoTX, ly = t % kRhoTY, lz = t / kRhoTY;
+      const int w = k >> 5, ln = k & 31;
+      const int p = w & 1, row = ((w >> 1) << 1) + (ln >> 4);
+      const int lx = 2 * (ln & 15) + p, ly = row % kRhoTY, lz = row / kRhoTY;
       const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
       if (gx >= sx || gy >= sy || gz >= sz) continue;
-      const int p = gx & 1;
-      const int c = (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
-      int32_t acc = 0;
-#pragma unroll 2
-      for (int i = 0; i < kShellNb; ++i) acc += fqc[tile[c + nbo[p][i]]][nbs[p][i]];
+      const uint8_t* t = tile + (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
+      const int32_t acc = p ? rho_terms<1, 0>(t, fqc) : rho_terms<0, 0>(t, fqc);
       rho[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)] = acc;
     }
   }
@@ -1679,7 +1750,8 @@ int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t 
   const int64_t ntiles = static_cast<int64_t>((sx + kRhoTX - 1) / kRhoTX) * ((sy + kRhoTY - 1) / kRhoTY) *
                          ((sz + kRhoTZ - 1) / kRhoTZ);
   const int64_t blocks = std::min<int64_t>(ntiles, 148 * 16);
-  k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, pot, geo);
+  (void)geo;
+  k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, pot);
   return static_cast<int>(cudaGetLastError());
 }
 
