@@ -526,19 +526,24 @@ def main():
                 "e_hop": (r1["evaluations"] - r0["evaluations"]) / max(1, rh),
                 "n_act_per_hop": (r1["n_act_sum"] - r0["n_act_sum"]) / max(1, rh)}
 
-    # end to end through the C ABI: lattice from pinned host memory, R rounds, lattice back
-    pinned = [torch.from_numpy(occ).pin_memory() for occ in lattices]
-    outs = [torch.empty(occ.size, dtype=torch.uint8).pin_memory() for occ in lattices]
+    # end to end through the C ABI: lattices from pinned host memory, R rounds, lattices back
+    # (one job: akmc_load_occupancy / akmc_get_occupancy; several: the all-jobs forms)
+    whole = torch.from_numpy(np.concatenate(lattices)).pin_memory()
+    whole_out = torch.empty(whole.numel(), dtype=torch.uint8).pin_memory()
     sync_all()
     e0 = eng.counters()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for j, p in enumerate(pinned):
-            eng.load_occupancy(j, p.numpy())
+        if len(lattices) == 1:
+            eng.load_occupancy(0, whole.numpy())
+        else:
+            eng.load_occupancies(whole.numpy())
         eng.run_rounds(R)
         eng.sync()
-        for j, o in enumerate(outs):
-            eng.occupancy(j, out=o.numpy())
+        if len(lattices) == 1:
+            eng.occupancy(0, out=whole_out.numpy())
+        else:
+            eng.occupancies(out=whole_out.numpy())
     sync_all()
     e_dt = time.perf_counter() - t0
     e1 = eng.counters()

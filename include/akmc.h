@@ -215,6 +215,13 @@ AKMC_API akmc_status akmc_get_phase_cycles(akmc_ctx* ctx, int64_t* out16);
  * (AKMC_EINVAL) by the next synchronising call. */
 AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8_t* occ, int64_t n_sites);
 
+/* All jobs at once: the lattices of every job of the context back to back in job order
+ * (total_sites = the sum of their sites).  akmc_load_occupancies is akmc_load_occupancy for
+ * every job, with one host copy and one launch of each kernel for the whole context
+ * (asynchronous; errors as there).  akmc_get_occupancies reads them all back the same way. */
+AKMC_API akmc_status akmc_load_occupancies(akmc_ctx* ctx, const uint8_t* occ, int64_t total_sites);
+AKMC_API akmc_status akmc_get_occupancies(akmc_ctx* ctx, uint8_t* out, int64_t total_sites);
+
 /* Restart snapshots.  The reference's restart is a stub (pkmc.cpp:183-184); this one holds
  * a job's lattice, its rounds, hop counts, sector clocks and random streams per block, in a
  * versioned byte buffer with a checksum.  Restored into a job added with the same

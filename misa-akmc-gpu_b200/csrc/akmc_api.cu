@@ -97,6 +97,16 @@ struct akmc_ctx {
   int32_t* d_cl = nullptr;
   int64_t cl_sites = 0;
   unsigned long long* d_cl_misc = nullptr;
+  // whole-context lattice transfers: staging buffer, chunk table, per-job vacancy counts,
+  // density tiles of the EAM jobs (built at the first transfer)
+  uint8_t* d_stage = nullptr;
+  SiteChunk* d_chunks = nullptr;
+  int32_t* d_job_counts = nullptr;
+  int32_t* d_job_want = nullptr;
+  int64_t* d_tile0 = nullptr;
+  int32_t* d_eam_jobs = nullptr;
+  JobsLoad jl{};
+  int64_t total_sites = 0;
   // kernel timing mode: rounds launched one by one with events around the hop kernel
   bool timing = false;
   std::vector<cudaEvent_t> ev;
@@ -156,6 +166,14 @@ void free_device(akmc_ctx* ctx) {
   ctx->d_cl = nullptr;
   ctx->d_cl_misc = nullptr;
   ctx->cl_sites = 0;
+  void* jl_ptrs[] = {ctx->d_stage, ctx->d_chunks, ctx->d_job_counts, ctx->d_job_want, ctx->d_tile0, ctx->d_eam_jobs};
+  for (void* p : jl_ptrs) cudaFree(p);
+  ctx->d_stage = nullptr;
+  ctx->d_chunks = nullptr;
+  ctx->d_job_counts = ctx->d_job_want = ctx->d_eam_jobs = nullptr;
+  ctx->d_tile0 = nullptr;
+  ctx->jl = JobsLoad{};
+  ctx->total_sites = 0;
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->graph_def) cudaGraphDestroy(ctx->graph_def);
   ctx->graph = nullptr;
@@ -772,6 +790,92 @@ AKMC_API akmc_status akmc_restore_snapshot(akmc_ctx* ctx, int32_t job, const uin
   CK(cudaMemcpyAsync(ctx->d_blocks + j.block0, B.data(), B.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
                      ctx->stream));
   return akmc_sync(ctx);  // B and J leave scope; also reports a lattice with a wrong vacancy count
+}
+
+// Tables of the whole-context transfers, built once after akmc_prepare.
+static akmc_status setup_jobs_load(akmc_ctx* ctx) {
+  if (ctx->d_stage) return AKMC_OK;
+  constexpr int64_t kChunk = 1 << 16;
+  std::vector<SiteChunk> ch;
+  std::vector<int32_t> want, eam_jobs;
+  std::vector<int64_t> tile0{0};
+  int64_t off = 0;
+  for (size_t k = 0; k < ctx->jobs.size(); ++k) {
+    const HostJob& j = ctx->jobs[k];
+    for (int64_t s0 = 0; s0 < j.nsites; s0 += kChunk) {
+      SiteChunk c{};
+      c.job = static_cast<int32_t>(k);
+      c.vac0 = j.vac0;
+      c.nvac = static_cast<int32_t>(j.nvac);
+      c.site0 = s0;
+      c.n = std::min(kChunk, j.nsites - s0);
+      c.stage0 = off + s0;
+      ch.push_back(c);
+    }
+    off += j.nsites;
+    want.push_back(static_cast<int32_t>(j.nvac));
+    if (j.has_eam) {
+      const int64_t sx = 2 * j.cfg.box[0], sy = j.cfg.box[1], sz = j.cfg.box[2];
+      eam_jobs.push_back(static_cast<int32_t>(k));
+      tile0.push_back(tile0.back() + ((sx + 31) / 32) * ((sy + 7) / 8) * ((sz + 3) / 4));
+    }
+  }
+  if (ch.size() > static_cast<size_t>(INT32_MAX)) return fail(ctx, AKMC_EINVAL, "too many sites");
+  CK(dalloc(&ctx->d_stage, static_cast<size_t>(off)));
+  CK(dalloc(&ctx->d_chunks, ch.size()));
+  CK(dalloc(&ctx->d_job_counts, want.size()));
+  CK(dalloc(&ctx->d_job_want, want.size()));
+  CK(dalloc(&ctx->d_tile0, tile0.size()));
+  CK(dalloc(&ctx->d_eam_jobs, std::max<size_t>(1, eam_jobs.size())));
+  CK(cudaMemcpy(ctx->d_chunks, ch.data(), ch.size() * sizeof(SiteChunk), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_job_want, want.data(), want.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_tile0, tile0.data(), tile0.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  if (!eam_jobs.empty())
+    CK(cudaMemcpy(ctx->d_eam_jobs, eam_jobs.data(), eam_jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  JobsLoad& L = ctx->jl;
+  L.stage = ctx->d_stage;
+  L.chunks = ctx->d_chunks;
+  L.nchunks = static_cast<int32_t>(ch.size());
+  L.njobs = static_cast<int32_t>(want.size());
+  L.counts = ctx->d_job_counts;
+  L.want = ctx->d_job_want;
+  L.tile0 = ctx->d_tile0;
+  L.eam_jobs = ctx->d_eam_jobs;
+  L.neam = static_cast<int32_t>(eam_jobs.size());
+  L.eam_tiles = tile0.back();
+  ctx->total_sites = off;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_load_occupancies(akmc_ctx* ctx, const uint8_t* occ, int64_t total_sites) {
+  if (!ctx || !occ) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const akmc_status st = setup_jobs_load(ctx);
+  if (st != AKMC_OK) return st;
+  if (total_sites != ctx->total_sites) return fail(ctx, AKMC_EINVAL, "total_sites must be the sum of the jobs' sites");
+  CK(cudaMemcpyAsync(ctx->d_stage, occ, static_cast<size_t>(total_sites), cudaMemcpyHostToDevice, ctx->stream));
+  const int e = launch_load_jobs(ctx->args, ctx->jl, ctx->stream);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("load: ") + cuda_name(e));
+  CK(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs.data(), ctx->h_jobs.size() * sizeof(JobDev), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks, ctx->h_blocks.data(), ctx->h_blocks.size() * sizeof(BlockDev),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  return AKMC_OK;  // a wrong vacancy count is reported by the next synchronising call
+}
+
+AKMC_API akmc_status akmc_get_occupancies(akmc_ctx* ctx, uint8_t* out, int64_t total_sites) {
+  if (!ctx || !out) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  CK(cudaSetDevice(ctx->cfg.device));
+  const akmc_status st = setup_jobs_load(ctx);
+  if (st != AKMC_OK) return st;
+  if (total_sites != ctx->total_sites) return fail(ctx, AKMC_EINVAL, "total_sites must be the sum of the jobs' sites");
+  const int e = launch_gather_jobs(ctx->args, ctx->jl, ctx->stream);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("gather: ") + cuda_name(e));
+  CK(cudaMemcpyAsync(out, ctx->d_stage, static_cast<size_t>(total_sites), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return AKMC_OK;
 }
 
 AKMC_API akmc_status akmc_set_kernel_timing(akmc_ctx* ctx, int32_t enable) {

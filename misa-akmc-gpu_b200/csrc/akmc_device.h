@@ -158,6 +158,27 @@ int launch_device_math(const double* x, int64_t n, double* e, double* l, void* s
 // hop budget); grid = persistent CTAs of the flow kernels.
 int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1);
 
+// Whole-context lattice transfers (akmc_load_occupancies / akmc_get_occupancies): the lattices
+// of all jobs back to back in a staging buffer, cut into chunks of one job each.
+struct SiteChunk {
+  int32_t job, vac0, nvac, pad;
+  int64_t site0, n, stage0;  // first site in the job, sites, offset in the staging buffer
+};
+struct JobsLoad {
+  const uint8_t* stage_in;  // unused by the kernels (host side)
+  uint8_t* stage;
+  const SiteChunk* chunks;
+  int32_t nchunks, njobs;
+  int32_t* counts;          // vacancies found per job
+  const int32_t* want;      // vacancies each job holds
+  const int64_t* tile0;     // density tiles of the EAM jobs, prefix (neam + 1)
+  const int32_t* eam_jobs;  // job index of each EAM job
+  int32_t neam;
+  int64_t eam_tiles;
+};
+int launch_load_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);
+int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);
+
 // Cu cluster statistics of one job's occupancy (akmc_cluster.cu).  list, parent and size hold
 // one int32 per site; iso and hist are cleared by the launch.
 struct ClusterArgs {

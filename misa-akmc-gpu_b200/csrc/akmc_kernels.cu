@@ -1615,53 +1615,121 @@ __device__ __forceinline__ int32_t rho_terms(const uint8_t* t, const int32_t* fq
   }
 }
 
-__global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy,
-                                                  int32_t sz, const Potential* pot) {
-  __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
-  __shared__ int32_t fqc[16 * 8];  // f in Q.24 by occupancy code and shell; V and other codes 0
-  const int tid = threadIdx.x;
-  for (int i = tid; i < 16 * 8; i += blockDim.x) {
+// f in Q.24 by occupancy code and shell into shared memory; V and other codes 0.
+__device__ void rho_table(int32_t* fqc, const Potential* pot) {
+  for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
     const int code = i >> 3;
     const bool atom = code == 1 || code == 2 || code == 4 || code == 8;
     fqc[i] = atom ? pot->fq[species_index(static_cast<uint8_t>(code))][i & 7] : 0;
   }
-  const int nx = (sx + kRhoTX - 1) / kRhoTX, ny = (sy + kRhoTY - 1) / kRhoTY, nz = (sz + kRhoTZ - 1) / kRhoTZ;
-  const int64_t ntiles = static_cast<int64_t>(nx) * ny * nz;
-  for (int64_t tix = blockIdx.x; tix < ntiles; tix += gridDim.x) {
-    const int x0 = static_cast<int>(tix % nx) * kRhoTX;
-    const int y0 = static_cast<int>((tix / nx) % ny) * kRhoTY;
-    const int z0 = static_cast<int>(tix / (static_cast<int64_t>(nx) * ny)) * kRhoTZ;
-    __syncthreads();  // table written; the previous tile's readers are done
-    for (int i = tid; i < kRhoLX * kRhoLY * kRhoLZ; i += blockDim.x) {
-      const int lx = i % kRhoLX, t = i / kRhoLX, ly = t % kRhoLY, lz = t / kRhoLY;
-      // periodic wrap without division: coordinates start at most one halo below 0 and end
-      // below 3 box lengths (sx >= 16 sites, sy, sz >= 8 cells)
-      int gx = x0 - kRhoHX + lx, gy = y0 - kRhoHY + ly, gz = z0 - kRhoHZ + lz;
-      gx += gx < 0 ? sx : 0;
-      gy += gy < 0 ? sy : 0;
-      gz += gz < 0 ? sz : 0;
+}
+
+// One tile of the density build (tix-th tile of the lattice); CTA-collective, 256 threads.
+__device__ void rho_tile(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, int64_t tix,
+                         uint8_t* tile, const int32_t* fqc) {
+  const int tid = threadIdx.x;
+  const int nx = (sx + kRhoTX - 1) / kRhoTX, ny = (sy + kRhoTY - 1) / kRhoTY;
+  const int x0 = static_cast<int>(tix % nx) * kRhoTX;
+  const int y0 = static_cast<int>((tix / nx) % ny) * kRhoTY;
+  const int z0 = static_cast<int>(tix / (static_cast<int64_t>(nx) * ny)) * kRhoTZ;
+  __syncthreads();  // table written; the previous tile's readers are done
+  for (int i = tid; i < kRhoLX * kRhoLY * kRhoLZ; i += blockDim.x) {
+    const int lx = i % kRhoLX, t = i / kRhoLX, ly = t % kRhoLY, lz = t / kRhoLY;
+    // periodic wrap without division: coordinates start at most one halo below 0 and end
+    // below 3 box lengths (sx >= 16 sites, sy, sz >= 8 cells)
+    int gx = x0 - kRhoHX + lx, gy = y0 - kRhoHY + ly, gz = z0 - kRhoHZ + lz;
+    gx += gx < 0 ? sx : 0;
+    gy += gy < 0 ? sy : 0;
+    gz += gz < 0 ? sz : 0;
 #pragma unroll
-      for (int w = 0; w < 2; ++w) {
-        gx -= gx >= sx ? sx : 0;
-        gy -= gy >= sy ? sy : 0;
-        gz -= gz >= sz ? sz : 0;
-      }
-      tile[i] = __ldg(occ + gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz));
+    for (int w = 0; w < 2; ++w) {
+      gx -= gx >= sx ? sx : 0;
+      gy -= gy >= sy ? sy : 0;
+      gz -= gz >= sz ? sz : 0;
     }
-    __syncthreads();
-    // each warp takes sites of one x parity (both parities' sums are unrolled code): warp w
-    // covers rows 2 (w / 2) and 2 (w / 2) + 1, the 16 sites of parity w % 2 of each
-    for (int k = tid; k < kRhoTX * kRhoTY * kRhoTZ; k += blockDim.x) {
-      const int w = k >> 5, ln = k & 31;
-      const int p = w & 1, row = ((w >> 1) << 1) + (ln >> 4);
-      const int lx = 2 * (ln & 15) + p, ly = row % kRhoTY, lz = row / kRhoTY;
-      const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-      if (gx >= sx || gy >= sy || gz >= sz) continue;
-      const uint8_t* t = tile + (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
-      const int32_t acc = p ? rho_terms<1, 0>(t, fqc) : rho_terms<0, 0>(t, fqc);
-      rho[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)] = acc;
+    tile[i] = __ldg(occ + gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz));
+  }
+  __syncthreads();
+  // each warp takes sites of one x parity (both parities' sums are unrolled code): warp w
+  // covers rows 2 (w / 2) and 2 (w / 2) + 1, the 16 sites of parity w % 2 of each
+  for (int k = tid; k < kRhoTX * kRhoTY * kRhoTZ; k += blockDim.x) {
+    const int w = k >> 5, ln = k & 31;
+    const int p = w & 1, row = ((w >> 1) << 1) + (ln >> 4);
+    const int lx = 2 * (ln & 15) + p, ly = row % kRhoTY, lz = row / kRhoTY;
+    const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+    if (gx >= sx || gy >= sy || gz >= sz) continue;
+    const uint8_t* t = tile + (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
+    const int32_t acc = p ? rho_terms<1, 0>(t, fqc) : rho_terms<0, 0>(t, fqc);
+    rho[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)] = acc;
+  }
+}
+
+__host__ __device__ __forceinline__ int64_t rho_tiles(int32_t sx, int32_t sy, int32_t sz) {
+  return static_cast<int64_t>((sx + kRhoTX - 1) / kRhoTX) * ((sy + kRhoTY - 1) / kRhoTY) *
+         ((sz + kRhoTZ - 1) / kRhoTZ);
+}
+
+__global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy,
+                                                  int32_t sz, const Potential* pot) {
+  __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
+  __shared__ int32_t fqc[16 * 8];
+  rho_table(fqc, pot);
+  const int64_t ntiles = rho_tiles(sx, sy, sz);
+  for (int64_t tix = blockIdx.x; tix < ntiles; tix += gridDim.x) rho_tile(occ, rho, sx, sy, sz, tix, tile, fqc);
+}
+
+// The density build of every EAM job of a context in one launch: global tile t belongs to the
+// job k with tile0[k] <= t < tile0[k + 1] (jobs[k] its index).
+__global__ void __launch_bounds__(256) k_init_rho_jobs(RoundArgs a, const int64_t* tile0, const int32_t* jobs,
+                                                       int32_t njobs) {
+  __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
+  __shared__ int32_t fqc[16 * 8];
+  int pot = -1;
+  for (int64_t t = blockIdx.x; t < tile0[njobs]; t += gridDim.x) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {  // last k with tile0[k] <= t
+      const int mid = (lo + hi + 1) >> 1;
+      if (tile0[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const JobDev& J = a.jobs[jobs[lo]];
+    if (J.pot != pot) {  // uniform over the CTA
+      __syncthreads();
+      rho_table(fqc, a.pots + J.pot);
+      pot = J.pot;
+    }
+    rho_tile(J.occ, J.rho, J.sx, J.sy, J.sz, t - tile0[lo], tile, fqc);
+  }
+}
+
+// Whole-context lattice load: chunk c copies its sites from the staging buffer into its job's
+// occupancy and appends the vacancies to the job's slice of the vacancy table.
+__global__ void k_scatter_collect(RoundArgs a, const uint8_t* stage, const SiteChunk* chunks, int32_t* counts) {
+  const SiteChunk c = chunks[blockIdx.x];
+  uint8_t* occ = a.jobs[c.job].occ;
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
+    const uint8_t o = stage[c.stage0 + i];
+    occ[c.site0 + i] = o;
+    if (o == kV) {
+      const int k = atomicAdd(counts + c.job, 1);
+      if (k < c.nvac) {
+        a.vac_site[c.vac0 + k] = static_cast<int32_t>(c.site0 + i);
+        a.vac_job[c.vac0 + k] = c.job;
+      }
     }
   }
+}
+
+__global__ void k_check_counts(const int32_t* counts, const int32_t* want, int32_t njobs, unsigned int* status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < njobs && counts[j] != want[j]) atomicOr(status, kErrVacCount);
+}
+
+// Whole-context lattice read-back: the reverse copy into the staging buffer.
+__global__ void k_gather(RoundArgs a, uint8_t* stage, const SiteChunk* chunks) {
+  const SiteChunk c = chunks[blockIdx.x];
+  const uint8_t* occ = a.jobs[c.job].occ;
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) stage[c.stage0 + i] = occ[c.site0 + i];
 }
 
 __global__ void k_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
@@ -1747,9 +1815,7 @@ int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t 
                     const Geometry* geo, unsigned int* status, void* stream) {
   (void)status;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int64_t ntiles = static_cast<int64_t>((sx + kRhoTX - 1) / kRhoTX) * ((sy + kRhoTY - 1) / kRhoTY) *
-                         ((sz + kRhoTZ - 1) / kRhoTZ);
-  const int64_t blocks = std::min<int64_t>(ntiles, 148 * 16);
+  const int64_t blocks = std::min<int64_t>(rho_tiles(sx, sy, sz), 148 * 16);
   (void)geo;
   k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, pot);
   return static_cast<int>(cudaGetLastError());
@@ -1757,6 +1823,23 @@ int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t 
 
 __global__ void k_check_vacancy_count(const int32_t* count, int32_t want, unsigned int* status) {
   if (*count != want) atomicOr(status, kErrVacCount);
+}
+
+int launch_load_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(L.counts, 0, sizeof(int32_t) * L.njobs, st);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  k_scatter_collect<<<L.nchunks, 256, 0, st>>>(a, L.stage, L.chunks, L.counts);
+  k_check_counts<<<(L.njobs + 127) / 128, 128, 0, st>>>(L.counts, L.want, L.njobs, a.status);
+  if (L.neam > 0)
+    k_init_rho_jobs<<<static_cast<int>(std::min<int64_t>(L.eam_tiles, 148 * 16)), 256, 0, st>>>(a, L.tile0, L.eam_jobs,
+                                                                                                L.neam);
+  return static_cast<int>(cudaGetLastError());
+}
+
+int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
+  k_gather<<<L.nchunks, 256, 0, static_cast<cudaStream_t>(stream)>>>(a, L.stage, L.chunks);
+  return static_cast<int>(cudaGetLastError());
 }
 
 int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,

@@ -211,6 +211,8 @@ SIGNATURES = {
     "akmc_gpu_final": (C.c_int, [_vp]),
     "akmc_get_job_state": (C.c_int, [_vp, _i32, C.POINTER(JobState)]),
     "akmc_get_job_states": (C.c_int, [_vp, _vp, _i32]),
+    "akmc_load_occupancies": (C.c_int, [_vp, _vp, _i64]),
+    "akmc_get_occupancies": (C.c_int, [_vp, _vp, _i64]),
     "akmc_get_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_get_rho": (C.c_int, [_vp, _i32, _vp, _i64]),
     "akmc_get_block_clocks": (C.c_int, [_vp, _i32, _vp, _vp, _i32]),
@@ -501,6 +503,21 @@ class Engine:
     def load_occupancy(self, job, occ):
         occ = np.ascontiguousarray(occ, np.uint8)
         self._ck(lib().akmc_load_occupancy(self.h, job, _ptr(occ), occ.size))
+
+    def load_occupancies(self, occ):
+        """akmc_load_occupancies: every job's lattice, back to back in job order."""
+        occ = np.ascontiguousarray(occ, np.uint8)
+        self._ck(lib().akmc_load_occupancies(self.h, _ptr(occ), occ.size))
+
+    def occupancies(self, out=None):
+        """akmc_get_occupancies: every job's lattice, back to back in job order (into `out`)."""
+        n = sum(j[1] for j in self.jobs)
+        if out is None:
+            out = np.empty(n, np.uint8)
+        elif out.dtype != np.uint8 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous uint8 array of %d sites" % n)
+        self._ck(lib().akmc_get_occupancies(self.h, _ptr(out), n))
+        return out
 
     def set_kernel_timing(self, enable):
         self._ck(lib().akmc_set_kernel_timing(self.h, int(enable)))

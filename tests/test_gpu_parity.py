@@ -259,6 +259,33 @@ def test_cpp_host_time_loop_matches_oracle(ak):
         assert np.array_equal(eng.occupancy(0), o.occupancy())
 
 
+def test_load_occupancies_restarts_every_job(ak):
+    jobs = [dict(box=(20, 20, 20), model=po.MODEL_EAM, seed=1),
+            dict(box=(17, 19, 21), model=po.MODEL_PAIRBOND, seed=2, alloy=QUATERNARY, n_vacancies=7),
+            dict(box=(32, 16, 16), blocks=(2, 1, 1), model=po.MODEL_EAM, precision=po.FP32C, seed=3,
+                 n_vacancies=12)]
+    starts = [oracle_job(**kw).occupancy() for kw in jobs]  # the initial lattices
+    order = ["job", "round", "block", "hop"]
+    eng, oracles = run_pair(ak, 48, jobs)
+    first = np.sort(eng.events(), order=order)
+    ends = [eng.occupancy(j) for j in range(len(jobs))]
+    assert len(first) > 100
+    assert np.array_equal(eng.occupancies(), np.concatenate(ends))
+    eng.load_occupancies(np.concatenate(starts))  # every job restarts
+    eng.run_rounds(48)
+    eng.sync()
+    second = np.sort(eng.events(), order=order)
+    assert first.tobytes() == second.tobytes()
+    assert np.array_equal(eng.occupancies(), np.concatenate(ends))
+    bad = np.concatenate(starts)
+    bad[np.nonzero(bad == 0)[0][-1]] = 1  # the last job holds one vacancy fewer
+    with pytest.raises(ak.AkmcError) as e:
+        eng.load_occupancies(bad)
+        eng.sync()
+    assert e.value.status == -1
+    eng.close()
+
+
 def test_load_occupancy_restarts_the_trajectory(ak):
     o = oracle_job(box=(20, 20, 20), seed=5)
     occ0 = o.occupancy()
