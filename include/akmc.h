@@ -82,7 +82,8 @@ typedef struct akmc_job_config {
   double temperature;       /* K (simulation.temperature) */
   double sector_window;     /* s; the reference hard-codes 3e-7 (src/simulation.h:73-74) */
   uint64_t seed;            /* xoshiro256** streams of event selection and time, per block */
-  int64_t hop_budget;       /* job ends after the round reaching it; <= 0: none */
+  int64_t hop_budget;       /* job ends at the end of the first time step (8 sector rounds) at
+                               which its hop count has reached it; <= 0: none */
   int64_t max_rounds;       /* job ends after this many sector rounds; <= 0: none */
   const akmc_eam_tables* eam; /* EAM model (copied at akmc_add_job); NULL for pair-bond */
 } akmc_job_config;
@@ -169,9 +170,10 @@ AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
  * ROUNDS: every block finishes round r before any starts r+1 (SubLattice::startTimeLoop,
  * sublattice.inl:61-179, with the blocks as MPI ranks).  FLOW: a block's round waits only
  * for the neighbour rounds whose staged regions (sector plus a 2-cell halo) overlap it, so
- * blocks with few hops run ahead; results are identical to ROUNDS.  FLOW serves no hop
- * budget.  AUTO (default): FLOW when the context holds more than one domain block, no job
- * has a hop budget and every block area starts with at most 32 vacancies, else ROUNDS.  akmc_run_rounds_noalloc always runs ROUNDS. */
+ * blocks with few hops run ahead; results are identical to ROUNDS.  Under FLOW, jobs with a
+ * hop budget advance one time step per launch.  AUTO (default): FLOW when the context holds
+ * more than one domain block and every block area starts with at most 32 vacancies, else
+ * ROUNDS.  akmc_run_rounds_noalloc always runs ROUNDS. */
 enum { AKMC_SCHEDULE_AUTO = 0, AKMC_SCHEDULE_ROUNDS = 1, AKMC_SCHEDULE_FLOW = 2 };
 AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule);
 /* The schedule akmc_run_rounds uses (ROUNDS or FLOW), AUTO resolved; after akmc_prepare. */

@@ -84,7 +84,7 @@ struct akmc_ctx {
   int32_t* d_vac_count = nullptr;
   // asynchronous round schedule
   int32_t schedule = AKMC_SCHEDULE_AUTO;
-  bool flow_ok = false;  // no hop budget, and every block area starts with few enough vacancies
+  bool flow_ok = false;  // more than one block, and every block area starts with few enough vacancies
   int flow_grid = 0;
   int32_t* d_lease = nullptr;
   unsigned long long* d_vclaim = nullptr;
@@ -374,6 +374,8 @@ AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, con
   return AKMC_OK;
 }
 
+static akmc_status build_rho_tables(akmc_ctx* ctx);
+
 AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   if (!ctx) return AKMC_EINVAL;
   if (ctx->prepared) return AKMC_OK;
@@ -434,12 +436,13 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device));
   int smem_sm = 0;
   CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
-  // k_hop: one CTA resident per SM (its register use); a second wave where two staged regions
-  // (plus the 1 KB the SM reserves per CTA) fit takes over as CTAs finish.  k_flow is
-  // persistent: one CTA per SM.  (Two per SM, at 96 registers, measured slower.)
-  const int per_sm = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
-  ctx->hop_grid = std::max(1, std::min(nb, sms * per_sm));
-  ctx->flow_grid = std::max(1, std::min(nb, sms));
+  // CTAs resident per SM: as many as the registers allow (hop_ctas_per_sm) and two staged
+  // regions (plus the 1 KB the SM reserves per CTA) fit; k_flow is persistent, one CTA per
+  // slot.  k_hop also gets a second wave where two regions fit.
+  const int fit = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
+  const int resident = std::min(fit, hop_ctas_per_sm());
+  ctx->hop_grid = std::max(1, std::min(nb, sms * fit));
+  ctx->flow_grid = std::max(1, std::min(nb, sms * resident));
 
   // geometry and potentials
   Geometry geo;
@@ -554,10 +557,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     // the asynchronous schedule keeps each block area's vacancies in kFlowSlots slots;
     // it is chosen only with room left for vacancies to gather
     std::vector<int32_t> per_block(static_cast<size_t>(nb), 0);
-    bool budget = false;
     for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
       const HostJob& j = ctx->jobs[ji];
-      budget = budget || j.cfg.hop_budget > 0;
       const int nbx = static_cast<int>(j.split[0].size()) - 1, nby = static_cast<int>(j.split[1].size()) - 1;
       for (int32_t k = j.vac0; k < j.vac0 + static_cast<int32_t>(j.nvac); ++k) {
         const int64_t s = vsite[static_cast<size_t>(k)];
@@ -574,7 +575,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     int32_t mx = 0;
     for (int32_t v : per_block) mx = std::max(mx, v);
     // one block gains nothing from running rounds apart
-    ctx->flow_ok = !budget && mx <= kFlowSlots / 2 && nb > 1;
+    ctx->flow_ok = mx <= kFlowSlots / 2 && nb > 1;
   }
   CK(dalloc(&ctx->d_log_count, 1));
   CK(dalloc(&ctx->d_api_total, 1));
@@ -595,12 +596,16 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_counters, 0, 192, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_log_count, 0, 8, ctx->stream));
-  for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
-    HostJob& j = ctx->jobs[ji];
-    if (!j.has_eam) continue;
-    const int e = launch_init_rho(j.d_occ, j.d_rho, hj[ji].sx, hj[ji].sy, hj[ji].sz, ctx->d_pots + j.pot, ctx->d_geo,
-                                  ctx->d_status, ctx->stream);
-    if (e) return fail(ctx, AKMC_ECUDA, std::string("init rho: ") + cuda_name(e));
+  {  // density caches of every EAM job, one launch
+    const akmc_status rt = build_rho_tables(ctx);
+    if (rt != AKMC_OK) return rt;
+    if (ctx->jl.neam > 0) {
+      RoundArgs ra{};
+      ra.jobs = ctx->d_jobs;
+      ra.pots = ctx->d_pots;
+      const int e = launch_init_rho_jobs(ra, ctx->jl, ctx->stream);
+      if (e) return fail(ctx, AKMC_ECUDA, std::string("init rho: ") + cuda_name(e));
+    }
   }
   RoundArgs& a = ctx->args;
   std::memset(&a, 0, sizeof(a));
@@ -792,13 +797,38 @@ AKMC_API akmc_status akmc_restore_snapshot(akmc_ctx* ctx, int32_t job, const uin
   return akmc_sync(ctx);  // B and J leave scope; also reports a lattice with a wrong vacancy count
 }
 
+// Density tiles of the EAM jobs (prefix over jobs) for the one-launch density build.
+static akmc_status build_rho_tables(akmc_ctx* ctx) {
+  if (ctx->d_tile0) return AKMC_OK;
+  std::vector<int32_t> eam_jobs;
+  std::vector<int64_t> tile0{0};
+  for (size_t k = 0; k < ctx->jobs.size(); ++k) {
+    const HostJob& j = ctx->jobs[k];
+    if (!j.has_eam) continue;
+    const int64_t sx = 2 * j.cfg.box[0], sy = j.cfg.box[1], sz = j.cfg.box[2];
+    eam_jobs.push_back(static_cast<int32_t>(k));
+    tile0.push_back(tile0.back() + ((sx + 31) / 32) * ((sy + 7) / 8) * ((sz + 3) / 4));
+  }
+  CK(dalloc(&ctx->d_tile0, tile0.size()));
+  CK(dalloc(&ctx->d_eam_jobs, std::max<size_t>(1, eam_jobs.size())));
+  CK(cudaMemcpy(ctx->d_tile0, tile0.data(), tile0.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  if (!eam_jobs.empty())
+    CK(cudaMemcpy(ctx->d_eam_jobs, eam_jobs.data(), eam_jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  ctx->jl.tile0 = ctx->d_tile0;
+  ctx->jl.eam_jobs = ctx->d_eam_jobs;
+  ctx->jl.neam = static_cast<int32_t>(eam_jobs.size());
+  ctx->jl.eam_tiles = tile0.back();
+  return AKMC_OK;
+}
+
 // Tables of the whole-context transfers, built once after akmc_prepare.
 static akmc_status setup_jobs_load(akmc_ctx* ctx) {
   if (ctx->d_stage) return AKMC_OK;
+  const akmc_status rt = build_rho_tables(ctx);
+  if (rt != AKMC_OK) return rt;
   constexpr int64_t kChunk = 1 << 16;
   std::vector<SiteChunk> ch;
-  std::vector<int32_t> want, eam_jobs;
-  std::vector<int64_t> tile0{0};
+  std::vector<int32_t> want;
   int64_t off = 0;
   for (size_t k = 0; k < ctx->jobs.size(); ++k) {
     const HostJob& j = ctx->jobs[k];
@@ -814,24 +844,14 @@ static akmc_status setup_jobs_load(akmc_ctx* ctx) {
     }
     off += j.nsites;
     want.push_back(static_cast<int32_t>(j.nvac));
-    if (j.has_eam) {
-      const int64_t sx = 2 * j.cfg.box[0], sy = j.cfg.box[1], sz = j.cfg.box[2];
-      eam_jobs.push_back(static_cast<int32_t>(k));
-      tile0.push_back(tile0.back() + ((sx + 31) / 32) * ((sy + 7) / 8) * ((sz + 3) / 4));
-    }
   }
   if (ch.size() > static_cast<size_t>(INT32_MAX)) return fail(ctx, AKMC_EINVAL, "too many sites");
   CK(dalloc(&ctx->d_stage, static_cast<size_t>(off)));
   CK(dalloc(&ctx->d_chunks, ch.size()));
   CK(dalloc(&ctx->d_job_counts, want.size()));
   CK(dalloc(&ctx->d_job_want, want.size()));
-  CK(dalloc(&ctx->d_tile0, tile0.size()));
-  CK(dalloc(&ctx->d_eam_jobs, std::max<size_t>(1, eam_jobs.size())));
   CK(cudaMemcpy(ctx->d_chunks, ch.data(), ch.size() * sizeof(SiteChunk), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_job_want, want.data(), want.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ctx->d_tile0, tile0.data(), tile0.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
-  if (!eam_jobs.empty())
-    CK(cudaMemcpy(ctx->d_eam_jobs, eam_jobs.data(), eam_jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   JobsLoad& L = ctx->jl;
   L.stage = ctx->d_stage;
   L.chunks = ctx->d_chunks;
@@ -839,10 +859,6 @@ static akmc_status setup_jobs_load(akmc_ctx* ctx) {
   L.njobs = static_cast<int32_t>(want.size());
   L.counts = ctx->d_job_counts;
   L.want = ctx->d_job_want;
-  L.tile0 = ctx->d_tile0;
-  L.eam_jobs = ctx->d_eam_jobs;
-  L.neam = static_cast<int32_t>(eam_jobs.size());
-  L.eam_tiles = tile0.back();
   ctx->total_sites = off;
   return AKMC_OK;
 }
@@ -913,9 +929,19 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
       e0 = ctx->ev[0];
       e1 = ctx->ev[1];
     }
-    for (int64_t left = n_rounds; left > 0;) {
-      a.flow_rounds = std::min<int64_t>(left, 1024);
-      left -= a.flow_rounds;
+    // each block runs n_rounds (fewer if its job ends); jobs with a hop budget stop at each
+    // time-step boundary, so their launches run at most to the next one (one more launch for
+    // a job that starts between boundaries)
+    bool budget = false;
+    for (const auto& j : ctx->jobs) budget = budget || j.cfg.hop_budget > 0;
+    {
+      const int e = launch_flow_begin(a, n_rounds, ctx->stream);
+      if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+    }
+    const int64_t per = budget ? 8 : 1024;
+    const int64_t launches = (n_rounds + per - 1) / per + (budget ? 1 : 0);
+    for (int64_t k = 0; k < launches; ++k) {
+      a.flow_rounds = per;
       const int e = launch_flow(a, ctx->flow_grid, ctx->smem, ctx->stream, e0, e1);
       if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
       if (ctx->timing) {
@@ -1032,9 +1058,6 @@ AKMC_API akmc_status akmc_set_round_schedule(akmc_ctx* ctx, int32_t schedule) {
   if (!ctx) return AKMC_EINVAL;
   if (schedule < AKMC_SCHEDULE_AUTO || schedule > AKMC_SCHEDULE_FLOW)
     return fail(ctx, AKMC_EINVAL, "schedule: AKMC_SCHEDULE_AUTO, _ROUNDS or _FLOW");
-  for (const auto& j : ctx->jobs)
-    if (schedule == AKMC_SCHEDULE_FLOW && j.cfg.hop_budget > 0)
-      return fail(ctx, AKMC_EINVAL, "the asynchronous schedule does not serve hop budgets");
   ctx->schedule = schedule;
   return AKMC_OK;
 }

@@ -85,6 +85,7 @@ struct BlockDev {
   int32_t cnt;           // vacancies bucketed into the active sector this round
   int32_t done;          // the job finished at or before this block's last round
   int64_t target;        // asynchronous schedule: round this launch runs the block up to
+  int64_t remaining;     // asynchronous schedule: rounds of the akmc_run_rounds call still to run
 };
 
 enum : uint32_t {
@@ -144,6 +145,7 @@ struct RoundArgs {
 // Kernel launchers (akmc_kernels.cu).
 size_t hop_smem_bytes(int max_region_sites);
 int configure_hop_smem(size_t smem);
+int hop_ctas_per_sm();  // CTAs of the hop kernels the register budget allows per SM
 // ev0/ev1 (cudaEvent_t or null) are recorded around the hop kernel.
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1);
 // Collects the vacancies of one job's lattice into its slice of the vacancy table and sets
@@ -157,6 +159,8 @@ int launch_device_math(const double* x, int64_t n, double* e, double* l, void* s
 // n rounds of every unfinished block under the asynchronous schedule (no job may have a
 // hop budget); grid = persistent CTAs of the flow kernels.
 int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1);
+// Sets every block's remaining rounds to n before the launches of one akmc_run_rounds call.
+int launch_flow_begin(const RoundArgs& a, int64_t n, void* stream);
 
 // Whole-context lattice transfers (akmc_load_occupancies / akmc_get_occupancies): the lattices
 // of all jobs back to back in a staging buffer, cut into chunks of one job each.
@@ -177,6 +181,7 @@ struct JobsLoad {
   int64_t eam_tiles;
 };
 int launch_load_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);
+int launch_init_rho_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);  // uses a.jobs, a.pots
 int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);
 
 // Cu cluster statistics of one job's occupancy (akmc_cluster.cu).  list, parent and size hold

@@ -4,13 +4,13 @@
 // runs as three launches:
 //   k_bucket   one thread per vacancy: find its domain block, keep it if it lies in
 //              the block's active sector, append it to the block's list;
-//   k_hop      one CTA of 9 warps per active block: stage the sector plus a 2-cell
-//              halo (occupancy bytes and the int32 density cache) into shared memory
-//              and run the hop loop there.  Warp w < 8 evaluates jump direction w of a
-//              vacancy (its 32 lanes split the 76 sites of the jump); warp 8 forms the
-//              ordered total, selects, performs the hop and keeps the vacancy list and
-//              the clock; each hop writes its two occupancy bytes and 78 densities
-//              through to global memory;
+//   k_hop      one CTA per active block: stage the sector plus a 2-cell halo (occupancy
+//              bytes and the int32 density cache) into shared memory and run the hop
+//              loop there.  Evaluator warp w evaluates jump directions w, w + kEvalWarps,
+//              ... of a vacancy (its 32 lanes split the 76 sites of a jump); the control
+//              warp forms the ordered total, selects, performs the hop and keeps the
+//              vacancy list and the clock; each hop writes its two occupancy bytes and 78
+//              densities through to global memory;
 //   k_finalize one thread per block: clock of blocks without vacancies, next round.
 // Concurrently active sectors are at least 4 cells apart, so the staged regions of
 // different blocks never overlap and no atomics are needed on the lattice.
@@ -28,8 +28,16 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kStageRows = 4;  // rows of the staged region each warp has in flight
 enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };  // energy kinds, one kernel instance each
-constexpr int kThreads = 288;  // warps 0..7 evaluate jump directions 0..7; warp 8 controls
-constexpr int kCtl = 256;      // control thread: first lane of warp 8
+// CTA shape: kEvalWarps warps evaluate the 8 jump directions (warp w takes jumps w, w +
+// kEvalWarps, ...), one more warp controls the hop loop.
+constexpr int kEvalWarps = 8;
+constexpr int kJumpsPerWarp = 8 / kEvalWarps;
+constexpr int kThreads = 32 * (kEvalWarps + 1);
+constexpr int kCtl = 32 * kEvalWarps;  // control thread: first lane of the control warp
+static_assert(8 % kEvalWarps == 0, "whole jump directions per warp");
+// CTAs per SM the register budget is cut for: two 5-warp CTAs fit (10 warps, at most 3 per SM
+// partition), two 9-warp ones would cut a thread to 96 registers.
+constexpr int kCtasPerSm = kEvalWarps <= 4 ? 2 : 1;
 
 __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >= m ? v - m : v); }
 
@@ -289,10 +297,9 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
 //             merge by a xor butterfly (16, 8, 4, 2, 1), then the moving atom's own
 //             embedding change is added.
 template <int KIND>
-__device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, const FTab& FT,
+__device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, int b, const FTab& FT,
                              const JobC& jc, const int32_t (&jr)[2][3], double* de_out) {
   const int lane = threadIdx.x & 31;
-  const int b = threadIdx.x >> 5;
   const int q = lane;
   const int l = sm.vloc[k];
   const int p = l & 1;
@@ -436,8 +443,9 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
 #endif
 
 // The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
-// Warps 0..7 evaluate rates (warp b = jump b) and refresh densities; warp 8 keeps the
-// ordered vacancy list, selects, performs the occupancy swap and runs the clock.
+// The evaluator warps evaluate rates (warp w: jumps w, w + kEvalWarps, ...) and refresh
+// densities; the control warp keeps the ordered vacancy list, selects, performs the occupancy
+// swap and runs the clock.
 // vlist holds the ids of the cnt_in vacancies inside the sector (any order).  Returns
 // false, uniformly, when the sector's clock is already past its window: nothing ran and
 // the vacancy arrays of sm were not filled.
@@ -446,7 +454,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
                           const int32_t* vlist, int cnt_in) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const bool evaluator = warp < 8;
+  const bool evaluator = warp < kEvalWarps;
 #ifdef AKMC_PHASE_PROFILE
   long long tph = clock64();
 #endif
@@ -620,15 +628,18 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
     __syncthreads();
   }
-  // this lane's entries of its warp's jump list, both x parities
-  int32_t jr[2][3];
+  // this lane's entries of its warp's jump lists, both x parities
+  int32_t jr[kJumpsPerWarp][2][3];
 #pragma unroll
-  for (int u = 0; u < 3; ++u) {
-    const int i = lane + 32 * u;
-    const bool in = eam && evaluator && i < kJumpN;
-    jr[0][u] = in ? sm.jl[0][warp][i] : 0;
-    jr[1][u] = in ? sm.jl[1][warp][i] : 0;
-  }
+  for (int jj = 0; jj < kJumpsPerWarp; ++jj)
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int i = lane + 32 * u;
+      const bool in = eam && evaluator && i < kJumpN;
+      const int b = warp + kEvalWarps * jj;
+      jr[jj][0][u] = in ? sm.jl[0][b][i] : 0;
+      jr[jj][1][u] = in ? sm.jl[1][b][i] : 0;
+    }
 
   // The 78 exact density deltas of the hop just performed (ABVIModel::perform's lattice
   // change seen by the density cache), in shared memory and through to global memory.
@@ -647,7 +658,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   };
 
   // Hop loop, two CTA barriers per hop:
-  //  (E) warps 0..7 refresh the densities of the hop just performed, then evaluate the
+  //  (E) the evaluator warps refresh the densities of the hop just performed, then evaluate the
   //      vacancies it made dirty; the control warp counts them, moves the hopped vacancy
   //      in the ordered list, runs the clock of the hop, decides whether the sector is
   //      done and draws the next selection uniform ahead of time;
@@ -678,7 +689,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     if (evaluator) {
       if (eam && hopped) {
         if (tid < kRefreshN) refresh(tid);
-        asm volatile("bar.sync 1, 256;" ::: "memory");  // the evaluator warps only
+        asm volatile("bar.sync 1, %0;" ::"n"(kCtl) : "memory");  // the evaluator warps only
       }
       if (first || hopped) {
         for (int base = 0; base < cnt; base += 32) {
@@ -686,7 +697,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           while (m) {
             const int k = base + __ffs(m) - 1;
             m &= m - 1;
-            eval_vacancy<KIND>(sm, occ_s, rho_s, k, FT, jc, jr, de_out);
+#pragma unroll
+            for (int jj = 0; jj < kJumpsPerWarp; ++jj)
+              eval_vacancy<KIND>(sm, occ_s, rho_s, k, warp + kEvalWarps * jj, FT, jc, jr[jj], de_out);
           }
         }
       }
@@ -761,7 +774,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     AKMC_PHASE(first ? 2 : 5);
     first = false;
     if (sm.ctl_next_stop) break;
-    if (warp == 8) {
+    if (warp == kEvalWarps) {
       if (lane == 0) {
         // ordered total; the running sums are kept: they are the selection scan's
         // accumulator values (ABVIModel::select, kmc.cpp:242-309) in the same order.
@@ -1041,7 +1054,7 @@ __device__ __forceinline__ int job_kind(const JobDev& J) {
 // One kernel per energy kind, so each holds only its own hop loop (instruction-cache
 // footprint); items of other kinds are left to their kernel.
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1) k_hop(RoundArgs a) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
   if (static_cast<int>(blockIdx.x) >= na) return;
@@ -1273,7 +1286,7 @@ constexpr int kFlowTake = kThreads;
 constexpr int kFlowChain = 1;
 
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1) k_flow(RoundArgs a) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   Smem* sm0 = reinterpret_cast<Smem*>(smem);
   const int tid = threadIdx.x;
@@ -1463,8 +1476,13 @@ __global__ void k_flow_prep(RoundArgs a) {
   if (gb >= a.nblocks) return;
   BlockDev& B = a.blocks[gb];
   const JobDev& J = a.jobs[B.job];
-  int64_t t = B.done ? B.round : B.round + a.flow_rounds;
+  // up to flow_rounds of the block's remaining rounds; a job with a hop budget stops at its next
+  // time-step boundary, where k_flow_finalize checks the budget
+  int64_t L = B.remaining < a.flow_rounds ? B.remaining : a.flow_rounds;
+  if (J.hop_budget > 0 && L > 8 - (B.round & 7)) L = 8 - (B.round & 7);
+  int64_t t = B.done ? B.round : B.round + L;
   if (J.max_rounds > 0 && t > J.max_rounds) t = J.max_rounds > B.round ? J.max_rounds : B.round;
+  B.remaining -= t - B.round;
   B.target = t;
   B.cnt = 0;
   a.lease[gb] = 0;
@@ -1498,7 +1516,10 @@ __global__ void k_flow_finalize(RoundArgs a) {
   BlockDev& B = a.blocks[gb];
   JobDev& J = a.jobs[B.job];
   B.cnt = 0;
-  const int done = J.max_rounds > 0 && B.round >= J.max_rounds;
+  // J.hops holds the launch's hops (added when k_flow ended); all blocks of a budget job stop
+  // at the same time-step boundary
+  const int done = (J.max_rounds > 0 && B.round >= J.max_rounds) ||
+                   (J.hop_budget > 0 && (B.round & 7) == 0 && J.hops >= J.hop_budget);
   B.done = done;
   if (B.local_id == 0) {
     J.round = B.round;
@@ -1528,7 +1549,9 @@ __global__ void k_finalize(RoundArgs a) {
     B.evo[sec] += sector_time;
   }
   B.round += 1;
-  const int done = (J.hop_budget > 0 && J.hops >= J.hop_budget) || (J.max_rounds > 0 && B.round >= J.max_rounds);
+  // a hop budget is checked at time-step boundaries (every 8 rounds)
+  const int done = (J.hop_budget > 0 && (B.round & 7) == 0 && J.hops >= J.hop_budget) ||
+                   (J.max_rounds > 0 && B.round >= J.max_rounds);
   B.done = done;
   if (B.local_id == 0) {
     J.round = B.round;
@@ -1779,6 +1802,16 @@ int launch_api(const RoundArgs& a, size_t smem, void* stream) {
   return static_cast<int>(cudaGetLastError());
 }
 
+__global__ void k_flow_begin(RoundArgs a, int64_t n) {
+  const int gb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gb < a.nblocks) a.blocks[gb].remaining = n;
+}
+
+int launch_flow_begin(const RoundArgs& a, int64_t n, void* stream) {
+  k_flow_begin<<<(a.nblocks + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(a, n);
+  return static_cast<int>(cudaGetLastError());
+}
+
 int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* ev0, void* ev1) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaMemsetAsync(a.flow_need, 0, 3 * sizeof(int32_t), st);
@@ -1793,6 +1826,8 @@ int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* e
   k_flow_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
 }
+
+int hop_ctas_per_sm() { return kCtasPerSm; }
 
 int configure_hop_smem(size_t smem) {
   cudaError_t e = cudaFuncSetAttribute(k_hop<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1825,17 +1860,22 @@ __global__ void k_check_vacancy_count(const int32_t* count, int32_t want, unsign
   if (*count != want) atomicOr(status, kErrVacCount);
 }
 
+int launch_init_rho_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
+  if (L.neam > 0)
+    k_init_rho_jobs<<<static_cast<int>(std::min<int64_t>(L.eam_tiles, 148 * 16)), 256, 0,
+                      static_cast<cudaStream_t>(stream)>>>(a, L.tile0, L.eam_jobs, L.neam);
+  return static_cast<int>(cudaGetLastError());
+}
+
 int launch_load_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(L.counts, 0, sizeof(int32_t) * L.njobs, st);
   if (e != cudaSuccess) return static_cast<int>(e);
   k_scatter_collect<<<L.nchunks, 256, 0, st>>>(a, L.stage, L.chunks, L.counts);
   k_check_counts<<<(L.njobs + 127) / 128, 128, 0, st>>>(L.counts, L.want, L.njobs, a.status);
-  if (L.neam > 0)
-    k_init_rho_jobs<<<static_cast<int>(std::min<int64_t>(L.eam_tiles, 148 * 16)), 256, 0, st>>>(a, L.tile0, L.eam_jobs,
-                                                                                                L.neam);
-  return static_cast<int>(cudaGetLastError());
+  return launch_init_rho_jobs(a, L, stream);
 }
+
 
 int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
   k_gather<<<L.nchunks, 256, 0, static_cast<cudaStream_t>(stream)>>>(a, L.stage, L.chunks);

@@ -1075,10 +1075,12 @@ int ao_run_rounds(void* h, int64_t n_rounds) {
   }
   return 0;
 }
+// A hop budget is checked at sublattice time-step boundaries (every 8 sector rounds): the job
+// ends at the end of the first time step at which its hop count has reached the budget.
 int ao_run(void* h, int64_t hop_budget, int64_t max_rounds) {
   Job* J = static_cast<Job*>(h);
   for (int64_t i = 0; i < max_rounds; ++i) {
-    if (hop_budget > 0 && J->hops >= hop_budget) break;
+    if (hop_budget > 0 && J->round % 8 == 0 && J->hops >= hop_budget) break;
     const int r = J->run_round();
     if (r) return r;
   }

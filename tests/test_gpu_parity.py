@@ -118,7 +118,7 @@ def test_batched_jobs_of_different_shapes(ak):
     eng.close()
 
 
-def test_hop_budget_stops_at_round_boundary(ak):
+def test_hop_budget_stops_at_time_step_boundary(ak):
     o = oracle_job(box=(20, 20, 20))
     with ak.Engine(event_log_capacity=1 << 20) as eng:
         device_job(eng, o, (20, 20, 20), hop_budget=2000)
@@ -127,8 +127,36 @@ def test_hop_budget_stops_at_round_boundary(ak):
         eng.run(100000)
         st = eng.job_state(0)
         assert st["done"] and st["hops"] == o.hops and st["round"] == o.round
-        assert o.hops >= 2000
+        assert o.hops >= 2000 and o.round % 8 == 0
         assert np.array_equal(eng.occupancy(0), o.occupancy())
+
+
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_hop_budgets_under_both_schedules(ak, schedule):
+    # a multi-block job with a budget next to one without, 93 rounds requested (not a multiple
+    # of 8): the budget job stops at a time-step boundary, the other runs all 93 rounds
+    kws = [dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=40,
+                temperature=563.0, seed=21),
+           dict(box=(24, 24, 24), blocks=(2, 1, 1), model=po.MODEL_EAM, precision=po.FP32C, n_vacancies=10, seed=22)]
+    budget = 2500
+    with ak.Engine(event_log_capacity=1 << 20) as eng:
+        eng.set_round_schedule(schedule)
+        oracles = [oracle_job(**kw) for kw in kws]
+        for k, (kw, o) in enumerate(zip(kws, oracles)):
+            dkw = {key: kw[key] for key in ("box", "blocks", "model", "precision", "seed", "temperature") if key in kw}
+            device_job(eng, o, hop_budget=budget if k == 0 else 0, **dkw)
+        eng.prepare()
+        assert eng.round_schedule() == schedule
+        eng.run_rounds(93)
+        eng.sync()
+        oracles[0].run(budget, 93)
+        oracles[1].run_rounds(93)
+        ev = eng.events()
+        for k, o in enumerate(oracles):
+            check_job(eng, o, k, ev)
+        st = eng.job_state(0)
+        assert st["done"] and st["round"] % 8 == 0 and st["round"] < 93 and st["hops"] >= budget
+        assert eng.job_state(1)["round"] == 93
 
 
 def test_job_without_vacancies_only_advances_clocks(ak):
