@@ -143,6 +143,7 @@ def run_serve(args, ak, device):
         lat.append(res["finish_s"] - res["submit_s"])
         hops += res["hops"]
     wall = time.perf_counter() - t0
+    prof = srv.profile()
     srv.close()
     lat = np.array(lat)
     line = {
@@ -154,7 +155,7 @@ def run_serve(args, ak, device):
                    "jobs": len(jobs), "lanes": args.serve_lanes, "chunk_rounds": args.serve_chunk,
                    "offered_hops_per_s": sum(j["hop_budget"] for j in jobs) / args.serve_seconds},
         "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-        "latency_max_s": float(lat.max()), "wall_s": wall,
+        "latency_max_s": float(lat.max()), "wall_s": wall, "server_profile": prof,
     }
     print(json.dumps(line))
 

@@ -369,6 +369,12 @@ AKMC_API akmc_status akmc_server_wait(akmc_server* s, int64_t ticket, double tim
 AKMC_API akmc_status akmc_server_stats(akmc_server* s, int64_t* queued, int64_t* running, int64_t* done);
 /* Finishes the running batches, fails the queued jobs (status AKMC_ESTATE) and frees the
  * server. */
+/* Where the lanes' time went, summed over lanes: seconds8 = [0] building contexts (create,
+ * add, prepare, restore, and saving and tearing down at a refill), [1] running chunks (rounds
+ * and the job-state read), [2] reading results, [3] waiting for work; parts of [0]: [4] create
+ * and add, [5] prepare, [6] restore, [7] saving the snapshots at a refill; counts3 = chunks
+ * run, live jobs summed over chunks (their ratio is the mean batch), contexts built. */
+AKMC_API akmc_status akmc_server_profile(akmc_server* s, double* seconds8, int64_t* counts3);
 AKMC_API akmc_status akmc_server_shutdown(akmc_server* s);
 
 #ifdef __cplusplus

@@ -129,9 +129,15 @@ akmc_status fail(akmc_ctx* c, akmc_status s, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(ctx, AKMC_ECUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
   } while (0)
 
+// Device memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the context's stream):
+// unlike cudaMalloc and cudaFree, neither waits for other contexts' work on the device, so
+// contexts that build and tear down while others run (the server's lanes) do not stall.
 template <class T>
-cudaError_t dalloc(T** p, size_t n) {
-  return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+cudaError_t dalloc(cudaStream_t s, T** p, size_t n) {
+  return cudaMallocAsync(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T), s);
+}
+void dfree(cudaStream_t s, void* p) {
+  if (p) cudaFreeAsync(p, s);
 }
 
 akmc_status check_status(akmc_ctx* ctx) {
@@ -154,20 +160,20 @@ akmc_status check_status(akmc_ctx* ctx) {
 void free_device(akmc_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
   ctx->ev.clear();
-  cudaFree(ctx->d_vac_count);
+  dfree(ctx->stream, ctx->d_vac_count);
   ctx->d_vac_count = nullptr;
   void* flow_ptrs[] = {ctx->d_lease, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vcount, ctx->d_flow};
-  for (void* p : flow_ptrs) cudaFree(p);
+  for (void* p : flow_ptrs) dfree(ctx->stream, p);
   ctx->d_lease = nullptr;
   ctx->d_vclaim = ctx->d_vvalid = nullptr;
   ctx->d_vslot = ctx->d_vcount = ctx->d_flow = nullptr;
-  cudaFree(ctx->d_cl);
-  cudaFree(ctx->d_cl_misc);
+  dfree(ctx->stream, ctx->d_cl);
+  dfree(ctx->stream, ctx->d_cl_misc);
   ctx->d_cl = nullptr;
   ctx->d_cl_misc = nullptr;
   ctx->cl_sites = 0;
   void* jl_ptrs[] = {ctx->d_stage, ctx->d_chunks, ctx->d_job_counts, ctx->d_job_want, ctx->d_tile0, ctx->d_eam_jobs};
-  for (void* p : jl_ptrs) cudaFree(p);
+  for (void* p : jl_ptrs) dfree(ctx->stream, p);
   ctx->d_stage = nullptr;
   ctx->d_chunks = nullptr;
   ctx->d_job_counts = ctx->d_job_want = ctx->d_eam_jobs = nullptr;
@@ -179,14 +185,14 @@ void free_device(akmc_ctx* ctx) {
   ctx->graph = nullptr;
   ctx->graph_def = nullptr;
   for (auto& j : ctx->jobs) {
-    cudaFree(j.d_occ);
-    cudaFree(j.d_rho);
+    dfree(ctx->stream, j.d_occ);
+    dfree(ctx->stream, j.d_rho);
     j.d_occ = nullptr;
     j.d_rho = nullptr;
   }
   for (auto& p : ctx->pots) {
-    cudaFree(p.d_coef);
-    cudaFree(p.d_f32);
+    dfree(ctx->stream, p.d_coef);
+    dfree(ctx->stream, p.d_f32);
     p.d_coef = nullptr;
     p.d_f32 = nullptr;
   }
@@ -194,7 +200,7 @@ void free_device(akmc_ctx* ctx) {
                   ctx->d_n_active, ctx->d_pots, ctx->d_geo, ctx->d_log, ctx->d_log_count, ctx->d_status,
                   ctx->d_counters, ctx->d_api_total, ctx->d_api_event, ctx->d_api_de, ctx->d_api_rates,
                   ctx->d_api_sites, ctx->d_api_count};
-  for (void* p : ptrs) cudaFree(p);
+  for (void* p : ptrs) dfree(ctx->stream, p);
   ctx->d_jobs = nullptr;
   ctx->d_blocks = nullptr;
   ctx->d_vac_site = ctx->d_vac_job = ctx->d_blk_list = ctx->d_active = ctx->d_n_active = nullptr;
@@ -245,11 +251,23 @@ struct SnapBlock {
   uint64_t xs[4], xt[4];
   int32_t done, pad;
 };
-constexpr uint32_t kSnapVersion = 1;
+constexpr uint32_t kSnapVersion = 2;
 
+// Checksum of the snapshot payload: an FNV-1a step per 64-bit little-endian word (the tail
+// zero-padded and tagged with its length), with an xor-shift after each multiply so that
+// high bits mix down.  It detects damaged or truncated buffers; it is not cryptographic.
 uint64_t fnv1a(const uint8_t* p, size_t n, uint64_t h = 1469598103934665603ull) {
-  for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
-  return h;
+  size_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t w;
+    std::memcpy(&w, p + i, 8);
+    h = (h ^ w) * 1099511628211ull;
+    h ^= h >> 29;
+  }
+  uint64_t w = 0;
+  std::memcpy(&w, p + i, n - i);
+  h = (h ^ w ^ (static_cast<uint64_t>(n - i) << 56)) * 1099511628211ull;
+  return h ^ (h >> 29);
 }
 
 uint64_t eam_hash(const HostJob& j) {
@@ -317,6 +335,13 @@ AKMC_API akmc_status akmc_create(const akmc_context_config* cfg, akmc_ctx** out)
     }
     ctx->own_stream = true;
   }
+  // freed device memory stays in the device's default pool (this process only), so the next
+  // context reuses it without a round trip through the driver
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->cfg.device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   *out = ctx;
   return AKMC_OK;
 }
@@ -326,6 +351,7 @@ AKMC_API akmc_status akmc_destroy(akmc_ctx* ctx) {
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_device(ctx);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // the stream-ordered frees
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return AKMC_OK;
@@ -453,7 +479,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
                       2.0 * j.cfg.lattice_const < j.cfg.cutoff_radius))
       return fail(ctx, AKMC_EINVAL, "the EAM path needs exactly the 5 BCC shells inside the cutoff");
   build_geometry(geo, 5);
-  CK(dalloc(&ctx->d_geo, 1));
+  CK(dalloc(ctx->stream, &ctx->d_geo, 1));
   CK(cudaMemcpyAsync(ctx->d_geo, &geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
   std::vector<Potential> hp;
   for (auto& p : ctx->pots) {
@@ -471,8 +497,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
       c32[4 * k + 3] = f.c2;
       c32[4 * static_cast<size_t>(kTabN) + k] = f.c3;
     }
-    CK(dalloc(&p.d_coef, c64.size()));
-    CK(dalloc(&p.d_f32, c32.size()));
+    CK(dalloc(ctx->stream, &p.d_coef, c64.size()));
+    CK(dalloc(ctx->stream, &p.d_f32, c32.size()));
     CK(cudaMemcpyAsync(p.d_coef, c64.data(), c64.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(p.d_f32, c32.data(), c32.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));  // the staging vectors go out of scope
@@ -483,7 +509,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     P.F32b = p.d_f32 + 4 * static_cast<size_t>(kTabN);
     hp.push_back(P);
   }
-  CK(dalloc(&ctx->d_pots, hp.size()));
+  CK(dalloc(ctx->stream, &ctx->d_pots, hp.size()));
   CK(cudaMemcpyAsync(ctx->d_pots, hp.data(), hp.size() * sizeof(Potential), cudaMemcpyHostToDevice, ctx->stream));
 
   // jobs, blocks, vacancies
@@ -492,9 +518,9 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   std::vector<int32_t> vsite(static_cast<size_t>(nv)), vjob(static_cast<size_t>(nv));
   for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
     HostJob& j = ctx->jobs[ji];
-    CK(dalloc(&j.d_occ, static_cast<size_t>(j.nsites)));
+    CK(dalloc(ctx->stream, &j.d_occ, static_cast<size_t>(j.nsites)));
     CK(cudaMemcpyAsync(j.d_occ, j.occ.data(), static_cast<size_t>(j.nsites), cudaMemcpyHostToDevice, ctx->stream));
-    if (j.has_eam) CK(dalloc(&j.d_rho, static_cast<size_t>(j.nsites)));
+    if (j.has_eam) CK(dalloc(ctx->stream, &j.d_rho, static_cast<size_t>(j.nsites)));
     JobDev& J = hj[ji];
     std::memset(&J, 0, sizeof(J));
     J.occ = j.d_occ;
@@ -537,22 +563,22 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
         ++k;
       }
   }
-  CK(dalloc(&ctx->d_jobs, hj.size()));
-  CK(dalloc(&ctx->d_blocks, hb.size()));
-  CK(dalloc(&ctx->d_vac_site, vsite.size()));
-  CK(dalloc(&ctx->d_vac_job, vjob.size()));
-  CK(dalloc(&ctx->d_blk_list, static_cast<size_t>(nb) * kMaxV));
-  CK(dalloc(&ctx->d_active, static_cast<size_t>(nb)));
-  CK(dalloc(&ctx->d_n_active, 1));
-  CK(dalloc(&ctx->d_status, 1));
-  CK(dalloc(&ctx->d_counters, 24));
-  CK(dalloc(&ctx->d_vac_count, 1));
-  CK(dalloc(&ctx->d_lease, static_cast<size_t>(nb)));
-  CK(dalloc(&ctx->d_vclaim, static_cast<size_t>(nb)));
-  CK(dalloc(&ctx->d_vvalid, static_cast<size_t>(nb)));
-  CK(dalloc(&ctx->d_vslot, static_cast<size_t>(nb) * kFlowSlots));
-  CK(dalloc(&ctx->d_vcount, static_cast<size_t>(nb)));
-  CK(dalloc(&ctx->d_flow, 6));
+  CK(dalloc(ctx->stream, &ctx->d_jobs, hj.size()));
+  CK(dalloc(ctx->stream, &ctx->d_blocks, hb.size()));
+  CK(dalloc(ctx->stream, &ctx->d_vac_site, vsite.size()));
+  CK(dalloc(ctx->stream, &ctx->d_vac_job, vjob.size()));
+  CK(dalloc(ctx->stream, &ctx->d_blk_list, static_cast<size_t>(nb) * kMaxV));
+  CK(dalloc(ctx->stream, &ctx->d_active, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_n_active, 1));
+  CK(dalloc(ctx->stream, &ctx->d_status, 1));
+  CK(dalloc(ctx->stream, &ctx->d_counters, 24));
+  CK(dalloc(ctx->stream, &ctx->d_vac_count, 1));
+  CK(dalloc(ctx->stream, &ctx->d_lease, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_vclaim, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_vvalid, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_vslot, static_cast<size_t>(nb) * kFlowSlots));
+  CK(dalloc(ctx->stream, &ctx->d_vcount, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_flow, 6));
   {
     // the asynchronous schedule keeps each block area's vacancies in kFlowSlots slots;
     // it is chosen only with room left for vacancies to gather
@@ -577,15 +603,15 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     // one block gains nothing from running rounds apart
     ctx->flow_ok = mx <= kFlowSlots / 2 && nb > 1;
   }
-  CK(dalloc(&ctx->d_log_count, 1));
-  CK(dalloc(&ctx->d_api_total, 1));
-  CK(dalloc(&ctx->d_api_event, 1));
-  CK(dalloc(&ctx->d_api_de, static_cast<size_t>(kMaxV) * 8));
-  CK(dalloc(&ctx->d_api_rates, static_cast<size_t>(kMaxV) * 8));
-  CK(dalloc(&ctx->d_api_sites, static_cast<size_t>(kMaxV)));
-  CK(dalloc(&ctx->d_api_count, 1));
+  CK(dalloc(ctx->stream, &ctx->d_log_count, 1));
+  CK(dalloc(ctx->stream, &ctx->d_api_total, 1));
+  CK(dalloc(ctx->stream, &ctx->d_api_event, 1));
+  CK(dalloc(ctx->stream, &ctx->d_api_de, static_cast<size_t>(kMaxV) * 8));
+  CK(dalloc(ctx->stream, &ctx->d_api_rates, static_cast<size_t>(kMaxV) * 8));
+  CK(dalloc(ctx->stream, &ctx->d_api_sites, static_cast<size_t>(kMaxV)));
+  CK(dalloc(ctx->stream, &ctx->d_api_count, 1));
   CK(cudaMemsetAsync(ctx->d_api_count, 0, sizeof(int32_t), ctx->stream));
-  if (ctx->cfg.event_log_capacity > 0) CK(dalloc(&ctx->d_log, static_cast<size_t>(ctx->cfg.event_log_capacity)));
+  if (ctx->cfg.event_log_capacity > 0) CK(dalloc(ctx->stream, &ctx->d_log, static_cast<size_t>(ctx->cfg.event_log_capacity)));
   CK(cudaMemcpyAsync(ctx->d_jobs, hj.data(), hj.size() * sizeof(JobDev), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_blocks, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
   if (nv) {
@@ -809,8 +835,8 @@ static akmc_status build_rho_tables(akmc_ctx* ctx) {
     eam_jobs.push_back(static_cast<int32_t>(k));
     tile0.push_back(tile0.back() + ((sx + 31) / 32) * ((sy + 7) / 8) * ((sz + 3) / 4));
   }
-  CK(dalloc(&ctx->d_tile0, tile0.size()));
-  CK(dalloc(&ctx->d_eam_jobs, std::max<size_t>(1, eam_jobs.size())));
+  CK(dalloc(ctx->stream, &ctx->d_tile0, tile0.size()));
+  CK(dalloc(ctx->stream, &ctx->d_eam_jobs, std::max<size_t>(1, eam_jobs.size())));
   CK(cudaMemcpy(ctx->d_tile0, tile0.data(), tile0.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   if (!eam_jobs.empty())
     CK(cudaMemcpy(ctx->d_eam_jobs, eam_jobs.data(), eam_jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -846,10 +872,10 @@ static akmc_status setup_jobs_load(akmc_ctx* ctx) {
     want.push_back(static_cast<int32_t>(j.nvac));
   }
   if (ch.size() > static_cast<size_t>(INT32_MAX)) return fail(ctx, AKMC_EINVAL, "too many sites");
-  CK(dalloc(&ctx->d_stage, static_cast<size_t>(off)));
-  CK(dalloc(&ctx->d_chunks, ch.size()));
-  CK(dalloc(&ctx->d_job_counts, want.size()));
-  CK(dalloc(&ctx->d_job_want, want.size()));
+  CK(dalloc(ctx->stream, &ctx->d_stage, static_cast<size_t>(off)));
+  CK(dalloc(ctx->stream, &ctx->d_chunks, ch.size()));
+  CK(dalloc(ctx->stream, &ctx->d_job_counts, want.size()));
+  CK(dalloc(ctx->stream, &ctx->d_job_want, want.size()));
   CK(cudaMemcpy(ctx->d_chunks, ch.data(), ch.size() * sizeof(SiteChunk), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_job_want, want.data(), want.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   JobsLoad& L = ctx->jl;
@@ -1311,13 +1337,13 @@ AKMC_API akmc_status akmc_job_cluster_stats(akmc_ctx* ctx, int32_t job, int64_t*
   CK(cudaSetDevice(ctx->cfg.device));
   if (ctx->cl_sites < j.nsites) {
     CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->d_cl);
+    dfree(ctx->stream, ctx->d_cl);
     ctx->d_cl = nullptr;
     ctx->cl_sites = 0;
-    CK(dalloc(&ctx->d_cl, static_cast<size_t>(3 * j.nsites)));
+    CK(dalloc(ctx->stream, &ctx->d_cl, static_cast<size_t>(3 * j.nsites)));
     ctx->cl_sites = j.nsites;
   }
-  if (!ctx->d_cl_misc) CK(dalloc(&ctx->d_cl_misc, 2 + AKMC_CLUSTER_MAX_BINS));
+  if (!ctx->d_cl_misc) CK(dalloc(ctx->stream, &ctx->d_cl_misc, 2 + AKMC_CLUSTER_MAX_BINS));
   ClusterArgs c{};
   c.occ = j.d_occ;
   c.ns = j.nsites;
@@ -1347,17 +1373,17 @@ AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n,
   if (!ctx || !x || !exp_out || !log_out || n <= 0) return AKMC_EINVAL;
   CK(cudaSetDevice(ctx->cfg.device));
   double *dx = nullptr, *de = nullptr, *dl = nullptr;
-  CK(dalloc(&dx, static_cast<size_t>(n)));
-  CK(dalloc(&de, static_cast<size_t>(n)));
-  CK(dalloc(&dl, static_cast<size_t>(n)));
+  CK(dalloc(ctx->stream, &dx, static_cast<size_t>(n)));
+  CK(dalloc(ctx->stream, &de, static_cast<size_t>(n)));
+  CK(dalloc(ctx->stream, &dl, static_cast<size_t>(n)));
   cudaMemcpyAsync(dx, x, static_cast<size_t>(n) * 8, cudaMemcpyHostToDevice, ctx->stream);
   const int e = launch_device_math(dx, n, de, dl, ctx->stream);
   cudaMemcpyAsync(exp_out, de, static_cast<size_t>(n) * 8, cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(log_out, dl, static_cast<size_t>(n) * 8, cudaMemcpyDeviceToHost, ctx->stream);
   const cudaError_t se = cudaStreamSynchronize(ctx->stream);
-  cudaFree(dx);
-  cudaFree(de);
-  cudaFree(dl);
+  dfree(ctx->stream, dx);
+  dfree(ctx->stream, de);
+  dfree(ctx->stream, dl);
   if (e) return fail(ctx, AKMC_ECUDA, cuda_name(e));
   if (se != cudaSuccess) return fail(ctx, AKMC_ECUDA, cudaGetErrorString(se));
   return AKMC_OK;

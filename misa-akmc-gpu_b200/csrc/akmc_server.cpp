@@ -6,8 +6,9 @@
 // the budget, as soon as that job is done.  When an eighth of a batch has finished and queued
 // jobs fit, the lane refills: the running jobs are saved as restart snapshots, the context is
 // rebuilt with them and the newly admitted jobs, and the snapshots are restored, so every
-// job's trajectory is exactly the one it has alone.  Lanes overlap on the GPU.  All shared
-// state is under one mutex; the device work runs outside it.
+// job's trajectory is exactly the one it has alone.  A lane also refills, after 8 chunks, when
+// at least as many jobs wait as it runs.  Lanes overlap on the GPU.  All shared state is under
+// one mutex; the device work runs outside it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -58,6 +59,17 @@ struct akmc_server {
   int64_t running = 0;  // jobs in running batches
   bool stopping = false;
   std::vector<std::thread> lanes;
+  // profile, summed over lanes (under the mutex): seconds building contexts (create, add,
+  // prepare, restore), running chunks (rounds and the job-state read), reading results, and
+  // waiting for work; chunks run, live jobs summed over chunks, contexts built
+  double t_build = 0, t_run = 0, t_publish = 0, t_wait = 0;
+  double t_add = 0, t_prepare = 0, t_restore = 0, t_save = 0;  // parts of t_build
+  int64_t n_chunks = 0, n_live = 0, n_builds = 0;
+  void add_time(double& slot, std::chrono::steady_clock::time_point since) {
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - since).count();
+    std::lock_guard<std::mutex> lk(m);
+    slot += dt;
+  }
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
   double now() const {
@@ -103,6 +115,7 @@ struct akmc_server {
   // Runs `live` until every job is done, refilling from the queue on the way.
   void run_batch(std::vector<std::shared_ptr<SJob>>& live) {
     while (!live.empty()) {
+      auto tb = std::chrono::steady_clock::now();
       akmc_context_config cc{};
       cc.device = cfg.device;
       cc.graph_rounds = cfg.chunk_rounds;
@@ -113,6 +126,7 @@ struct akmc_server {
         live.clear();
         return;
       }
+      auto tpart = std::chrono::steady_clock::now();
       std::vector<std::shared_ptr<SJob>> in;  // jobs of this context, by job id
       for (auto& j : live) {
         akmc_job_config c = j->cfg;
@@ -122,19 +136,37 @@ struct akmc_server {
         if (s != AKMC_OK) publish(j, s, ctx);
         else in.push_back(j);
       }
+      add_time(t_add, tpart);
+      tpart = std::chrono::steady_clock::now();
       if (!in.empty()) st = akmc_prepare(ctx);
+      add_time(t_prepare, tpart);
+      tpart = std::chrono::steady_clock::now();
       for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k)
         if (!in[k]->snap.empty())
           st = akmc_restore_snapshot(ctx, static_cast<int32_t>(k), in[k]->snap.data(),
                                      static_cast<int64_t>(in[k]->snap.size()));
+      add_time(t_restore, tpart);
+      add_time(t_build, tb);
+      {
+        std::lock_guard<std::mutex> lk(m);
+        ++n_builds;
+      }
       std::vector<bool> over(in.size(), false);
       std::vector<akmc_job_state> js(in.size());
-      size_t left = in.size(), finished = 0;
+      size_t left = in.size(), finished = 0, chunks_here = 0;
       const size_t refill_after = std::max<size_t>(1, in.size() / 8);
       bool refill = false;
       while (st == AKMC_OK && left > 0 && !refill) {
+        auto tr = std::chrono::steady_clock::now();
         st = akmc_run_rounds(ctx, cfg.chunk_rounds);
         if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(in.size()));
+        add_time(t_run, tr);
+        {
+          std::lock_guard<std::mutex> lk(m);
+          ++n_chunks;
+          n_live += static_cast<int64_t>(left);
+        }
+        auto tp = std::chrono::steady_clock::now();
         for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k) {
           if (over[k] || !js[k].done) continue;
           auto& j = in[k];
@@ -149,12 +181,19 @@ struct akmc_server {
           --left;
           ++finished;
         }
-        if (st == AKMC_OK && left > 0 && finished >= refill_after) {
+        add_time(t_publish, tp);
+        ++chunks_here;
+        if (st == AKMC_OK && left > 0) {
+          // refill when an eighth of the batch is done, or when at least as many jobs wait as
+          // run (a small early batch of long jobs must not hold the queue back)
           std::lock_guard<std::mutex> lk(m);
-          refill = !stopping && fits_locked() && static_cast<int32_t>(left) < cfg.max_batch_jobs;
+          const bool grow = queue.size() >= left && chunks_here >= 8;
+          refill = !stopping && fits_locked() && static_cast<int32_t>(left) < cfg.max_batch_jobs &&
+                   (finished >= refill_after || grow);
         }
       }
       live.clear();
+      tb = std::chrono::steady_clock::now();
       for (size_t k = 0; k < in.size(); ++k) {
         if (over[k]) continue;
         if (st != AKMC_OK) {
@@ -172,7 +211,9 @@ struct akmc_server {
         if (st != AKMC_OK) publish(in[k], st, ctx);
         else live.push_back(in[k]);
       }
+      add_time(t_save, tb);
       akmc_destroy(ctx);
+      add_time(t_build, tb);
       if (!live.empty()) {
         std::lock_guard<std::mutex> lk(m);
         take_locked(live);
@@ -184,8 +225,10 @@ struct akmc_server {
     for (;;) {
       std::vector<std::shared_ptr<SJob>> live;
       {
+        const auto tw = std::chrono::steady_clock::now();
         std::unique_lock<std::mutex> lk(m);
         cv_work.wait(lk, [&] { return stopping || fits_locked(); });
+        t_wait += std::chrono::duration<double>(std::chrono::steady_clock::now() - tw).count();
         if (stopping) return;
         take_locked(live);
       }
@@ -302,6 +345,23 @@ AKMC_API akmc_status akmc_server_stats(akmc_server* s, int64_t* queued, int64_t*
   if (queued) *queued = static_cast<int64_t>(s->queue.size());
   if (running) *running = s->running;
   if (done) *done = d;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_server_profile(akmc_server* s, double* seconds8, int64_t* counts3) {
+  if (!s || !seconds8 || !counts3) return AKMC_EINVAL;
+  std::lock_guard<std::mutex> lk(s->m);
+  seconds8[0] = s->t_build;
+  seconds8[1] = s->t_run;
+  seconds8[2] = s->t_publish;
+  seconds8[3] = s->t_wait;
+  seconds8[4] = s->t_add;
+  seconds8[5] = s->t_prepare;
+  seconds8[6] = s->t_restore;
+  seconds8[7] = s->t_save;
+  counts3[0] = s->n_chunks;
+  counts3[1] = s->n_live;
+  counts3[2] = s->n_builds;
   return AKMC_OK;
 }
 

@@ -233,6 +233,7 @@ SIGNATURES = {
     "akmc_server_submit": (C.c_int, [_vp, _vp, _vp, _i64, C.POINTER(_i64)]),
     "akmc_server_poll": (C.c_int, [_vp, _i64, _vp, _vp, _i64, C.POINTER(_i32)]),
     "akmc_server_wait": (C.c_int, [_vp, _i64, _d, _vp, _vp, _i64]),
+    "akmc_server_profile": (C.c_int, [_vp, _vp, _vp]),
     "akmc_server_stats": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "akmc_server_shutdown": (C.c_int, [_vp]),
     "akmc_load_occupancy": (C.c_int, [_vp, _i32, _vp, _i64]),
@@ -626,6 +627,15 @@ class Server:
         _check(lib().akmc_server_wait(self.h, ticket, timeout, C.byref(r), _ptr(out), n))
         self.sizes.pop(ticket, None)
         return _result(r), out
+
+    def profile(self):
+        """akmc_server_profile: lane seconds (build, run, publish, wait) and counts."""
+        t = np.zeros(8, np.float64)
+        c = np.zeros(3, np.int64)
+        _check(lib().akmc_server_profile(self.h, _ptr(t), _ptr(c)))
+        return dict(build_s=float(t[0]), run_s=float(t[1]), publish_s=float(t[2]), wait_s=float(t[3]),
+                    add_s=float(t[4]), prepare_s=float(t[5]), restore_s=float(t[6]), save_s=float(t[7]),
+                    chunks=int(c[0]), mean_batch=float(c[1]) / max(1, int(c[0])), builds=int(c[2]))
 
     def stats(self):
         q, r, d = C.c_int64(0), C.c_int64(0), C.c_int64(0)

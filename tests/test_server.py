@@ -40,6 +40,8 @@ def test_submit_rejects_jobs_that_cannot_run(ak):
         with pytest.raises(ak.AkmcError):
             srv.submit(cfg, occ[:-2])  # wrong lattice size
         assert srv.stats() == dict(queued=0, running=0, done=0)
+        prof = srv.profile()  # an idle server has built nothing and run nothing
+        assert prof["builds"] == 0 and prof["chunks"] == 0 and prof["run_s"] == 0.0
 
 
 @pytest.mark.gpu
