@@ -128,7 +128,8 @@ def run_serve(args, ak, device):
         cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=j["precision"],
                             temperature=j["temperature"], seed=j["seed"], eam=eam, hop_budget=j["hop_budget"])
         prepared.append((j["t"], cfg, occ))
-    srv = ak.Server(device=device, lanes=args.serve_lanes, chunk_rounds=args.serve_chunk)
+    srv = ak.Server(device=device, lanes=args.serve_lanes, chunk_rounds=args.serve_chunk,
+                    order=1 if args.serve_order == "smallest" else 0)
     t0 = time.perf_counter()
     tickets = []
     for t, cfg, occ in prepared:
@@ -153,6 +154,7 @@ def run_serve(args, ak, device):
         "config": {"workload": "serving: Poisson arrivals %.0f/s for %.0f s, edge log-uniform 16-96 cells, hop "
                                "budget log-uniform 1e4-1e6, EAM FP32-compensated" % (args.serve_rate, args.serve_seconds),
                    "jobs": len(jobs), "lanes": args.serve_lanes, "chunk_rounds": args.serve_chunk,
+                   "order": args.serve_order,
                    "offered_hops_per_s": sum(j["hop_budget"] for j in jobs) / args.serve_seconds},
         "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
         "latency_max_s": float(lat.max()), "wall_s": wall, "server_profile": prof,
@@ -401,6 +403,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--serve-chunk", type=int, default=16, help="sector rounds per server chunk")
+    ap.add_argument("--serve-order", default="fifo", choices=["fifo", "smallest"],
+                    help="admission order: arrival, or smallest hop budget first")
     ap.add_argument("--rounds-per-step", type=int, default=256)
     ap.add_argument("--one-at-a-time", type=int, default=0, metavar="N",
                     help="time the first N jobs of the workload in plain FP64, each alone (the baseline of "

@@ -340,7 +340,11 @@ typedef struct akmc_server_config {
   int64_t budget_bytes;     /* device memory the jobs of all running batches may hold (0: 8 GiB) */
   int32_t max_batch_jobs;   /* jobs per batch (0: 512) */
   int32_t chunk_rounds;     /* rounds between checks for finished jobs (0: 16) */
+  int32_t order;            /* admission order of queued jobs: AKMC_SERVE_FIFO (arrival) or
+                               AKMC_SERVE_SMALLEST_BUDGET (smallest hop budget first; jobs
+                               without a budget last; ties in arrival order) */
 } akmc_server_config;
+enum { AKMC_SERVE_FIFO = 0, AKMC_SERVE_SMALLEST_BUDGET = 1 };
 typedef struct akmc_job_result {
   int64_t hops;
   int64_t rounds;

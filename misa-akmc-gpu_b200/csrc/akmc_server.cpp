@@ -1,6 +1,6 @@
 // akmc_server.cpp -- job server over the context API of include/akmc.h.
 //
-// Jobs queue in arrival order.  Each lane (a host thread with its own context, hence its own
+// Jobs queue in arrival order and are admitted oldest first, or smallest hop budget first.  Each lane (a host thread with its own context, hence its own
 // CUDA stream) takes the queued jobs that fit the device-memory budget as one batch and runs
 // them together in chunks of rounds.  A job's result is published, and its memory returned to
 // the budget, as soon as that job is done.  When an eighth of a batch has finished and queued
@@ -11,6 +11,7 @@
 // one mutex; the device work runs outside it.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -95,15 +96,29 @@ struct akmc_server {
     cv_work.notify_all();
   }
 
+  // The queued job admitted next: the oldest, or the one with the smallest hop budget (jobs
+  // without a budget last, ties by arrival).
+  std::deque<std::shared_ptr<SJob>>::const_iterator next_locked() const {
+    if (cfg.order != AKMC_SERVE_SMALLEST_BUDGET || queue.empty()) return queue.begin();
+    auto key = [](const std::shared_ptr<SJob>& j) {
+      return j->cfg.hop_budget > 0 ? j->cfg.hop_budget : INT64_MAX;
+    };
+    auto best = queue.begin();
+    for (auto it = queue.begin(); it != queue.end(); ++it)
+      if (key(*it) < key(*best)) best = it;  // strictly smaller: the earliest of equals stays
+    return best;
+  }
+
   bool fits_locked() const {
-    return !queue.empty() && held + queue.front()->bytes <= cfg.budget_bytes;
+    return !queue.empty() && held + (*next_locked())->bytes <= cfg.budget_bytes;
   }
 
   // Under the lock: moves queued jobs that fit into `live`.
   void take_locked(std::vector<std::shared_ptr<SJob>>& live) {
     while (fits_locked() && static_cast<int32_t>(live.size()) < cfg.max_batch_jobs) {
-      auto j = queue.front();
-      queue.pop_front();
+      const auto it = next_locked();
+      auto j = *it;
+      queue.erase(it);
       j->state = 1;
       j->res.start_s = now();
       held += j->bytes;

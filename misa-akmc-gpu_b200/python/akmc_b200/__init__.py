@@ -16,6 +16,7 @@ HEADER = os.path.join(os.path.dirname(PKG), "include", "akmc.h")
 
 MODEL_PAIRBOND, MODEL_EAM = 0, 1
 FP64, FP32C = 0, 1
+SERVE_FIFO, SERVE_SMALLEST_BUDGET = 0, 1
 RNG_XOSHIRO = 0
 V, FE, CU, NI, MN = 0, 1, 2, 4, 8
 MAX_SECTOR_VACANCIES = 64
@@ -139,6 +140,7 @@ class ServerConfig(C.Structure):
         ("budget_bytes", C.c_int64),
         ("max_batch_jobs", C.c_int32),
         ("chunk_rounds", C.c_int32),
+        ("order", C.c_int32),
     ]
 
 
@@ -594,8 +596,8 @@ def _result(r):
 class Server:
     """akmc_server: queued jobs run in batches by worker lanes, results as each job ends."""
 
-    def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0):
-        cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds)
+    def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0, order=0):
+        cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds, order)
         h = C.c_void_p()
         _check(lib().akmc_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

@@ -45,8 +45,9 @@ def test_submit_rejects_jobs_that_cannot_run(ak):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes,max_batch", [(2, 3), (1, 2)])  # (1, 2): every finish refills the batch
-def test_server_results_equal_jobs_run_alone(ak, lanes, max_batch):
+# (1, 2): every finish refills the batch; order 1 admits the smallest hop budget first
+@pytest.mark.parametrize("lanes,max_batch,order", [(2, 3, 0), (1, 2, 0), (1, 2, 1)])
+def test_server_results_equal_jobs_run_alone(ak, lanes, max_batch, order):
     specs = [((16, 16, 16), ak.MODEL_EAM, 1, 3000, 0, (1, 1, 1), 0),
              ((24, 20, 16), ak.MODEL_PAIRBOND, 2, 0, 40, (1, 1, 1), 0),
              ((32, 32, 32), ak.MODEL_EAM, 3, 5000, 0, (2, 2, 2), 0),
@@ -54,7 +55,7 @@ def test_server_results_equal_jobs_run_alone(ak, lanes, max_batch):
              ((16, 24, 20), ak.MODEL_EAM, 5, 800, 0, (1, 1, 1), 0),
              ((40, 16, 16), ak.MODEL_PAIRBOND, 6, 2000, 0, (2, 1, 1), 0)]
     jobs = [_job(ak, *sp) for sp in specs]
-    with ak.Server(lanes=lanes, max_batch_jobs=max_batch, chunk_rounds=8) as srv:
+    with ak.Server(lanes=lanes, max_batch_jobs=max_batch, chunk_rounds=8, order=order) as srv:
         tickets = [srv.submit(cfg, occ) for cfg, occ in jobs]
         got = [srv.wait(t, timeout=300.0) for t in tickets]
     for (cfg, occ), (res, out) in zip(jobs, got):
