@@ -1109,6 +1109,9 @@ __device__ __forceinline__ int64_t ld_relaxed64(const int64_t* p) {
 }
 // Release/acquire fence at GPU scope (lighter than the sequentially consistent __threadfence).
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void st_release32(int32_t* p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ void st_release64(int64_t* p, int64_t v) {
   asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -1365,10 +1368,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
 #endif
         BlockDev& B = a.blocks[gb];
         const JobDev& J = a.jobs[B.job];
+        // the thread that found this round ready read the neighbours' round counters and then
+        // fenced (an acquire), and a CTA barrier followed: every thread's reads come after the
+        // rounds it waits for (shared data is read at L2)
         const int64_t r = ld_acquire64(&B.round);
-        // the rounds this one waits for are acquired again here; the barrier below orders
-        // every thread's reads after these acquires (shared data is read at L2)
-        if (tid < 27 && sm0->flow_lag[r & 7][tid]) (void)ld_acquire64(&a.blocks[flow_neighbour(J, B.local_id, tid)].round);
         const int sec = sector_of_round(r);
         Region R;
         make_region(B, sec, R);
@@ -1405,7 +1408,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
         // vacancies carried into a neighbour's area change owner (only if the round ran:
         // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
         if (ran && tid < cnt) {
-          const int o = owner_block(J, sm->vlid[tid]);
+          // a vacancy still inside the block's area keeps its owner; only one that left it
+          // needs the owner lookup
+          const int cx = sm->vgx[tid] >> 1, cy = sm->vgy[tid], cz = sm->vgz[tid];
+          const bool inside = cx >= B.c0[0] && cx < B.c1[0] && cy >= B.c0[1] && cy < B.c1[1] && cz >= B.c0[2] &&
+                              cz < B.c1[2];
+          const int o = inside ? gb : owner_block(J, sm->vlid[tid]);
           if (o != gb) {
             flow_give(a, o, sm->vidx[tid]);
             const unsigned long long bit = 1ull << sm->fslot[tid];
@@ -1430,10 +1438,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
           const long long q2 = clock64();
 #endif
           sm->flow_more = more;
-          if (!more) {
-            fence_acq_rel();
-            atomicExch(&a.lease[gb], 0);
-          }
+          if (!more) st_release32(&a.lease[gb], 0);  // after the round's release: ordered behind it
 #ifdef AKMC_FLOW_PROFILE
           atomicAdd(a.counters + 20, static_cast<unsigned long long>(q1 - q0));
           atomicAdd(a.counters + 21, static_cast<unsigned long long>(q2 - q1));
