@@ -94,6 +94,16 @@ def workload_jobs(name, rank=0):
     raise SystemExit("unknown workload %s" % name)
 
 
+def with_model(jobs, model):
+    """The jobs in the named energy model: the synthetic EAM (as generated), or the reference's
+    own pair-bond model, which has one precision (FP64)."""
+    if model == "pairbond":
+        for j in jobs:
+            j["model"] = 0
+            j["precision"] = 0
+    return jobs
+
+
 def serve_jobs(rate, seconds, rank=0):
     """Job stream of the serving workload: Poisson arrivals at `rate` per second for `seconds`,
     box edge log-uniform in [16, 96] cells, hop budget log-uniform in [1e4, 1e6], the batched
@@ -182,8 +192,8 @@ def run_one_at_a_time(args, ak, jobs, device, stream, torch):
     sample = jobs[: args.one_at_a_time]
     for j in sample:
         occ = ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"])
-        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=ak.FP64,
-                            temperature=j["temperature"], seed=j["seed"], eam=eam)
+        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=j.get("model", 1), precision=ak.FP64,
+                            temperature=j["temperature"], seed=j["seed"], eam=eam if j.get("model", 1) else None)
         with ak.Engine(device=device, stream=stream.cuda_stream) as eng:
             eng.add_job(cfg, occ)
             eng.prepare()
@@ -312,8 +322,8 @@ def build_engine(ak, jobs, device, stream, log=0, schedule=0):
     eam = ak.eam_johnson(42)
     for j in jobs:
         occ = ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"])
-        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=ak.MODEL_EAM, precision=j["precision"],
-                            temperature=j["temperature"], seed=j["seed"], eam=eam)
+        cfg = ak.job_config(j["box"], blocks=j["blocks"], energy_model=j.get("model", 1), precision=j["precision"],
+                            temperature=j["temperature"], seed=j["seed"], eam=eam if j.get("model", 1) else None)
         eng.add_job(cfg, occ)
         lattices.append(occ)
     eng.prepare()
@@ -326,7 +336,7 @@ def cpu_baseline(jobs, seconds=15.0, rounds_per_chunk=8):
     import pyoracle as po
 
     j = jobs[0]
-    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=po.MODEL_EAM, precision=j["precision"],
+    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=j.get("model", 1), precision=j["precision"],
                          temperature=j["temperature"], seed=j["seed"], pot_seed=42, alloy=j["alloy"],
                          n_vacancies=j["n_vacancies"], log_events=0)
     o = po.Oracle(cfg)
@@ -346,7 +356,7 @@ def run_reference(args, jobs):
     import pyoracle as po
 
     j = jobs[0]
-    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=po.MODEL_EAM, precision=j["precision"],
+    cfg = po.make_config(box=j["box"], blocks=j["blocks"], energy_model=j.get("model", 1), precision=j["precision"],
                          temperature=j["temperature"], seed=j["seed"], pot_seed=42, alloy=j["alloy"],
                          n_vacancies=j["n_vacancies"], log_events=0)
     o = po.Oracle(cfg)
@@ -383,10 +393,14 @@ def config_of(args, jobs):
                       "serial": "BCC 20^3 cells Fe-1.34Cu, 20 vacancies, single domain, EAM, T=573 K"}[args.workload],
          "jobs": len(jobs), "sites": int(sum(2 * np.prod(x["box"]) for x in jobs)),
          "vacancies": int(sum(x["n_vacancies"] for x in jobs)), "rounds_per_step": args.rounds_per_step,
-         "sector_window_s": 3e-7, "energy_model": "synthetic Johnson EAM (5 shells, rc 5.6 A)",
+         "sector_window_s": 3e-7,
+         "energy_model": "synthetic Johnson EAM (5 shells, rc 5.6 A)" if j.get("model", 1) else
+                         "pair bond (the reference's model: 1nn and masked 2nn bond energies)",
          "parallelism": "replicas x%d" % args.gpus,
          "l2": "inputs larger than L2 (occupancy + int32 density cache of %.0f MB)"
                % (5 * sum(2 * np.prod(x["box"]) for x in jobs) / 1e6)}
+    if not j.get("model", 1):
+        c["workload"] = c["workload"].replace("EAM FP32-compensated", "pair bond, FP64").replace("EAM", "pair bond")
     if len(jobs) == 1:
         c["box"] = list(j["box"])
         c["blocks"] = list(j["blocks"])
@@ -409,6 +423,8 @@ def main():
     ap.add_argument("--one-at-a-time", type=int, default=0, metavar="N",
                     help="time the first N jobs of the workload in plain FP64, each alone (the baseline of "
                          "the batched form)")
+    ap.add_argument("--model", default="eam", choices=["eam", "pairbond"],
+                    help="energy model: the synthetic EAM, or the reference's own pair-bond model (FP64)")
     ap.add_argument("--schedule", default="auto", choices=["auto", "rounds", "flow"],
                     help="round schedule of the context (auto: dependency-driven where allowed)")
     ap.add_argument("--block-edge", type=int, default=0,
@@ -430,11 +446,11 @@ def main():
         elif rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the serving workload has no CPU reference arm"}))
         return
-    jobs = workload_jobs(args.workload, rank)
+    jobs = with_model(workload_jobs(args.workload, rank), args.model)
 
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args, workload_jobs(args.workload, 0))
+            run_reference(args, with_model(workload_jobs(args.workload, 0), args.model))
         return
 
     import torch
@@ -475,7 +491,7 @@ def main():
     eng, lattices = build_engine(ak, jobs, local, stream.cuda_stream,
                                  schedule={"auto": 0, "rounds": 1, "flow": 2}[args.schedule])
     R = args.rounds_per_step
-    eam = True
+    eam = jobs[0].get("model", 1) == 1
 
     def sync_all():
         torch.cuda.synchronize()

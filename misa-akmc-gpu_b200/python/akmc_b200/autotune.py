@@ -28,8 +28,10 @@ def _trial(jobs, lattices, eam, max_block_edge, rounds, warmup, device):
     with Engine(device=device) as eng:
         for j, occ in zip(jobs, lattices):
             nb = tuple(blocks_for(e, max_block_edge) for e in j["box"])
-            eng.add_job(job_config(j["box"], blocks=nb, energy_model=MODEL_EAM, precision=j["precision"],
-                                   temperature=j["temperature"], seed=j["seed"], eam=eam), occ)
+            model = j.get("model", MODEL_EAM)
+            eng.add_job(job_config(j["box"], blocks=nb, energy_model=model, precision=j["precision"],
+                                   temperature=j["temperature"], seed=j["seed"],
+                                   eam=eam if model == MODEL_EAM else None), occ)
         eng.prepare()
         eng.run_rounds(warmup)
         eng.sync()
