@@ -217,7 +217,10 @@ void free_device(akmc_ctx* ctx) {
   ctx->prepared = false;
 }
 
-int region_sites(const HostJob& j) {
+// Sites of the largest staged region of a job.  With bulk staging a region's rows are
+// rounded out to 16-site boundaries, which start up to 14 sites before the region, so the
+// rows are laid out with a pitch of the region's width plus 14, rounded up to 16.
+int region_sites(const HostJob& j, bool bulk) {
   int64_t mx = 1;
   for (int d = 0; d < 3; ++d) {
     int wmax = 0;
@@ -225,10 +228,16 @@ int region_sites(const HostJob& j) {
       const int w = j.split[d][k + 1] - j.split[d][k];
       wmax = std::max(wmax, w - w / 2);
     }
-    mx *= (wmax + 4) * (d == 0 ? 2 : 1);
+    int ext = (wmax + 4) * (d == 0 ? 2 : 1);
+    if (bulk && d == 0) ext = (ext + 14 + 15) & ~15;
+    mx *= ext;
   }
   return static_cast<int>(mx);
 }
+
+// Bulk staging needs lattice rows of a multiple of 16 sites: then every row of a region
+// starts at the same offset from a 16-byte boundary, in the occupancy and density arrays alike.
+bool bulk_rows(const HostJob& j) { return (2 * j.cfg.box[0]) % 16 == 0; }
 
 // Restart snapshot layout: SnapHeader, then one SnapBlock per domain block, then the
 // occupancy bytes.  All fields little-endian, as the host writes them.
@@ -414,7 +423,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     if (build_potential(nullptr, pb.P, pb.coef, pb.f32)) return fail(ctx, AKMC_EINVAL, "potential");
     ctx->pots.push_back(std::move(pb));
   }
-  int max_region = 0;
+  int max_region = 0, max_region_bulk = 0;
   int32_t nb = 0, nv = 0;
   for (auto& j : ctx->jobs) {
     j.pot = 0;
@@ -438,7 +447,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     j.vac0 = nv;
     nb += j.nblocks;
     nv += static_cast<int32_t>(j.nvac);
-    max_region = std::max(max_region, region_sites(j));
+    max_region = std::max(max_region, region_sites(j, false));
+    max_region_bulk = std::max(max_region_bulk, region_sites(j, bulk_rows(j)));
     for (size_t k = 0; k + 1 < j.split[0].size(); ++k) {
       const int w = j.split[0][k + 1] - j.split[0][k];
       if (2 * (w - w / 2 + 4) > 64)  // staged rows hold at most 64 sites (two per lane)
@@ -447,9 +457,11 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   }
   ctx->nblocks = nb;
   ctx->nvac = nv;
-  ctx->smem = hop_smem_bytes(max_region);
   int dev_smem = 0;
   CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
+  // bulk staging where its wider rows fit, else row loads everywhere
+  const bool bulk = hop_smem_bytes(max_region_bulk) <= static_cast<size_t>(dev_smem);
+  ctx->smem = hop_smem_bytes(bulk ? max_region_bulk : max_region);
   if (ctx->smem > static_cast<size_t>(dev_smem))
     return fail(ctx, AKMC_EINVAL, "sector region does not fit in shared memory; use more domain blocks");
   {
@@ -525,6 +537,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     std::memset(&J, 0, sizeof(J));
     J.occ = j.d_occ;
     J.rho = j.d_rho;
+    J.bulk = bulk && bulk_rows(j) && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
+             (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
     for (int d = 0; d < 3; ++d) {
       J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
       J.nb[d] = static_cast<int32_t>(j.split[d].size() - 1);

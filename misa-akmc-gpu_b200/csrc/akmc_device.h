@@ -68,7 +68,7 @@ struct JobDev {
   int32_t nblocks;
   int32_t model, precision, pot;
   int32_t done;
-  int32_t pad;
+  int32_t bulk;       // 1: regions that do not wrap in x are staged by bulk copies of whole rows
   int64_t round;
   int64_t hops;
   int64_t hop_budget, max_rounds;

@@ -51,10 +51,19 @@ __device__ __forceinline__ int block_of(int c, int n, int p) {
 struct Region {
   int slo[3], w[3];
   int ox, oy, oz;  // origin in sites (x doubled); may be negative (periodic wrap)
-  int LX, LY, LZ, n;
+  int LX, LY, LZ, n;  // row pitch in sites and rows of the shared layout, its sites
+  int LXt, xo, nt;    // region row width, its first site within the pitch, region sites
+  int hx;             // cells before the sector in x within the pitch (the 2-cell halo, plus xo / 2)
+  int bulk;           // rows staged by bulk copies: bo occupancy bytes and br densities each
+  int bo, br;
 };
 
-__device__ __forceinline__ void make_region(const BlockDev& B, int sec, Region& R) {
+// The staged region of a block's sector: the sector and a 2-cell halo.  Rows are staged
+// whole by the bulk-copy unit when the job allows it (J.bulk: rows of a multiple of 16 sites,
+// 16-byte aligned arrays, shared memory sized for the wider rows) and the region does not
+// wrap in x: each row is rounded out to 16-site boundaries, so every copy starts on a 16-byte
+// boundary of its lattice row and ends inside it.
+__device__ __forceinline__ void make_region(const BlockDev& B, const JobDev& J, int sec, Region& R) {
   for (int d = 0; d < 3; ++d) {
     const int half = (B.c1[d] - B.c0[d]) / 2;
     if ((sec >> d) & 1) {
@@ -71,7 +80,22 @@ __device__ __forceinline__ void make_region(const BlockDev& B, int sec, Region& 
   R.LX = 2 * (R.w[0] + 4);
   R.LY = R.w[1] + 4;
   R.LZ = R.w[2] + 4;
+  R.LXt = R.LX;
+  R.xo = 0;
+  R.bulk = 0;
+  R.bo = R.br = 0;
+  if (J.bulk && R.ox >= 0 && R.ox + R.LX <= J.sx) {
+    const int x0 = R.ox & ~15;
+    R.xo = R.ox - x0;
+    R.ox = x0;
+    R.LX = (R.LXt + 14 + 15) & ~15;  // one pitch for every alignment: tables stay valid
+    R.bo = (R.xo + R.LXt + 15) & ~15;
+    R.br = (R.xo + R.LXt + 3) & ~3;
+    R.bulk = 1;
+  }
+  R.hx = R.slo[0] - R.ox / 2;
   R.n = R.LX * R.LY * R.LZ;
+  R.nt = R.LXt * R.LY * R.LZ;
 }
 
 // Shared-memory working set of one CTA (followed by the staged region).
@@ -98,7 +122,8 @@ struct Smem {
   // FP32 (hi, lo, c1, c2) x kFWin then c3 x kFWin
   alignas(16) unsigned char fwin[kFWin * 32];
   alignas(8) uint64_t mbar;                    // completion barrier of the window's bulk copy
-  uint32_t mbar_phase;
+  uint64_t mbar_st;                            // completion barrier of the region's bulk copies
+  uint32_t mbar_phase, mbst_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
   int32_t tab_key[2];                          // potential, kind and region strides the tables hold
   // hop-loop control, written by thread 0 between barriers
@@ -484,7 +509,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   jc.nu = J.nu;
   jc.kT = J.kT;
   Region R;
-  make_region(B, sec, R);
+  make_region(B, J, sec, R);
   // F-table window: one bulk copy issued by the control thread, overlapped with the staging
   const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
   const bool need_win = eam && sm.win_pot != win_key;
@@ -492,6 +517,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   // row strides only: kept from the CTA's previous block when those match
   const int tab0 = J.pot * 4 + KIND, tab1 = R.LX | (R.LY << 16);
   const bool need_tab = sm.tab_key[0] != tab0 || sm.tab_key[1] != tab1;
+  const int nrows = R.LY * R.LZ;
+  if (R.bulk && tid == kCtl)  // armed before any copy is issued (after the barrier below)
+    bulk_expect(&sm.mbar_st, static_cast<uint32_t>(nrows) * static_cast<uint32_t>(R.bo + (eam ? 4 * R.br : 0)));
   __syncthreads();  // every thread has read win_pot and tab_key; the previous item's readers are done
   AKMC_STAGE_T(0);
   if (need_win && tid == kCtl) {
@@ -526,8 +554,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
 
   // stage the region: warp w takes rows w, w+9, ...; kStageRows rows of loads are issued
   // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
-  {
-    const int nrows = R.LY * R.LZ;
+  if (!R.bulk) {
     const int gx0 = wrap1(R.ox + lane, jc.sx), gx1 = wrap1(R.ox + lane + 32, jc.sx);
     const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
     constexpr int kW = kThreads / 32;
@@ -566,6 +593,17 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           }
         }
       }
+    }
+  } else {
+    // the bulk-copy unit moves whole rows: R.bo occupancy bytes and R.br densities from the
+    // row's 16-site boundary R.ox, into shared rows of pitch R.LX; thread t issues row t
+    asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
+    for (int row = tid; row < nrows; row += kThreads) {
+      const int ly = row % R.LY, lz = row / R.LY;
+      const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
+      const int64_t base = static_cast<int64_t>(jc.sx) * (gy + static_cast<int64_t>(jc.sy) * gz) + R.ox;
+      bulk_copy(occ_s + R.LX * row, jc.occ + base, static_cast<uint32_t>(R.bo), &sm.mbar_st);
+      if (eam) bulk_copy(rho_s + R.LX * row, jc.rho + base, 4u * static_cast<uint32_t>(R.br), &sm.mbar_st);
     }
   }
   AKMC_STAGE_T(2);
@@ -620,12 +658,29 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         sm.ctl_ok = 0;
       }
     }
+    if (R.bulk) {  // the region's rows
+      if (mbar_wait(&sm.mbar_st, sm.mbst_phase)) {
+        sm.mbst_phase ^= 1u;
+      } else {
+        atomicOr(a.status, kErrTimeout);
+        if (mbar_wait(&sm.mbar_st, sm.mbst_phase)) sm.mbst_phase ^= 1u;  // bounded second wait
+        sm.ctl_ok = 0;
+      }
+    }
   }
   __syncthreads();
   AKMC_PHASE(1);
   if (!sm.ctl_ok) return true;
-  if (KIND == kEam64) {  // F(rho) of every staged site, reused by all jumps that touch it
-    for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
+  if (KIND == kEam64) {  // F(rho) of every site of the region, reused by all jumps that touch it
+    if (!R.bulk) {
+      for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
+    } else {  // the region's columns of each row; the rest of the pitch is not the region's
+      for (int i = tid; i < R.nt; i += kThreads) {
+        const int row = i / R.LXt;
+        const int l = R.xo + (i - row * R.LXt) + R.LX * row;
+        FT.fc[l] = F64(FT, rho_s[l]);
+      }
+    }
     __syncthreads();
   }
   // this lane's entries of its warp's jump lists, both x parities
@@ -880,7 +935,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           sm.vgz[ksel] = ngz;
           const int cx = nlx >> 1;
           sm.vact[ksel] =
-              cx >= 2 && cx < 2 + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
+              cx >= R.hx && cx < R.hx + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
         } else if (!sm.ctl_stop && a.mode == kModeSelectPerform) {  // u * total reached no event
           akmc_event* e = a.api_event;
           e->round = 0;
@@ -955,7 +1010,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.acc[1] += static_cast<unsigned long long>(evals);
     sm.acc[2] += 1ull;
     sm.acc[3] += static_cast<unsigned long long>(nact_sum);
-    sm.acc[4] += static_cast<unsigned long long>(R.n);
+    sm.acc[4] += static_cast<unsigned long long>(R.nt);
     sm.acc[5] += static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2));
   }
   // the lattice was written through at every hop; only the vacancy positions remain
@@ -975,7 +1030,7 @@ __device__ void dispatch_block(const RoundArgs& a, int gb, uint8_t* smem) {
   const JobDev& J = a.jobs[B.job];
   const int sec = a.mode == kModeRound ? sector_of_round(B.round) : a.api_sector;
   Region R;
-  make_region(B, sec, R);
+  make_region(B, J, sec, R);
   Smem* sm;
   uint8_t* occ_s;
   int32_t* rho_s;
@@ -1026,7 +1081,9 @@ __device__ void init_cta_smem(uint8_t* smem) {
     sm->win_pot = -1;
     sm->tab_key[0] = sm->tab_key[1] = -1;
     sm->mbar_phase = 0;
+    sm->mbst_phase = 0;
     mbar_init(&sm->mbar);
+    mbar_init(&sm->mbar_st);
     for (int i = 0; i < 6; ++i) sm->acc[i] = 0;
     sm->acc_job = -1;
     sm->acc_job_hops = 0;
@@ -1064,7 +1121,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_hop(RoundArgs a) {
     const BlockDev& B = a.blocks[gb];
     if (job_kind(a.jobs[B.job]) != KIND) continue;
     Region R;
-    make_region(B, sector_of_round(B.round), R);
+    make_region(B, a.jobs[B.job], sector_of_round(B.round), R);
     Smem* sm;
     uint8_t* occ_s;
     int32_t* rho_s;
@@ -1374,7 +1431,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
         const int64_t r = ld_acquire64(&B.round);
         const int sec = sector_of_round(r);
         Region R;
-        make_region(B, sec, R);
+        make_region(B, J, sec, R);
         Smem* sm;
         uint8_t* occ_s;
         int32_t* rho_s;
