@@ -190,7 +190,6 @@ struct FTab {
   const float* g32b;
   unsigned int* status;
   unsigned long long* prof;  // sub-phase cycles of the evaluation (profiling builds)
-  double* fc;                // F(rho) of every staged site (FP64 form)
 };
 
 // Job constants of the running block, held in registers (the job record sits in global
@@ -221,10 +220,9 @@ __device__ __forceinline__ int local_delta(int32_t w, const Region& R) {
   return unpack_dx(w) + R.LX * (unpack_dy(w) + R.LY * unpack_dz(w));
 }
 
-// Region layout after Smem: int32 densities, double F(rho) cache (16-byte aligned), bytes.
-__device__ __forceinline__ double* fcache_of(int32_t* rho_s, int nreg) {
-  return reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(rho_s) +
-                                   ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15)));
+// Region layout after Smem: int32 densities, then occupancy bytes (16-byte aligned).
+__device__ __forceinline__ uint8_t* occ_of(int32_t* rho_s, int nreg) {
+  return reinterpret_cast<uint8_t*>(rho_s) + ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15));
 }
 
 __device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, const Region& R, int kind) {
@@ -366,7 +364,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     const int X = species_index(Xc);
     // the moving atom's own embedding change; every lane reads the same cells (broadcast),
     // so its latency overlaps the site loop
-    const double EX = avail ? F64(FT, rho_s[l] - sm.fq1[X]) - FT.fc[tl] : 0.0;
+    const double EX = avail ? F64(FT, rho_s[l] - sm.fq1[X]) - F64(FT, rho_s[tl]) : 0.0;
     if (avail) {
 #pragma unroll
       for (int u = 0; u < 3; ++u) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
@@ -377,7 +375,7 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
         const uint8_t o = occ_s[j];
         const int32_t r = rho_s[j];
         const double Fa = F64(FT, r + sm.dfq[X * 64 + h]);
-        const double Fb = FT.fc[j];  // F(rho_j), cached
+        const double Fb = F64(FT, r);  // independent of Fa: the two overlap
         if (o != kV) {
           const int Y = species_index(o);
           acc += (Fa - Fb) + sm.dphi64[(X * 4 + Y) * 64 + h];
@@ -549,7 +547,6 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   FT.g32b = P.F32b;
   FT.status = a.status;
   FT.prof = a.counters + 16;
-  FT.fc = fcache_of(rho_s, R.n);
   AKMC_STAGE_T(1);
 
   // stage the region: warp w takes rows w, w+9, ...; kStageRows rows of loads are issued
@@ -671,18 +668,6 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   __syncthreads();
   AKMC_PHASE(1);
   if (!sm.ctl_ok) return true;
-  if (KIND == kEam64) {  // F(rho) of every site of the region, reused by all jumps that touch it
-    if (!R.bulk) {
-      for (int i = tid; i < R.n; i += kThreads) FT.fc[i] = F64(FT, rho_s[i]);
-    } else {  // the region's columns of each row; the rest of the pitch is not the region's
-      for (int i = tid; i < R.nt; i += kThreads) {
-        const int row = i / R.LXt;
-        const int l = R.xo + (i - row * R.LXt) + R.LX * row;
-        FT.fc[l] = F64(FT, rho_s[l]);
-      }
-    }
-    __syncthreads();
-  }
   // this lane's entries of its warp's jump lists, both x parities
   int32_t jr[kJumpsPerWarp][2][3];
 #pragma unroll
@@ -706,7 +691,6 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     const int j = s + local_delta(e, R);
     const int32_t v = rho_s[j] + sm.dfq[X * 64 + rshells(e)];
     rho_s[j] = v;
-    if (KIND == kEam64) FT.fc[j] = F64(FT, v);
     const int gx = wrap1(sm.ctl_gx + unpack_dx(e), jc.sx), gy = wrap1(sm.ctl_gy + unpack_dy(e), jc.sy),
               gz = wrap1(sm.ctl_gz + unpack_dz(e), jc.sz);
     jc.rho[gx + jc.sx * (gy + jc.sy * gz)] = v;  // site ids fit in int32 (checked at akmc_add_job)
@@ -1022,7 +1006,7 @@ __device__ __forceinline__ void carve(uint8_t* smem, int nreg, Smem*& sm, uint8_
   sm = reinterpret_cast<Smem*>(smem);
   uint8_t* p = smem + ((sizeof(Smem) + 15) & ~static_cast<size_t>(15));
   rho_s = reinterpret_cast<int32_t*>(p);
-  occ_s = reinterpret_cast<uint8_t*>(fcache_of(rho_s, nreg) + nreg);
+  occ_s = occ_of(rho_s, nreg);
 }
 
 __device__ void dispatch_block(const RoundArgs& a, int gb, uint8_t* smem) {
@@ -1841,7 +1825,7 @@ __global__ void k_device_math(const double* x, int64_t n, double* e, double* l) 
 
 size_t hop_smem_bytes(int max_region_sites) {
   return ((sizeof(Smem) + 15) & ~static_cast<size_t>(15)) + ((static_cast<size_t>(max_region_sites) * 4 + 15) & ~static_cast<size_t>(15)) +
-         static_cast<size_t>(max_region_sites) * 9 + 16;
+         static_cast<size_t>(max_region_sites) + 16;
 }
 
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1) {
