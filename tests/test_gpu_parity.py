@@ -104,6 +104,19 @@ def test_uneven_blocks_and_odd_edges(ak):
     eng.close()
 
 
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_uneven_blocks_with_bulk_staging(ak, schedule):
+    # rows of 80 sites (a multiple of 16): regions that do not wrap in x are staged by bulk
+    # copies; the x split 14/13/13 gives sectors of 7 and 6 cells, staged with one row pitch
+    kw = dict(box=(40, 24, 56), blocks=(3, 2, 3), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=40,
+              temperature=563.0, seed=13)
+    eng, (o,) = run_pair(ak, 128, [kw], schedule)
+    assert o.hops > 500
+    check_job(eng, o, 0, eng.events())
+    assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
+
+
 def test_batched_jobs_of_different_shapes(ak):
     jobs = [
         dict(box=(20, 20, 20), model=po.MODEL_EAM, seed=1, temperature=573.0),
