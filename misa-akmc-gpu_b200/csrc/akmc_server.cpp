@@ -7,8 +7,12 @@
 // jobs fit, the lane refills: the running jobs are saved as restart snapshots, the context is
 // rebuilt with them and the newly admitted jobs, and the snapshots are restored, so every
 // job's trajectory is exactly the one it has alone.  A lane also refills, after 8 chunks, when
-// at least as many jobs wait as it runs.  Lanes overlap on the GPU.  All shared state is under
-// one mutex; the device work runs outside it.
+// at least as many jobs wait as it runs.  A lane whose live jobs are all single-block boxes, with
+// none queued, runs them round by round in chunks 8 times longer: those jobs are the small boxes
+// with large hop budgets that end a run, latency bound, and the dependency-driven schedule's
+// launches (at most a time step each for budget jobs) cost more than their rounds; single-block
+// jobs keep one another's pace in lockstep.  Both schedules give the same trajectory.  Lanes overlap on the GPU.  All shared state is under one mutex; the device work
+// runs outside it.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -26,6 +30,10 @@
 #include "../../include/akmc.h"
 
 namespace {
+
+// Chunks of a batch's tail (single-block jobs only, empty queue): this many times the
+// configured length.
+constexpr int64_t kTailChunks = 8;
 
 struct SJob {
   int64_t ticket = 0;
@@ -173,7 +181,14 @@ struct akmc_server {
       bool refill = false;
       while (st == AKMC_OK && left > 0 && !refill) {
         auto tr = std::chrono::steady_clock::now();
-        st = akmc_run_rounds(ctx, cfg.chunk_rounds);
+        bool tail = chunks_here > 0;  // job states known
+        for (size_t k = 0; tail && k < in.size(); ++k) tail = over[k] || js[k].n_blocks == 1;
+        if (tail) {
+          std::lock_guard<std::mutex> lk(m);
+          tail = queue.empty();
+        }
+        st = akmc_set_round_schedule(ctx, tail ? AKMC_SCHEDULE_ROUNDS : AKMC_SCHEDULE_AUTO);
+        if (st == AKMC_OK) st = akmc_run_rounds(ctx, tail ? kTailChunks * cfg.chunk_rounds : cfg.chunk_rounds);
         if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(in.size()));
         add_time(t_run, tr);
         {

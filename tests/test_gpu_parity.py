@@ -172,6 +172,38 @@ def test_hop_budgets_under_both_schedules(ak, schedule):
         assert eng.job_state(1)["round"] == 93
 
 
+def test_schedule_switch_between_calls(ak):
+    # the job server switches a context between the two schedules from one chunk to the next:
+    # the trajectory must not notice.  A budget job (it stops at a time-step boundary inside the
+    # third call), a job without budget and a single-block job, 40 + 56 + 24 + 7 rounds under
+    # flow, rounds (a captured graph and eager rounds), flow, rounds
+    kws = [dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=40,
+                temperature=563.0, seed=31),
+           dict(box=(24, 24, 24), blocks=(2, 1, 1), model=po.MODEL_EAM, precision=po.FP32C, n_vacancies=10, seed=32),
+           dict(box=(16, 16, 16), model=po.MODEL_EAM, precision=po.FP32C, n_vacancies=4, seed=33)]
+    budget = 5700  # the oracle reaches it in the time step that ends at round 112
+    with ak.Engine(event_log_capacity=1 << 20) as eng:
+        oracles = [oracle_job(**kw) for kw in kws]
+        for k, (kw, o) in enumerate(zip(kws, oracles)):
+            dkw = {key: kw[key] for key in ("box", "blocks", "model", "precision", "seed", "temperature") if key in kw}
+            device_job(eng, o, hop_budget=budget if k == 0 else 0, **dkw)
+        eng.prepare()
+        for schedule, n in ((2, 40), (1, 56), (2, 24), (1, 7)):
+            eng.set_round_schedule(schedule)
+            assert eng.round_schedule() == schedule
+            eng.run_rounds(n)
+        eng.sync()
+        oracles[0].run(budget, 127)
+        oracles[1].run_rounds(127)
+        oracles[2].run_rounds(127)
+        ev = eng.events()
+        for k, o in enumerate(oracles):
+            check_job(eng, o, k, ev)
+        st = eng.job_state(0)
+        assert st["done"] and st["round"] % 8 == 0 and 96 < st["round"] < 120, st
+        assert eng.job_state(1)["round"] == 127 and eng.job_state(2)["round"] == 127
+
+
 def test_job_without_vacancies_only_advances_clocks(ak):
     o = oracle_job(box=(16, 16, 16), n_vacancies=0)
     with ak.Engine() as eng:
