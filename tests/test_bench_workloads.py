@@ -48,3 +48,27 @@ def test_serving_stream_is_poisson_with_the_named_ranges():
     for j in jobs[:200]:
         assert all(b >= 1 and e // b >= 8 for e, b in zip(j["box"], j["blocks"]))  # blocks of >= 8 cells
         assert all(-(-e // b) <= 24 for e, b in zip(j["box"], j["blocks"]))  # staged regions fit
+
+
+def test_reference_arm_prints_the_contract_line():
+    # one process, no GPU: the reference arm times the oracle on the host cores and prints one
+    # JSON line with the benchmark's keys, an end-to-end figure without transfers and its own
+    # CPU baseline record
+    import json
+    import subprocess
+
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--workload", "serial",
+                        "--steps", "3", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "hops/s" and d["higher_is_better"] is True
+    assert d["n_gpus"] == 1 and d["steps"] == 3 and d["warmup"] == 3 and d["dtype"] == "f64"
+    assert d["value"] > 0 and d["ms_per_step"] > 0 and d["vs_baseline"] is None
+    assert d["e2e"] == {"value": d["value"], "unit": "hops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    c = d["cpu_baseline"]
+    assert c["value"] == d["value"] and c["kind"] == "port" and c["cores"] >= 1 and c["sample"]
+    assert "20^3" in d["config"]["workload"]
