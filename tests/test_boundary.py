@@ -82,3 +82,14 @@ def test_invalid_inputs_are_rejected_without_gpu(ak):
         ak.create_lattice((8, 8, 8), ((po.FE, 0),), 0, 1)  # no atoms to draw from
     with pytest.raises(ak.AkmcError):
         ak.eam_johnson(1, 2.855, 6.0)  # cutoff beyond the 5th shell
+
+
+def test_engine_fails_loudly_without_a_gpu(ak):
+    # no CPU fallback: with no CUDA device, creating a context is an error, not a slower path
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(ak.AkmcError) as ei:
+        ak.Engine()
+    assert ei.value.status == -3  # AKMC_ECUDA
