@@ -307,11 +307,17 @@ typedef struct akmc_run_config {
   int64_t dump_interval, logs_interval;
   char dump_file_path[256];
   char logs_file[256];
+  int32_t create_pipe;        /* create.pipe.enable (ConfigParsing::parseCreate, config_parsing.cpp:171-189) */
+  int32_t reserved2;
+  char pipe_input_box[256];   /* create.pipe.input_box: vacancy positions "x y z" (x doubled), whitespace
+                                 separated, read by akmc_config_lattice relative to the working directory */
 } akmc_run_config;
 
 AKMC_API akmc_status akmc_config_parse(const char* yaml_text, akmc_run_config* out, char* err, int32_t errlen);
 /* The lattice of a config: creation = reference reproduces creation::createRandom's
- * mt19937 draw order (ghost sites included, src/creation.cpp:18-164). */
+ * mt19937 draw order (ghost sites included, src/creation.cpp:18-164).  With create.pipe the
+ * alloy is drawn the same way and the vacancies are the in-box positions of the pile file
+ * (creation::createFromPile, src/creation.cpp:184-230); EINVAL if the file cannot be read. */
 AKMC_API akmc_status akmc_config_lattice(const akmc_run_config* cfg, uint8_t* occ, int64_t n_sites);
 AKMC_API akmc_status akmc_config_job(const akmc_run_config* cfg, const akmc_eam_tables* eam, akmc_job_config* out);
 /* SubLattice::startTimeLoop (sublattice.inl:24-190) for a single-domain job,

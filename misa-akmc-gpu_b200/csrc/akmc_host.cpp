@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <random>
 #include <string>
 #include <vector>
@@ -192,14 +193,28 @@ AKMC_API akmc_status akmc_config_parse(const char* text, akmc_run_config* out, c
   to_f64(sim->get("attempt_freq"), out->attempt_freq);
   to_f64(sim->get("dpasm1"), out->dpasm1);
   out->isgenr = to_bool(sim->get("isgenr"), false) ? 1 : 0;
-  // create (parseCreate): random only; pipe and restart are reported as unsupported
+  // create (parseCreate, config_parsing.cpp:150-205): random first, else pipe; restart is
+  // reported as unsupported (this library restarts from its own snapshots)
   const Node* create = root.get("create");
   if (!create) return set_err(err, errlen, "create in config is not specified."), AKMC_EINVAL;
   const Node* random = create->get("random");
-  if (random && to_bool(random->get("enable"), false)) {
-    out->create_random = 1;
-    to_i64(random->get("va_count"), out->va_count);
-    const Node* alloy = random->get("alloy");
+  const Node* pipe = create->get("pipe");
+  const bool random_on = random && to_bool(random->get("enable"), false);
+  const bool pipe_on = !random_on && pipe && to_bool(pipe->get("enable"), false);
+  if (random_on || pipe_on) {
+    if (random_on) {
+      out->create_random = 1;
+      to_i64(random->get("va_count"), out->va_count);
+    } else {
+      // the pipe option takes its alloy from create.random.alloy, as the reference does
+      // (config_parsing.cpp:177); the vacancy count is that of the pile file
+      out->create_pipe = 1;
+      out->va_count = -1;
+      if (const Node* ib = pipe->get("input_box"))
+        std::snprintf(out->pipe_input_box, sizeof(out->pipe_input_box), "%s", ib->scalar.c_str());
+      if (!out->pipe_input_box[0]) return set_err(err, errlen, "create.pipe.input_box is empty."), AKMC_EINVAL;
+    }
+    const Node* alloy = random ? random->get("alloy") : nullptr;
     if (!alloy || !alloy->is_map) return set_err(err, errlen, "alloy must be a map in config."), AKMC_EINVAL;
     for (const auto& kv : alloy->map) {
       const int c = type_code(kv.first);
@@ -216,10 +231,11 @@ AKMC_API akmc_status akmc_config_parse(const char* text, akmc_run_config* out, c
       ++out->n_types;
     }
   } else {
-    const Node* pipe = create->get("pipe");
     const Node* restart = create->get("restart");
-    if ((pipe && to_bool(pipe->get("enable"), false)) || (restart && to_bool(restart->get("enable"), false)))
-      return set_err(err, errlen, "create.pipe / create.restart are not supported; use create.random"), AKMC_EINVAL;
+    if (restart && to_bool(restart->get("enable"), false))
+      return set_err(err, errlen,
+                     "create.restart is not supported; restart from a snapshot (akmc_restore_snapshot)"),
+             AKMC_EINVAL;
     return set_err(err, errlen, "no create option in config."), AKMC_EINVAL;
   }
   // seeds (parseSeeds)
@@ -264,10 +280,29 @@ AKMC_API akmc_status akmc_config_parse(const char* text, akmc_run_config* out, c
 // array (ghost = ceil(cutoff / lattice_const)) in z-y-x order with mt19937(create_types),
 // then vacancies from uniform_int_distribution<long long>(0, sites - 1) with
 // mt19937(create_vacancy).  creation = 1 uses the xoshiro streams instead.
+//
+// create.pipe (creation::createFromPile, src/creation.cpp:184-230): the same alloy draws, then a
+// vacancy at every position "x y z" (x doubled) of the pile file that lies inside the box, read
+// as the reference reads it (`while (file >> x >> y >> z)`); positions outside the box are
+// skipped.  The reference marks these vacancies in LatticesList::_lattices only, which its
+// hash-set occupancy store never reads; here the site becomes a vacancy, whatever atom it held.
 AKMC_API akmc_status akmc_config_lattice(const akmc_run_config* cfg, uint8_t* occ, int64_t n_sites) {
   if (!cfg || !occ) return AKMC_EINVAL;
   const int64_t sx = 2 * cfg->box[0], sy = cfg->box[1], sz = cfg->box[2];
-  if (n_sites != sx * sy * sz || cfg->va_count < 0 || cfg->va_count > n_sites) return AKMC_EINVAL;
+  if (n_sites != sx * sy * sz) return AKMC_EINVAL;
+  if (!cfg->create_pipe && (cfg->va_count < 0 || cfg->va_count > n_sites)) return AKMC_EINVAL;
+  std::vector<int64_t> pile;
+  if (cfg->create_pipe) {
+    if (cfg->creation == 1) return AKMC_EINVAL;  // the pile file is a reference-order creation
+    std::ifstream f(cfg->pipe_input_box);
+    if (!f) return AKMC_EINVAL;
+    int64_t x, y, z;
+    while (f >> x >> y >> z) {
+      pile.push_back(x);
+      pile.push_back(y);
+      pile.push_back(z);
+    }
+  }
   int64_t codes64[4] = {0, 0, 0, 0};
   int32_t codes[4] = {akmc::kFe, akmc::kFe, akmc::kFe, akmc::kFe};
   int64_t total = 0;
@@ -300,6 +335,14 @@ AKMC_API akmc_status akmc_config_lattice(const akmc_run_config* cfg, uint8_t* oc
         const int64_t ix = x - 2 * g, iy = y - g, iz = z - g;
         if (ix >= 0 && ix < sx && iy >= 0 && iy < sy && iz >= 0 && iz < sz) occ[ix + sx * (iy + sy * iz)] = t;
       }
+  if (cfg->create_pipe) {
+    for (size_t i = 0; i + 2 < pile.size(); i += 3) {
+      const int64_t x = pile[i], y = pile[i + 1], z = pile[i + 2];
+      if (x < 0 || x >= sx || y < 0 || y >= sy || z < 0 || z >= sz) continue;  // isIn(x / 2, y, z)
+      occ[x + sx * (y + sy * z)] = akmc::kV;
+    }
+    return AKMC_OK;
+  }
   std::uniform_int_distribution<long long> va_dis(0, n_sites - 1);
   std::mt19937 va_rng(static_cast<std::mt19937::result_type>(cfg->seed_create_vacancy));
   int64_t placed = 0;

@@ -190,6 +190,9 @@ class RunConfig(C.Structure):
         ("logs_interval", C.c_int64),
         ("dump_file_path", C.c_char * 256),
         ("logs_file", C.c_char * 256),
+        ("create_pipe", C.c_int32),
+        ("reserved2", C.c_int32),
+        ("pipe_input_box", C.c_char * 256),
     ]
 
 

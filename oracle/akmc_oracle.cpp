@@ -943,7 +943,10 @@ void create_xoshiro(Job& J) {
 
 // creation::createAtomsRandom / createRandom (src/creation.cpp:18-164) for one rank:
 // one draw per site of the ghost-padded array in z-y-x order, ghost = ceil(rc/a).
-void create_mt(Job& J) {
+// creation::createAtomsRandom (src/creation.cpp:18-94) for one rank holding the whole box: one
+// uniform_int_distribution<>(1, sum ratio) draw per site of the ghost-padded array (ghost =
+// ceil(cutoff / lattice_const) cells) in z-y-x order with mt19937(create_types).
+void create_atoms_mt(Job& J) {
   const int64_t R = ratio_total(J.c);
   const int64_t g = static_cast<int64_t>(std::ceil(J.c.cutoff / J.c.lattice_const));
   const int64_t px = 2 * (J.n[0] + 2 * g), py = J.n[1] + 2 * g, pz = J.n[2] + 2 * g;
@@ -958,6 +961,12 @@ void create_mt(Job& J) {
         if (ix >= 0 && ix < J.sx && iy >= 0 && iy < J.sy && iz >= 0 && iz < J.sz)
           J.occ[static_cast<size_t>(ix + J.sx * (iy + J.sy * iz))] = t;
       }
+}
+
+// creation::createRandom's vacancies (src/creation.cpp:126-160): uniform_int_distribution<long
+// long>(0, sites - 1) with mt19937(create_vacancy) until n_vacancies distinct sites hold one.
+void create_mt(Job& J) {
+  create_atoms_mt(J);
   std::uniform_int_distribution<long long> va_dis(0, J.ns - 1);
   std::mt19937 va_rng(static_cast<std::mt19937::result_type>(J.c.seed_vacancy));
   int64_t placed = 0;
@@ -972,6 +981,20 @@ void create_mt(Job& J) {
       J.occ[s] = kV;
       ++placed;
     }
+  }
+}
+
+// creation::createFromPile (src/creation.cpp:184-230): the alloy of createAtomsRandom, then a
+// vacancy at every position of the pile file (x doubled, y, z) that lies inside the box; positions
+// outside it are skipped and repeated ones change nothing.  The reference marks the vacancy in
+// LatticesList::_lattices only, which its hash-set occupancy store never reads; here the site
+// becomes a vacancy of the occupancy, whatever atom it held (as createRandom's placement).
+void create_pile(Job& J) {
+  create_atoms_mt(J);
+  for (int64_t i = 0; i < J.c.pile_n; ++i) {
+    const int64_t x = J.c.pile_xyz[3 * i], y = J.c.pile_xyz[3 * i + 1], z = J.c.pile_xyz[3 * i + 2];
+    if (x < 0 || x >= J.sx || y < 0 || y >= J.sy || z < 0 || z >= J.sz) continue;  // isIn(x / 2, y, z)
+    J.occ[static_cast<size_t>(x + J.sx * (y + J.sy * z))] = kV;
   }
 }
 
@@ -1026,6 +1049,7 @@ void* ao_create(const ao_config* cfg, char* err, int errlen) {
   J->occ.assign(static_cast<size_t>(J->ns), kFe);
   if (cfg->creation_mode == AO_CREATE_XOSHIRO) create_xoshiro(*J);
   else if (cfg->creation_mode == AO_CREATE_MT19937_REF) create_mt(*J);
+  else if (cfg->creation_mode == AO_CREATE_MT19937_PILE) create_pile(*J);
   J->compute_rho();
   J->blk.resize(static_cast<size_t>(J->nblocks));
   for (int b = 0; b < J->nblocks; ++b) {

@@ -32,7 +32,7 @@ enum { AO_MODEL_PAIRBOND = 0, AO_MODEL_EAM = 1 };
 enum { AO_FP64 = 0, AO_FP32C = 1 };
 enum { AO_RNG_XOSHIRO = 0, AO_RNG_MT19937_REF = 1 };
 enum { AO_MATH_PORTABLE = 0, AO_MATH_LIBM = 1 };
-enum { AO_CREATE_XOSHIRO = 0, AO_CREATE_MT19937_REF = 1, AO_CREATE_EXTERNAL = 2 };
+enum { AO_CREATE_XOSHIRO = 0, AO_CREATE_MT19937_REF = 1, AO_CREATE_EXTERNAL = 2, AO_CREATE_MT19937_PILE = 3 };
 
 typedef struct ao_config {
   int64_t box[3];         /* cells per dimension (config.yaml box.size) */
@@ -55,6 +55,9 @@ typedef struct ao_config {
   int32_t type_codes[4];  /* alloy species codes in config order (reference: YAML map order) */
   int64_t ratio[4];       /* alloy ratio of type_codes[i] */
   int64_t n_vacancies;
+  /* AO_CREATE_MT19937_PILE: vacancy positions (x doubled, y, z) of the pile file, pile_n triples */
+  const int64_t* pile_xyz;
+  int64_t pile_n;
 } ao_config;
 
 typedef struct ao_event {

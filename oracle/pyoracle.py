@@ -17,7 +17,7 @@ MODEL_PAIRBOND, MODEL_EAM = 0, 1
 FP64, FP32C = 0, 1
 RNG_XOSHIRO, RNG_MT19937_REF = 0, 1
 MATH_PORTABLE, MATH_LIBM = 0, 1
-CREATE_XOSHIRO, CREATE_MT19937_REF, CREATE_EXTERNAL = 0, 1, 2
+CREATE_XOSHIRO, CREATE_MT19937_REF, CREATE_EXTERNAL, CREATE_MT19937_PILE = 0, 1, 2, 3
 
 V, FE, CU, NI, MN = 0, 1, 2, 4, 8
 
@@ -44,6 +44,8 @@ class AoConfig(C.Structure):
         ("type_codes", C.c_int32 * 4),
         ("ratio", C.c_int64 * 4),
         ("n_vacancies", C.c_int64),
+        ("pile_xyz", C.c_void_p),
+        ("pile_n", C.c_int64),
     ]
 
 
@@ -158,7 +160,9 @@ def make_config(
     pot_seed=42,
     alloy=((FE, 9866), (CU, 134)),
     n_vacancies=20,
+    pile=None,
 ):
+    """pile: vacancy positions (x doubled, y, z) for creation_mode CREATE_MT19937_PILE."""
     c = AoConfig()
     c.box[:] = list(box)
     c.blocks[:] = list(blocks)
@@ -182,6 +186,11 @@ def make_config(
     c.type_codes[:] = codes
     c.ratio[:] = ratios
     c.n_vacancies = n_vacancies
+    if pile is not None:
+        arr = np.ascontiguousarray(np.asarray(pile, np.int64).reshape(-1, 3))
+        c._pile = arr  # keeps the positions alive with the config
+        c.pile_xyz = arr.ctypes.data
+        c.pile_n = len(arr)
     return c
 
 

@@ -138,3 +138,47 @@ def test_dump_format(ak, tmp_path):
     assert lines[2] == "V\t2\t2\t2"          # corner site (0,0,0) at local ghost offset 2
     assert lines[3] == "Cu\t2.5\t2.5\t2.5"   # centre site
     assert len(lines) == 2 + 128
+
+
+def _pipe_config(path):
+    # create.random disabled, create.pipe enabled: the reference still takes the alloy from
+    # create.random.alloy (config_parsing.cpp:177)
+    return CONFIG.replace("    enable: true\n    va_count: 7", "    enable: false\n    va_count: 7").replace(
+        "  pipe:\n    enable: false\n    input_box: last_frame.xyz", "  pipe:\n    enable: true\n    input_box: %s" % path)
+
+
+def test_pipe_creation_matches_oracle(ak, tmp_path):
+    # vacancy positions (x doubled): inside the box, a repeat, and two outside it (skipped)
+    pile = [(0, 0, 0), (5, 3, 7), (23, 9, 13), (5, 3, 7), (24, 0, 0), (-1, 2, 2), (10, 2, 11)]
+    p = tmp_path / "last_frame.xyz"
+    p.write_text("".join("%d %d %d\n" % xyz for xyz in pile))
+    c = ak.config_parse(_pipe_config(str(p)))
+    assert c.create_pipe == 1 and c.create_random == 0 and c.pipe_input_box == str(p).encode()
+    assert list(c.type_codes) == [po.FE, po.CU, po.MN, po.NI] and list(c.ratio) == [9598, 134, 134, 134]
+    occ = ak.config_lattice(c)
+    cfg = po.make_config(box=(12, 10, 14), creation_mode=po.CREATE_MT19937_PILE, seed=100565,
+                         alloy=((po.FE, 9598), (po.CU, 134), (po.MN, 134), (po.NI, 134)), n_vacancies=0,
+                         lattice_const=2.85532, energy_model=po.MODEL_PAIRBOND, pile=pile)
+    o = po.Oracle(cfg)
+    assert np.array_equal(occ, o.occupancy())
+    sx, sy = 24, 10
+    want = sorted({x + sx * (y + sy * z) for x, y, z in pile if 0 <= x < 24 and 0 <= y < 10 and 0 <= z < 14})
+    assert list(np.flatnonzero(occ == 0)) == want
+    # the alloy is the random creation's (same mt19937 draws) away from the listed sites
+    rnd = ak.config_lattice(ak.config_parse(CONFIG))
+    keep = np.ones(occ.size, bool)
+    keep[want] = False
+    keep[rnd == 0] = False
+    assert np.array_equal(occ[keep], rnd[keep])
+
+
+def test_pipe_file_missing_and_restart(ak, tmp_path):
+    c = ak.config_parse(_pipe_config(str(tmp_path / "nowhere.xyz")))
+    with pytest.raises(ak.AkmcError) as e:
+        ak.config_lattice(c)
+    assert e.value.status == -1
+    restart = CONFIG.replace("    enable: true\n    va_count: 7", "    enable: false\n    va_count: 7").replace(
+        "  restart:\n    enable: false", "  restart:\n    enable: true")
+    with pytest.raises(ak.AkmcError) as e:
+        ak.config_parse(restart)
+    assert "akmc_restore_snapshot" in str(e.value)
