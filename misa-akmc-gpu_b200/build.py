@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libakmc_b200.so")
 SOURCES = ["akmc_kernels.cu", "akmc_cluster.cu", "akmc_api.cu", "akmc_model.cpp", "akmc_host.cpp", "akmc_server.cpp"]
-HEADERS = ["akmc_common.cuh", "akmc_device.h", "akmc_model.h", "akmc_host.h"]
+HEADERS = ["akmc_common.cuh", "akmc_device.h", "akmc_model.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -32,7 +32,10 @@ def _inputs():
     files = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
     files.append(os.path.join(ROOT, "include", "akmc.h"))
     files.append(os.path.abspath(__file__))
-    return [f for f in files if os.path.exists(f)]
+    missing = [f for f in files if not os.path.exists(f)]
+    if missing:
+        raise FileNotFoundError("build inputs missing: %s" % ", ".join(missing))
+    return files
 
 
 def up_to_date():
@@ -62,8 +65,6 @@ def build(force=False, verbose=False, extra_flags=(), lib_path=None):
     ] + ARCH + list(extra_flags)
     for s in SOURCES:
         src = os.path.join(CSRC, s)
-        if not os.path.exists(src):
-            continue
         obj = os.path.join(objdir, s + (".prof" if extra_flags else "") + ".o")
         cmd = [nvcc()] + common + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", src, "-o", obj]
         if verbose:

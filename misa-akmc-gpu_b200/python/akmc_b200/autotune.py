@@ -14,7 +14,7 @@ choice is made once, before the run it serves.
 """
 import time
 
-from . import MODEL_EAM, Engine, job_config
+from . import MODEL_EAM, AkmcError, Engine, job_config
 
 CANDIDATES = (8, 12, 16, 20, 24)
 
@@ -43,14 +43,27 @@ def _trial(jobs, lattices, eam, max_block_edge, rounds, warmup, device):
         return (eng.counters()["hops"] - h0) / dt
 
 
+# akmc_prepare's answer to a decomposition whose sector regions the hop kernels cannot stage
+_REGION_TOO_LARGE = ("does not fit in shared memory", "wider than 28 cells")
+
+
+def _region_too_large(e):
+    return isinstance(e, AkmcError) and e.status == -1 and any(m in str(e) for m in _REGION_TOO_LARGE)
+
+
 def tune_block_edge(jobs, lattices, eam, candidates=CANDIDATES, rounds=64, warmup=16, device=0):
     """jobs: dicts with box, precision, temperature, seed (as bench.py builds them); lattices:
-    their occupancy arrays.  Returns (best edge, {edge: hops/s})."""
+    their occupancy arrays.  Returns (best edge, {edge: hops/s}).  A candidate whose regions
+    do not fit the hop kernels is left out of the table; any other failure raises, and so does
+    a candidate list with no runnable entry."""
     table = {}
     for c in candidates:
         try:
             table[c] = _trial(jobs, lattices, eam, c, rounds, warmup, device)
-        except Exception:  # a decomposition the kernels cannot take (region too large)
-            table[c] = 0.0
+        except AkmcError as e:
+            if not _region_too_large(e):
+                raise
+    if not table:
+        raise RuntimeError("autotune: no candidate block edge of %r can run these jobs" % (tuple(candidates),))
     best = max(table, key=lambda c: table[c])
     return best, table

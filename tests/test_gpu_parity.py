@@ -85,6 +85,22 @@ def test_single_domain_20_cubed(ak, model, prec):
     eng.close()
 
 
+def test_serial_box_20_cubed_to_1e5_hops(ak):
+    # The plain serial workload at its stated length: BCC 20^3 cells, Fe-1.34Cu, 20 vacancies,
+    # T = 573 K, seed 42, EAM in FP64, single domain, run until past 1e5 hops (3328 sector
+    # rounds, 416 sublattice time steps of SubLattice::startTimeLoop, sublattice.inl:61-179).
+    # Every event (sites, species, u, total, dt), the final occupancy, the density cache, the 8
+    # sector clocks and the hop count must equal the oracle's bit for bit.
+    rounds = 3328
+    eng, (o,) = run_pair(ak, rounds, [dict(box=(20, 20, 20), model=po.MODEL_EAM, precision=po.FP64, seed=42,
+                                           temperature=573.0, alloy=CU_134, n_vacancies=20)])
+    assert o.hops >= 100000, o.hops
+    assert o.round == rounds
+    check_job(eng, o, 0, eng.events())
+    assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
+
+
 @pytest.mark.parametrize("schedule", [1, 2])  # round by round; dependency-driven
 def test_domain_blocks_quaternary(ak, schedule):
     kw = dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=60,
