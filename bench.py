@@ -255,8 +255,11 @@ def algorithmic_bytes(hops, evals, nact_sum, eam=True):
 
 
 # ---------------------------------------------------------------------------
-def build_engine(ak, jobs, device, stream, log=0, schedule=0):
-    eng = ak.Engine(device=device, stream=stream, event_log_capacity=log)
+def build_engine(ak, jobs, device, stream, log=0, schedule=0, shape=None):
+    """An engine with the jobs added and prepared; shape: the tuner's eval_warps / flow_take."""
+    shape = shape or {}
+    eng = ak.Engine(device=device, stream=stream, event_log_capacity=log, eval_warps=shape.get("eval_warps", 0),
+                    flow_take=shape.get("flow_take", 0))
     eng.set_round_schedule(schedule)
     lattices = []
     eam = ak.eam_johnson(42)
@@ -471,19 +474,18 @@ def config_of(args, jobs, workload=None, rounds=None):
 
 # ---------------------------------------------------------------------------
 def autotune_batched(ak, jobs, device, block_edge):
-    """The batched jobs' decomposition: the fastest of the tuner's candidates on this job set
-    (outside any timed region), or the fixed edge given."""
+    """The batched jobs' decomposition and kernel shape: the fastest of the tuner's candidates
+    on this job set (outside any timed region), or the fixed edge given with the default shape."""
     import akmc_b200.autotune as at
 
     if block_edge <= 0:
         lats = [ak.create_lattice(j["box"], j["alloy"], j["n_vacancies"], j["seed"]) for j in jobs]
-        edge, table = at.tune_block_edge(jobs, lats, ak.eam_johnson(42), device=device)
-        tuned = {"block_edge": edge, "trial_hops_per_s": {str(k): round(v) for k, v in table.items()}}
+        choice, table = at.tune(jobs, lats, ak.eam_johnson(42), device=device)
+        tuned = dict(choice, trial_hops_per_s={k: round(v) for k, v in table.items()})
     else:
-        edge = block_edge
-        tuned = {"block_edge": edge}
+        tuned = {"block_edge": block_edge, "eval_warps": 8, "flow_take": 0}
     for j in jobs:
-        j["blocks"] = tuple(at.blocks_for(e, edge) for e in j["box"])
+        j["blocks"] = tuple(at.blocks_for(e, tuned["block_edge"]) for e in j["box"])
     return tuned
 
 
@@ -595,7 +597,7 @@ def extras(args, ak, device, stream, torch, runner, clocks):
     R = args.batched_rounds
     jobs = workload_jobs("batched")
     tuned = autotune_batched(ak, jobs, device, args.block_edge)
-    eng, lattices = build_engine(ak, jobs, device, stream.cuda_stream)
+    eng, lattices = build_engine(ak, jobs, device, stream.cuda_stream, shape=tuned)
     ms, hops = runner.device_rate(eng, R, args.steps, args.warmup, "batched")
     e_dt, e_hops, nbytes = runner.end_to_end(eng, lattices, R, max(3, args.steps // 2), "batched_e2e")
     cfg = config_of(args, jobs, "batched", R)
@@ -718,7 +720,7 @@ def main():
     if args.workload == "batched":
         tuned = autotune_batched(ak, jobs, local, args.block_edge)
     eng, lattices = build_engine(ak, jobs, local, stream.cuda_stream,
-                                 schedule={"auto": 0, "rounds": 1, "flow": 2}[args.schedule])
+                                 schedule={"auto": 0, "rounds": 1, "flow": 2}[args.schedule], shape=tuned)
     R = args.rounds_per_step
     eam = jobs[0].get("model", 1) == 1
 

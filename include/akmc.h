@@ -124,6 +124,20 @@ typedef struct akmc_context_config {
   int64_t flow_sweep_limit;    /* AKMC_SCHEDULE_FLOW watchdog: sweeps per CTA and launch before
                                   the launch gives up with AKMC_ETIMEOUT; 0: 2^24.  Rounds
                                   already published stay complete; recover from a snapshot. */
+  /* Room for jobs admitted after akmc_prepare (akmc_admit_job); max_jobs = 0: none.  The device
+   * tables are sized at akmc_prepare for this many jobs, domain blocks and vacancies held at
+   * once (the jobs added before akmc_prepare included), and shared memory for domain blocks of
+   * up to max_block_edge cells (0: 24). */
+  int32_t max_jobs;
+  int32_t max_block_edge;
+  int64_t max_blocks;
+  int64_t max_vacancies;
+  /* Launch shape of the hop kernels (autotuned by akmc_b200.autotune): eval_warps = warps that
+   * evaluate a vacancy's 8 jumps, 8 (one jump each, one CTA per SM; 0 = 8) or 4 (two jumps each,
+   * two CTAs per SM); flow_take = rounds with vacancies a CTA of the dependency-driven schedule
+   * takes per sweep (0: all it finds).  Results do not depend on either. */
+  int32_t eval_warps;
+  int32_t flow_take;
 } akmc_context_config;
 
 typedef struct akmc_ctx akmc_ctx;
@@ -151,6 +165,19 @@ AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, con
  * device state of every registered job, uploads the lattices and builds the
  * density caches. */
 AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx);
+
+/* No reference counterpart (the reference runs one box per process).  Continuous batching:
+ * adds a job to a prepared context created with room for it (akmc_context_config.max_jobs),
+ * between calls that run rounds, without touching the jobs already running.  Its lattice,
+ * density cache, vacancies and random streams go into free slots of the device tables; it
+ * starts at round 0 and advances with every later akmc_run_rounds, its trajectory the same as
+ * alone.  A retired job's slot id may be given out again.  EBUSY when the context has no room
+ * left (jobs, blocks, vacancies or potentials), EINVAL for blocks larger than max_block_edge. */
+AKMC_API akmc_status akmc_admit_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
+                                    int32_t* job_id);
+/* Frees an admitted or added job's slots and device memory (read its results first); the other
+ * jobs run on untouched.  Later calls that name the job return ENOTFOUND. */
+AKMC_API akmc_status akmc_retire_job(akmc_ctx* ctx, int32_t job);
 
 /* Runs n sector rounds of every unfinished job on the device (the loop body of
  * SubLattice::startTimeLoop, sublattice.inl:64-177, for all domain blocks at
@@ -332,20 +359,23 @@ AKMC_API akmc_status akmc_dump_lattice(const uint8_t* occ, const int64_t box[3],
 AKMC_API akmc_status akmc_device_math(akmc_ctx* ctx, const double* x, int64_t n, double* exp_out, double* log_out);
 
 /*
- * Job server: many independent jobs (parameter sweeps, ensembles, requests) on one GPU.
- * Submitted jobs queue; worker lanes (one host thread and one CUDA stream each) take the
- * queued jobs in arrival order as a batch that fits the memory budget, run them together
- * in one context (akmc_add_job per job, then akmc_run_rounds in chunks), and publish each
- * job's result as soon as that job is done.  The server is internally synchronised: any
+ * Job server: many independent jobs (parameter sweeps, ensembles, requests) on one GPU, with
+ * continuous batching.  Submitted jobs queue; worker lanes (one host thread, one CUDA stream and
+ * one context each) admit queued jobs in arrival order into their running context as the
+ * device-memory budget and the context's room allow (akmc_admit_job), advance all of their live
+ * jobs together in chunks of rounds, and publish each job's result, and free its memory, as soon
+ * as that job is done (akmc_retire_job).  A job's state stays in device memory from admission to
+ * its end, and its result is the one it has alone.  The server is internally synchronised: any
  * host thread may submit and poll.  This replaces running one MPI job per box.
  */
 typedef struct akmc_server akmc_server;
 typedef struct akmc_server_config {
   int32_t device;           /* CUDA device ordinal */
-  int32_t lanes;            /* concurrent batches (0: 2) */
-  int64_t budget_bytes;     /* device memory the jobs of all running batches may hold (0: 8 GiB) */
-  int32_t max_batch_jobs;   /* jobs per batch (0: 512) */
-  int32_t chunk_rounds;     /* rounds between checks for finished jobs (0: 16) */
+  int32_t lanes;            /* lanes, each with its own context and stream (0: 2) */
+  int64_t budget_bytes;     /* device memory the running jobs of all lanes may hold (0: 8 GiB) */
+  int32_t max_batch_jobs;   /* jobs one lane runs at once (0: 512) */
+  int32_t chunk_rounds;     /* rounds between admissions and checks for finished jobs (0: 16; 4x
+                               that while nothing is queued) */
   int32_t order;            /* admission order of queued jobs: AKMC_SERVE_FIFO (arrival) or
                                AKMC_SERVE_SMALLEST_BUDGET (smallest hop budget first; jobs
                                without a budget last; ties in arrival order) */
@@ -355,16 +385,19 @@ typedef struct akmc_job_result {
   int64_t hops;
   int64_t rounds;
   double submit_s;          /* server clock (seconds since akmc_server_create) */
-  double start_s;           /* its batch started */
+  double start_s;           /* a lane took it */
   double finish_s;          /* the result was published */
   int32_t status;           /* akmc_status of the job */
   int32_t n_blocks;
-  char error[128];          /* akmc_last_error of its batch when status != AKMC_OK */
+  char error[128];          /* akmc_last_error of its lane's context when status != AKMC_OK */
+  uint64_t clocks_fnv;      /* FNV-1a 64 of the bytes of every domain block's 8 sector clocks (FP64)
+                               and hop count (int64), block after block, as akmc_get_block_clocks
+                               gives them: the end state of the job's clocks in one word */
 } akmc_job_result;
 AKMC_API akmc_status akmc_server_create(const akmc_server_config* cfg, akmc_server** out);
 /* Queues a job (cfg, its EAM tables and occ are copied).  The job must end by itself: a hop
- * budget or max_rounds.  EINVAL for a job no batch could run (bad config, or more device
- * memory than the whole budget). */
+ * budget or max_rounds.  EINVAL for a job no lane could run (bad config, domain blocks larger
+ * than 24 cells, or more device memory than the whole budget). */
 AKMC_API akmc_status akmc_server_submit(akmc_server* s, const akmc_job_config* cfg, const uint8_t* occ,
                                         int64_t n_sites, int64_t* ticket);
 /* ready = 1 once the job is done: res is filled and, when occ_out is not NULL, the final
@@ -379,11 +412,11 @@ AKMC_API akmc_status akmc_server_wait(akmc_server* s, int64_t ticket, double tim
 AKMC_API akmc_status akmc_server_stats(akmc_server* s, int64_t* queued, int64_t* running, int64_t* done);
 /* Finishes the running batches, fails the queued jobs (status AKMC_ESTATE) and frees the
  * server. */
-/* Where the lanes' time went, summed over lanes: seconds8 = [0] building contexts (create,
- * add, prepare, restore, and saving and tearing down at a refill), [1] running chunks (rounds
- * and the job-state read), [2] reading results, [3] waiting for work; parts of [0]: [4] create
- * and add, [5] prepare, [6] restore, [7] saving the snapshots at a refill; counts3 = chunks
- * run, live jobs summed over chunks (their ratio is the mean batch), contexts built. */
+/* Where the lanes' time went, summed over lanes: seconds8 = [0] changing the job sets (creating
+ * the lanes' contexts, admitting and retiring jobs), [1] running chunks (rounds and the job-state
+ * read), [2] reading results, [3] waiting for work; parts of [0]: [4] admitting, [5] creating the
+ * contexts, [6] retiring, [7] 0; counts3 = chunks run, live jobs summed over chunks (their ratio
+ * is the mean number of jobs a chunk advanced), contexts created. */
 AKMC_API akmc_status akmc_server_profile(akmc_server* s, double* seconds8, int64_t* counts3);
 AKMC_API akmc_status akmc_server_shutdown(akmc_server* s);
 

@@ -27,6 +27,8 @@ struct HostJob {
   int32_t block0 = 0, nblocks = 0;
   int32_t vac0 = 0;
   int32_t pot = 0;
+  int32_t area_max = 0;   // most vacancies in one of its block areas at the start
+  bool live = true;       // false: a retired slot (akmc_retire_job)
   std::vector<int32_t> split[3];
   uint8_t* d_occ = nullptr;
   int32_t* d_rho = nullptr;
@@ -86,7 +88,7 @@ struct akmc_ctx {
   int32_t schedule = AKMC_SCHEDULE_AUTO;
   bool flow_ok = false;  // more than one block, and every block area starts with few enough vacancies
   int flow_grid = 0;
-  int32_t* d_lease = nullptr;
+  unsigned long long* d_fstate = nullptr;
   unsigned long long* d_vclaim = nullptr;
   unsigned long long* d_vvalid = nullptr;
   int32_t* d_vslot = nullptr;
@@ -115,6 +117,12 @@ struct akmc_ctx {
   // host images of the initial device records (akmc_load_occupancy resets from them)
   std::vector<JobDev> h_jobs;
   std::vector<BlockDev> h_blocks;
+  // room for jobs admitted after akmc_prepare: capacities of the device tables, the largest
+  // block edge an admitted job may have, and the table ranges not in use ([start, end))
+  int32_t cap_jobs = 0, cap_blocks = 0, cap_vac = 0, cap_pots = 0;
+  int32_t max_edge = 0;
+  bool bulk_ok = false;  // shared memory sized for bulk staging
+  std::vector<std::pair<int32_t, int32_t>> free_blocks, free_vac;
 };
 
 namespace {
@@ -162,9 +170,9 @@ void free_device(akmc_ctx* ctx) {
   ctx->ev.clear();
   dfree(ctx->stream, ctx->d_vac_count);
   ctx->d_vac_count = nullptr;
-  void* flow_ptrs[] = {ctx->d_lease, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vcount, ctx->d_flow};
+  void* flow_ptrs[] = {ctx->d_fstate, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vcount, ctx->d_flow};
   for (void* p : flow_ptrs) dfree(ctx->stream, p);
-  ctx->d_lease = nullptr;
+  ctx->d_fstate = nullptr;
   ctx->d_vclaim = ctx->d_vvalid = nullptr;
   ctx->d_vslot = ctx->d_vcount = ctx->d_flow = nullptr;
   dfree(ctx->stream, ctx->d_cl);
@@ -283,6 +291,10 @@ uint64_t eam_hash(const HostJob& j) {
   return j.has_eam ? fnv1a(reinterpret_cast<const uint8_t*>(&j.eam), sizeof(j.eam)) : 0;
 }
 
+bool live_job(const akmc_ctx* ctx, int32_t job) {
+  return job >= 0 && job < static_cast<int32_t>(ctx->jobs.size()) && ctx->jobs[static_cast<size_t>(job)].live;
+}
+
 int64_t snapshot_bytes(const HostJob& j) {
   return static_cast<int64_t>(sizeof(SnapHeader)) + j.nblocks * static_cast<int64_t>(sizeof(SnapBlock)) + j.nsites;
 }
@@ -331,6 +343,11 @@ AKMC_API akmc_status akmc_create(const akmc_context_config* cfg, akmc_ctx** out)
   if (ctx->cfg.graph_rounds <= 0) ctx->cfg.graph_rounds = 32;
   if (ctx->cfg.hop_cap_per_round <= 0) ctx->cfg.hop_cap_per_round = 10000000;
   if (ctx->cfg.flow_sweep_limit <= 0) ctx->cfg.flow_sweep_limit = int64_t(1) << 24;
+  if (ctx->cfg.eval_warps == 0) ctx->cfg.eval_warps = 8;
+  if ((ctx->cfg.eval_warps != 8 && ctx->cfg.eval_warps != 4) || ctx->cfg.flow_take < 0) {
+    delete ctx;
+    return AKMC_EINVAL;
+  }
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) {
     delete ctx;
     return AKMC_ECUDA;
@@ -368,11 +385,12 @@ AKMC_API akmc_status akmc_destroy(akmc_ctx* ctx) {
 
 AKMC_API void* akmc_stream(akmc_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
-AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
-                                  int32_t* job_id) {
-  if (!ctx || !cfg || !occ) return AKMC_EINVAL;
-  if (ctx->prepared) return fail(ctx, AKMC_ESTATE, "jobs must be added before akmc_prepare");
-  HostJob j;
+}  // extern "C"
+
+namespace {
+
+// A job's configuration and lattice checked and copied into j (akmc_add_job, akmc_admit_job).
+akmc_status check_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites, HostJob& j) {
   j.cfg = *cfg;
   j.cfg.eam = nullptr;
   for (int d = 0; d < 3; ++d) {
@@ -396,6 +414,9 @@ AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, con
     if (!cfg->eam) return fail(ctx, AKMC_EINVAL, "EAM job without tables");
     j.has_eam = true;
     j.eam = *cfg->eam;
+    if (j.eam.n_shells != 5 || shells_within(cfg->lattice_const, cfg->cutoff_radius) != 5 ||
+        2.0 * cfg->lattice_const < cfg->cutoff_radius)
+      return fail(ctx, AKMC_EINVAL, "the EAM path needs exactly the 5 BCC shells inside the cutoff");
   }
   j.occ.assign(occ, occ + n_sites);
   for (int64_t s = 0; s < n_sites; ++s) {
@@ -404,6 +425,225 @@ AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, con
   }
   j.nblocks = (cfg->blocks[0] > 0 ? cfg->blocks[0] : 1) * (cfg->blocks[1] > 0 ? cfg->blocks[1] : 1) *
               (cfg->blocks[2] > 0 ? cfg->blocks[2] : 1);
+  for (size_t k = 0; k + 1 < j.split[0].size(); ++k) {
+    const int w = j.split[0][k + 1] - j.split[0][k];
+    if (2 * (w - w / 2 + 4) > 64)  // staged rows hold at most 64 sites (two per lane)
+      return fail(ctx, AKMC_EINVAL, "sector wider than 28 cells in x; use more domain blocks");
+  }
+  // vacancies per block area (the dependency-driven schedule keeps each area's in 64 slots)
+  std::vector<int32_t> per(static_cast<size_t>(j.nblocks), 0);
+  const int nbx = static_cast<int>(j.split[0].size()) - 1, nby = static_cast<int>(j.split[1].size()) - 1;
+  for (int64_t s = 0; s < n_sites; ++s) {
+    if (occ[s] != kV) continue;
+    const int64_t X = s % (2 * cfg->box[0]), t = s / (2 * cfg->box[0]);
+    const int64_t c[3] = {X >> 1, t % cfg->box[1], t / cfg->box[1]};
+    int bi[3];
+    for (int d = 0; d < 3; ++d) {
+      const auto& sp = j.split[d];
+      bi[d] = static_cast<int>(std::upper_bound(sp.begin(), sp.end(), static_cast<int32_t>(c[d])) - sp.begin()) - 1;
+    }
+    j.area_max = std::max(j.area_max, ++per[static_cast<size_t>(bi[0] + nbx * (bi[1] + nby * bi[2]))]);
+  }
+  return AKMC_OK;
+}
+
+// Largest block edge of a job, over the three dimensions.
+int max_block_edge(const HostJob& j) {
+  int e = 0;
+  for (int d = 0; d < 3; ++d)
+    for (size_t k = 0; k + 1 < j.split[d].size(); ++k) e = std::max(e, j.split[d][k + 1] - j.split[d][k]);
+  return e;
+}
+
+// Sites of the staged region of a block of edge e in every dimension (the largest a job with
+// blocks of at most e cells stages), rows padded as region_sites pads them.
+int region_sites_edge(int e, bool bulk) {
+  const int h = e - e / 2 + 4;
+  int ext = 2 * h;
+  if (bulk) ext = (ext + 14 + 15) & ~15;
+  return ext * h * h;
+}
+
+// The potential table entry of job j: an equal one already held, else a new entry (built on the
+// host; uploaded by upload_pot).  -1 when the context has no room for another potential.
+int find_or_add_pot(akmc_ctx* ctx, HostJob& j, int* rc) {
+  *rc = 0;
+  if (!j.has_eam) return 0;
+  for (size_t i = 1; i < ctx->pots.size(); ++i)
+    if (ctx->pots[i].has_eam && std::memcmp(&ctx->pots[i].src, &j.eam, sizeof(j.eam)) == 0) return static_cast<int>(i);
+  if (ctx->cap_pots > 0 && static_cast<int32_t>(ctx->pots.size()) >= ctx->cap_pots) return -1;
+  DevPot p;
+  p.has_eam = true;
+  p.src = j.eam;
+  *rc = build_potential(&j.eam, p.P, p.coef, p.f32);
+  if (*rc) return -1;
+  ctx->pots.push_back(std::move(p));
+  return static_cast<int>(ctx->pots.size() - 1);
+}
+
+// Device tables of potential i: F coefficients in two FP64 planes and the FP32 cells, and the
+// Potential record pointing at them (written to hp).
+akmc_status upload_pot(akmc_ctx* ctx, size_t i, Potential& hp) {
+  DevPot& p = ctx->pots[i];
+  std::vector<double> c64(static_cast<size_t>(kTabN) * 4);
+  std::vector<float> c32(static_cast<size_t>(kTabN) * 5);
+  for (size_t k = 0; k < static_cast<size_t>(kTabN); ++k) {
+    for (int jj = 0; jj < 2; ++jj) {
+      c64[2 * k + jj] = p.coef[4 * k + jj];
+      c64[2 * kTabN + 2 * k + jj] = p.coef[4 * k + 2 + jj];
+    }
+    const FCell32& f = p.f32[k];
+    c32[4 * k + 0] = f.hi;
+    c32[4 * k + 1] = f.lo;
+    c32[4 * k + 2] = f.c1;
+    c32[4 * k + 3] = f.c2;
+    c32[4 * static_cast<size_t>(kTabN) + k] = f.c3;
+  }
+  CK(dalloc(ctx->stream, &p.d_coef, c64.size()));
+  CK(dalloc(ctx->stream, &p.d_f32, c32.size()));
+  CK(cudaMemcpyAsync(p.d_coef, c64.data(), c64.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(p.d_f32, c32.data(), c32.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // the staging vectors go out of scope
+  hp = p.P;
+  hp.F64lo = reinterpret_cast<const double2*>(p.d_coef);
+  hp.F64hi = reinterpret_cast<const double2*>(p.d_coef) + kTabN;
+  hp.F32a = reinterpret_cast<const float4*>(p.d_f32);
+  hp.F32b = p.d_f32 + 4 * static_cast<size_t>(kTabN);
+  return AKMC_OK;
+}
+
+// Device memory of job j (occupancy uploaded; density cache allocated) and its records: the
+// JobDev, its blocks and its slice of the vacancy table (sites in id order), for slot ji.
+akmc_status setup_job(akmc_ctx* ctx, int32_t ji, JobDev& J, BlockDev* hb, int32_t* vsite, int32_t* vjob) {
+  HostJob& j = ctx->jobs[static_cast<size_t>(ji)];
+  CK(dalloc(ctx->stream, &j.d_occ, static_cast<size_t>(j.nsites)));
+  CK(cudaMemcpyAsync(j.d_occ, j.occ.data(), static_cast<size_t>(j.nsites), cudaMemcpyHostToDevice, ctx->stream));
+  if (j.has_eam) CK(dalloc(ctx->stream, &j.d_rho, static_cast<size_t>(j.nsites)));
+  std::memset(&J, 0, sizeof(J));
+  J.occ = j.d_occ;
+  J.rho = j.d_rho;
+  J.bulk = ctx->bulk_ok && (2 * j.cfg.box[0]) % 16 == 0 && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
+           (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
+  for (int d = 0; d < 3; ++d) {
+    J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
+    J.nb[d] = static_cast<int32_t>(j.split[d].size() - 1);
+  }
+  J.sx = 2 * J.n[0];
+  J.sy = J.n[1];
+  J.sz = J.n[2];
+  J.block0 = j.block0;
+  J.nblocks = j.nblocks;
+  J.model = j.cfg.energy_model;
+  J.precision = j.cfg.precision;
+  J.pot = j.pot;
+  J.hop_budget = j.cfg.hop_budget;
+  J.max_rounds = j.cfg.max_rounds;
+  J.nu = j.cfg.attempt_freq;
+  J.kT = kBoltzmann * j.cfg.temperature;
+  J.window = j.cfg.sector_window;
+  for (int b = 0; b < j.nblocks; ++b) {
+    BlockDev& B = hb[b];
+    std::memset(&B, 0, sizeof(B));
+    B.job = ji;
+    B.local_id = b;
+    const int bi[3] = {b % J.nb[0], (b / J.nb[0]) % J.nb[1], b / (J.nb[0] * J.nb[1])};
+    for (int d = 0; d < 3; ++d) {
+      B.c0[d] = j.split[d][static_cast<size_t>(bi[d])];
+      B.c1[d] = j.split[d][static_cast<size_t>(bi[d]) + 1];
+    }
+    xoshiro_seed(B.xs, j.cfg.seed, kTagSelect, static_cast<uint64_t>(b));
+    xoshiro_seed(B.xt, j.cfg.seed, kTagTime, static_cast<uint64_t>(b));
+  }
+  int32_t k = 0;
+  for (int64_t s = 0; s < j.nsites; ++s)
+    if (j.occ[static_cast<size_t>(s)] == kV) {
+      vsite[k] = static_cast<int32_t>(s);
+      vjob[k] = ji;
+      ++k;
+    }
+  return AKMC_OK;
+}
+
+// A free block slot and a free job slot as the kernels see them.
+BlockDev free_block_record() {
+  BlockDev B;
+  std::memset(&B, 0, sizeof(B));
+  B.job = -1;
+  B.done = 1;
+  return B;
+}
+JobDev free_job_record() {
+  JobDev J;
+  std::memset(&J, 0, sizeof(J));
+  J.done = 1;
+  return J;
+}
+
+// First-fit allocation of n consecutive entries from a list of free [start, end) ranges.
+int32_t take_range(std::vector<std::pair<int32_t, int32_t>>& fr, int32_t n) {
+  if (n == 0) return 0;
+  for (size_t i = 0; i < fr.size(); ++i)
+    if (fr[i].second - fr[i].first >= n) {
+      const int32_t at = fr[i].first;
+      fr[i].first += n;
+      if (fr[i].first == fr[i].second) fr.erase(fr.begin() + static_cast<std::ptrdiff_t>(i));
+      return at;
+    }
+  return -1;
+}
+void give_range(std::vector<std::pair<int32_t, int32_t>>& fr, int32_t at, int32_t n) {
+  if (n == 0) return;
+  fr.emplace_back(at, at + n);
+  std::sort(fr.begin(), fr.end());
+  std::vector<std::pair<int32_t, int32_t>> m;
+  for (const auto& r : fr) {
+    if (!m.empty() && m.back().second >= r.first) m.back().second = std::max(m.back().second, r.second);
+    else m.push_back(r);
+  }
+  fr.swap(m);
+}
+
+// Energy kinds present, and whether AUTO may pick the dependency-driven schedule: more than one
+// block slot, and every live job's block areas start with at most 32 vacancies.
+void refresh_job_set(akmc_ctx* ctx) {
+  int mask = 0, area = 0;
+  for (const auto& j : ctx->jobs) {
+    if (!j.live) continue;
+    mask |= 1 << (j.cfg.energy_model == AKMC_MODEL_PAIRBOND ? 0 : (j.cfg.precision == AKMC_FP32C ? 2 : 1));
+    area = std::max(area, j.area_max);
+  }
+  ctx->args.kind_mask = mask;
+  ctx->flow_ok = area <= kFlowSlots / 2 && ctx->cap_blocks > 1;
+}
+
+// After the job set changed: the captured round graph and the whole-context transfer tables
+// describe the old set; they are rebuilt when next needed.
+void drop_job_set_caches(akmc_ctx* ctx) {
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  if (ctx->graph_def) cudaGraphDestroy(ctx->graph_def);
+  ctx->graph = nullptr;
+  ctx->graph_def = nullptr;
+  void* jl_ptrs[] = {ctx->d_stage, ctx->d_chunks, ctx->d_job_counts, ctx->d_job_want, ctx->d_tile0, ctx->d_eam_jobs};
+  for (void* p : jl_ptrs) dfree(ctx->stream, p);
+  ctx->d_stage = nullptr;
+  ctx->d_chunks = nullptr;
+  ctx->d_job_counts = ctx->d_job_want = ctx->d_eam_jobs = nullptr;
+  ctx->d_tile0 = nullptr;
+  ctx->jl = JobsLoad{};
+  ctx->total_sites = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+AKMC_API akmc_status akmc_add_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
+                                  int32_t* job_id) {
+  if (!ctx || !cfg || !occ) return AKMC_EINVAL;
+  if (ctx->prepared) return fail(ctx, AKMC_ESTATE, "jobs must be added before akmc_prepare (akmc_admit_job after it)");
+  HostJob j;
+  const akmc_status st = check_job(ctx, cfg, occ, n_sites, j);
+  if (st != AKMC_OK) return st;
   ctx->jobs.push_back(std::move(j));
   if (job_id) *job_id = static_cast<int32_t>(ctx->jobs.size() - 1);
   return AKMC_OK;
@@ -414,7 +654,8 @@ static akmc_status build_rho_tables(akmc_ctx* ctx);
 AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   if (!ctx) return AKMC_EINVAL;
   if (ctx->prepared) return AKMC_OK;
-  if (ctx->jobs.empty()) return fail(ctx, AKMC_ESTATE, "no jobs");
+  const bool room = ctx->cfg.max_jobs > 0;
+  if (ctx->jobs.empty() && !room) return fail(ctx, AKMC_ESTATE, "no jobs");
   CK(cudaSetDevice(ctx->cfg.device));
   // potentials: pair-bond tables in every entry; EAM tables deduplicated by content
   ctx->pots.clear();
@@ -423,45 +664,42 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     if (build_potential(nullptr, pb.P, pb.coef, pb.f32)) return fail(ctx, AKMC_EINVAL, "potential");
     ctx->pots.push_back(std::move(pb));
   }
+  ctx->cap_pots = 0;  // no limit while the initial jobs are added
   int max_region = 0, max_region_bulk = 0;
   int32_t nb = 0, nv = 0;
   for (auto& j : ctx->jobs) {
-    j.pot = 0;
-    if (j.has_eam) {
-      int found = -1;
-      for (size_t i = 1; i < ctx->pots.size(); ++i)
-        if (std::memcmp(&ctx->pots[i].src, &j.eam, sizeof(j.eam)) == 0) found = static_cast<int>(i);
-      if (found < 0) {
-        DevPot p;
-        p.has_eam = true;
-        p.src = j.eam;
-        const int rc = build_potential(&j.eam, p.P, p.coef, p.f32);
-        if (rc == -2) return fail(ctx, AKMC_ERANGE, "EAM densities can exceed the F table");
-        if (rc) return fail(ctx, AKMC_EINVAL, "invalid EAM tables");
-        ctx->pots.push_back(std::move(p));
-        found = static_cast<int>(ctx->pots.size() - 1);
-      }
-      j.pot = found;
-    }
+    int rc = 0;
+    j.pot = find_or_add_pot(ctx, j, &rc);
+    if (rc == -2) return fail(ctx, AKMC_ERANGE, "EAM densities can exceed the F table");
+    if (rc || j.pot < 0) return fail(ctx, AKMC_EINVAL, "invalid EAM tables");
     j.block0 = nb;
     j.vac0 = nv;
     nb += j.nblocks;
     nv += static_cast<int32_t>(j.nvac);
     max_region = std::max(max_region, region_sites(j, false));
     max_region_bulk = std::max(max_region_bulk, region_sites(j, bulk_rows(j)));
-    for (size_t k = 0; k + 1 < j.split[0].size(); ++k) {
-      const int w = j.split[0][k + 1] - j.split[0][k];
-      if (2 * (w - w / 2 + 4) > 64)  // staged rows hold at most 64 sites (two per lane)
-        return fail(ctx, AKMC_EINVAL, "sector wider than 28 cells in x; use more domain blocks");
-    }
   }
-  ctx->nblocks = nb;
-  ctx->nvac = nv;
+  // room for jobs admitted later: tables sized to the configured capacities, shared memory to
+  // the largest block edge an admitted job may have
+  ctx->max_edge = room ? (ctx->cfg.max_block_edge > 0 ? ctx->cfg.max_block_edge : 24) : 0;
+  if (room) {
+    if (ctx->max_edge < 8 || 2 * (ctx->max_edge - ctx->max_edge / 2 + 4) > 64)
+      return fail(ctx, AKMC_EINVAL, "max_block_edge must be in [8, 56] cells");
+    max_region = std::max(max_region, region_sites_edge(ctx->max_edge, false));
+    max_region_bulk = std::max(max_region_bulk, region_sites_edge(ctx->max_edge, true));
+  }
+  ctx->cap_jobs = std::max<int32_t>(static_cast<int32_t>(ctx->jobs.size()), room ? ctx->cfg.max_jobs : 0);
+  ctx->cap_blocks = std::max<int32_t>(nb, room ? static_cast<int32_t>(std::min<int64_t>(ctx->cfg.max_blocks, INT32_MAX)) : 0);
+  ctx->cap_vac = std::max<int32_t>(nv, room ? static_cast<int32_t>(std::min<int64_t>(ctx->cfg.max_vacancies, INT32_MAX)) : 0);
+  if (room && (ctx->cap_blocks < 1 || ctx->cap_vac < 1)) return fail(ctx, AKMC_EINVAL, "max_blocks and max_vacancies must be > 0");
+  ctx->cap_pots = static_cast<int32_t>(ctx->pots.size()) + (room ? 16 : 0);
+  ctx->nblocks = ctx->cap_blocks;
+  ctx->nvac = ctx->cap_vac;
   int dev_smem = 0;
   CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
   // bulk staging where its wider rows fit, else row loads everywhere
-  const bool bulk = hop_smem_bytes(max_region_bulk) <= static_cast<size_t>(dev_smem);
-  ctx->smem = hop_smem_bytes(bulk ? max_region_bulk : max_region);
+  ctx->bulk_ok = hop_smem_bytes(max_region_bulk) <= static_cast<size_t>(dev_smem);
+  ctx->smem = hop_smem_bytes(ctx->bulk_ok ? max_region_bulk : max_region);
   if (ctx->smem > static_cast<size_t>(dev_smem))
     return fail(ctx, AKMC_EINVAL, "sector region does not fit in shared memory; use more domain blocks");
   {
@@ -478,145 +716,56 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   // regions (plus the 1 KB the SM reserves per CTA) fit; k_flow is persistent, one CTA per
   // slot.  k_hop also gets a second wave where two regions fit.
   const int fit = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
-  const int resident = std::min(fit, hop_ctas_per_sm());
-  ctx->hop_grid = std::max(1, std::min(nb, sms * fit));
-  ctx->flow_grid = std::max(1, std::min(nb, sms * resident));
+  const int resident = std::min(fit, hop_ctas_per_sm(ctx->cfg.eval_warps));
+  const int32_t cb = ctx->cap_blocks;
+  ctx->hop_grid = std::max(1, std::min(cb, sms * fit));
+  ctx->flow_grid = std::max(1, std::min(cb, sms * resident));
 
   // geometry and potentials
   Geometry geo;
-  int nsh = 5;
-  for (auto& j : ctx->jobs) nsh = std::min(nsh, shells_within(j.cfg.lattice_const, j.cfg.cutoff_radius));
-  for (auto& j : ctx->jobs)
-    if (j.has_eam && (j.eam.n_shells != 5 || shells_within(j.cfg.lattice_const, j.cfg.cutoff_radius) != 5 ||
-                      2.0 * j.cfg.lattice_const < j.cfg.cutoff_radius))
-      return fail(ctx, AKMC_EINVAL, "the EAM path needs exactly the 5 BCC shells inside the cutoff");
   build_geometry(geo, 5);
   CK(dalloc(ctx->stream, &ctx->d_geo, 1));
   CK(cudaMemcpyAsync(ctx->d_geo, &geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
-  std::vector<Potential> hp;
-  for (auto& p : ctx->pots) {
-    std::vector<double> c64(static_cast<size_t>(kTabN) * 4);
-    std::vector<float> c32(static_cast<size_t>(kTabN) * 5);
-    for (size_t k = 0; k < static_cast<size_t>(kTabN); ++k) {
-      for (int j = 0; j < 2; ++j) {
-        c64[2 * k + j] = p.coef[4 * k + j];
-        c64[2 * kTabN + 2 * k + j] = p.coef[4 * k + 2 + j];
-      }
-      const FCell32& f = p.f32[k];
-      c32[4 * k + 0] = f.hi;
-      c32[4 * k + 1] = f.lo;
-      c32[4 * k + 2] = f.c1;
-      c32[4 * k + 3] = f.c2;
-      c32[4 * static_cast<size_t>(kTabN) + k] = f.c3;
-    }
-    CK(dalloc(ctx->stream, &p.d_coef, c64.size()));
-    CK(dalloc(ctx->stream, &p.d_f32, c32.size()));
-    CK(cudaMemcpyAsync(p.d_coef, c64.data(), c64.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(p.d_f32, c32.data(), c32.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));  // the staging vectors go out of scope
-    Potential P = p.P;
-    P.F64lo = reinterpret_cast<const double2*>(p.d_coef);
-    P.F64hi = reinterpret_cast<const double2*>(p.d_coef) + kTabN;
-    P.F32a = reinterpret_cast<const float4*>(p.d_f32);
-    P.F32b = p.d_f32 + 4 * static_cast<size_t>(kTabN);
-    hp.push_back(P);
+  std::vector<Potential> hp(ctx->pots.size());
+  for (size_t i = 0; i < ctx->pots.size(); ++i) {
+    const akmc_status st = upload_pot(ctx, i, hp[i]);
+    if (st != AKMC_OK) return st;
   }
-  CK(dalloc(ctx->stream, &ctx->d_pots, hp.size()));
+  CK(dalloc(ctx->stream, &ctx->d_pots, static_cast<size_t>(ctx->cap_pots)));
   CK(cudaMemcpyAsync(ctx->d_pots, hp.data(), hp.size() * sizeof(Potential), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // hp leaves scope
 
-  // jobs, blocks, vacancies
-  std::vector<JobDev> hj(ctx->jobs.size());
-  std::vector<BlockDev> hb(static_cast<size_t>(nb));
-  std::vector<int32_t> vsite(static_cast<size_t>(nv)), vjob(static_cast<size_t>(nv));
+  // jobs, blocks, vacancies; free slots as the kernels skip them
+  std::vector<JobDev> hj(static_cast<size_t>(ctx->cap_jobs), free_job_record());
+  std::vector<BlockDev> hb(static_cast<size_t>(cb), free_block_record());
+  std::vector<int32_t> vsite(static_cast<size_t>(ctx->cap_vac), 0), vjob(static_cast<size_t>(ctx->cap_vac), -1);
   for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
     HostJob& j = ctx->jobs[ji];
-    CK(dalloc(ctx->stream, &j.d_occ, static_cast<size_t>(j.nsites)));
-    CK(cudaMemcpyAsync(j.d_occ, j.occ.data(), static_cast<size_t>(j.nsites), cudaMemcpyHostToDevice, ctx->stream));
-    if (j.has_eam) CK(dalloc(ctx->stream, &j.d_rho, static_cast<size_t>(j.nsites)));
-    JobDev& J = hj[ji];
-    std::memset(&J, 0, sizeof(J));
-    J.occ = j.d_occ;
-    J.rho = j.d_rho;
-    J.bulk = bulk && bulk_rows(j) && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
-             (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
-    for (int d = 0; d < 3; ++d) {
-      J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
-      J.nb[d] = static_cast<int32_t>(j.split[d].size() - 1);
-    }
-    J.sx = 2 * J.n[0];
-    J.sy = J.n[1];
-    J.sz = J.n[2];
-    J.block0 = j.block0;
-    J.nblocks = j.nblocks;
-    J.model = j.cfg.energy_model;
-    J.precision = j.cfg.precision;
-    J.pot = j.pot;
-    J.hop_budget = j.cfg.hop_budget;
-    J.max_rounds = j.cfg.max_rounds;
-    J.nu = j.cfg.attempt_freq;
-    J.kT = kBoltzmann * j.cfg.temperature;
-    J.window = j.cfg.sector_window;
-    for (int b = 0; b < j.nblocks; ++b) {
-      BlockDev& B = hb[static_cast<size_t>(j.block0 + b)];
-      std::memset(&B, 0, sizeof(B));
-      B.job = static_cast<int32_t>(ji);
-      B.local_id = b;
-      const int bi[3] = {b % J.nb[0], (b / J.nb[0]) % J.nb[1], b / (J.nb[0] * J.nb[1])};
-      for (int d = 0; d < 3; ++d) {
-        B.c0[d] = j.split[d][static_cast<size_t>(bi[d])];
-        B.c1[d] = j.split[d][static_cast<size_t>(bi[d]) + 1];
-      }
-      xoshiro_seed(B.xs, j.cfg.seed, kTagSelect, static_cast<uint64_t>(b));
-      xoshiro_seed(B.xt, j.cfg.seed, kTagTime, static_cast<uint64_t>(b));
-    }
-    int32_t k = j.vac0;
-    for (int64_t s = 0; s < j.nsites; ++s)
-      if (j.occ[static_cast<size_t>(s)] == kV) {
-        vsite[static_cast<size_t>(k)] = static_cast<int32_t>(s);
-        vjob[static_cast<size_t>(k)] = static_cast<int32_t>(ji);
-        ++k;
-      }
+    const akmc_status st = setup_job(ctx, static_cast<int32_t>(ji), hj[ji], hb.data() + j.block0, vsite.data() + j.vac0,
+                                     vjob.data() + j.vac0);
+    if (st != AKMC_OK) return st;
   }
+  ctx->free_blocks.clear();
+  ctx->free_vac.clear();
+  if (cb > nb) ctx->free_blocks.emplace_back(nb, cb);
+  if (ctx->cap_vac > nv) ctx->free_vac.emplace_back(nv, ctx->cap_vac);
+  const size_t ncap = static_cast<size_t>(cb);
   CK(dalloc(ctx->stream, &ctx->d_jobs, hj.size()));
   CK(dalloc(ctx->stream, &ctx->d_blocks, hb.size()));
   CK(dalloc(ctx->stream, &ctx->d_vac_site, vsite.size()));
   CK(dalloc(ctx->stream, &ctx->d_vac_job, vjob.size()));
-  CK(dalloc(ctx->stream, &ctx->d_blk_list, static_cast<size_t>(nb) * kMaxV));
-  CK(dalloc(ctx->stream, &ctx->d_active, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_blk_list, ncap * kMaxV));
+  CK(dalloc(ctx->stream, &ctx->d_active, ncap));
   CK(dalloc(ctx->stream, &ctx->d_n_active, 1));
   CK(dalloc(ctx->stream, &ctx->d_status, 1));
   CK(dalloc(ctx->stream, &ctx->d_counters, 24));
   CK(dalloc(ctx->stream, &ctx->d_vac_count, 1));
-  CK(dalloc(ctx->stream, &ctx->d_lease, static_cast<size_t>(nb)));
-  CK(dalloc(ctx->stream, &ctx->d_vclaim, static_cast<size_t>(nb)));
-  CK(dalloc(ctx->stream, &ctx->d_vvalid, static_cast<size_t>(nb)));
-  CK(dalloc(ctx->stream, &ctx->d_vslot, static_cast<size_t>(nb) * kFlowSlots));
-  CK(dalloc(ctx->stream, &ctx->d_vcount, static_cast<size_t>(nb)));
+  CK(dalloc(ctx->stream, &ctx->d_fstate, ncap));
+  CK(dalloc(ctx->stream, &ctx->d_vclaim, ncap));
+  CK(dalloc(ctx->stream, &ctx->d_vvalid, ncap));
+  CK(dalloc(ctx->stream, &ctx->d_vslot, ncap * kFlowSlots));
+  CK(dalloc(ctx->stream, &ctx->d_vcount, ncap));
   CK(dalloc(ctx->stream, &ctx->d_flow, 6));
-  {
-    // the asynchronous schedule keeps each block area's vacancies in kFlowSlots slots;
-    // it is chosen only with room left for vacancies to gather
-    std::vector<int32_t> per_block(static_cast<size_t>(nb), 0);
-    for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) {
-      const HostJob& j = ctx->jobs[ji];
-      const int nbx = static_cast<int>(j.split[0].size()) - 1, nby = static_cast<int>(j.split[1].size()) - 1;
-      for (int32_t k = j.vac0; k < j.vac0 + static_cast<int32_t>(j.nvac); ++k) {
-        const int64_t s = vsite[static_cast<size_t>(k)];
-        const int64_t X = s % (2 * j.cfg.box[0]), t = s / (2 * j.cfg.box[0]);
-        const int64_t c[3] = {X >> 1, t % j.cfg.box[1], t / j.cfg.box[1]};
-        int bi[3];
-        for (int d = 0; d < 3; ++d) {
-          const auto& sp = j.split[d];
-          bi[d] = static_cast<int>(std::upper_bound(sp.begin(), sp.end(), static_cast<int32_t>(c[d])) - sp.begin()) - 1;
-        }
-        per_block[static_cast<size_t>(j.block0 + bi[0] + nbx * (bi[1] + nby * bi[2]))] += 1;
-      }
-    }
-    int32_t mx = 0;
-    for (int32_t v : per_block) mx = std::max(mx, v);
-    // one block gains nothing from running rounds apart
-    ctx->flow_ok = mx <= kFlowSlots / 2 && nb > 1;
-  }
   CK(dalloc(ctx->stream, &ctx->d_log_count, 1));
   CK(dalloc(ctx->stream, &ctx->d_api_total, 1));
   CK(dalloc(ctx->stream, &ctx->d_api_event, 1));
@@ -628,14 +777,13 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   if (ctx->cfg.event_log_capacity > 0) CK(dalloc(ctx->stream, &ctx->d_log, static_cast<size_t>(ctx->cfg.event_log_capacity)));
   CK(cudaMemcpyAsync(ctx->d_jobs, hj.data(), hj.size() * sizeof(JobDev), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_blocks, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice, ctx->stream));
-  if (nv) {
-    CK(cudaMemcpyAsync(ctx->d_vac_site, vsite.data(), vsite.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->d_vac_job, vjob.data(), vjob.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-  }
+  CK(cudaMemcpyAsync(ctx->d_vac_site, vsite.data(), vsite.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_vac_job, vjob.data(), vjob.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_n_active, 0, 4, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_counters, 0, 192, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_log_count, 0, 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_fstate, 0, ncap * 8, ctx->stream));
   {  // density caches of every EAM job, one launch
     const akmc_status rt = build_rho_tables(ctx);
     if (rt != AKMC_OK) return rt;
@@ -650,16 +798,13 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   RoundArgs& a = ctx->args;
   std::memset(&a, 0, sizeof(a));
   a.jobs = ctx->d_jobs;
-  a.njobs = static_cast<int32_t>(ctx->jobs.size());
-  a.nblocks = nb;
+  a.njobs = ctx->cap_jobs;
+  a.nblocks = cb;
   a.blocks = ctx->d_blocks;
   a.vac_site = ctx->d_vac_site;
   a.vac_job = ctx->d_vac_job;
-  a.nvac = nv;
+  a.nvac = ctx->cap_vac;
   a.mode = kModeRound;
-  a.kind_mask = 0;
-  for (const auto& j : ctx->jobs)
-    a.kind_mask |= 1 << (j.cfg.energy_model == AKMC_MODEL_PAIRBOND ? 0 : (j.cfg.precision == AKMC_FP32C ? 2 : 1));
   a.blk_list = ctx->d_blk_list;
   a.active = ctx->d_active;
   a.n_active = ctx->d_n_active;
@@ -680,13 +825,16 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.api_rates = ctx->d_api_rates;
   a.api_sites = ctx->d_api_sites;
   a.api_count = ctx->d_api_count;
-  a.lease = ctx->d_lease;
+  a.fstate = ctx->d_fstate;
   a.vclaim = ctx->d_vclaim;
   a.vvalid = ctx->d_vvalid;
   a.vslot = ctx->d_vslot;
   a.vcount = ctx->d_vcount;
   a.flow_need = ctx->d_flow;
   a.flow_done = ctx->d_flow + 3;
+  a.flow_take = ctx->cfg.flow_take;
+  a.eval_warps = ctx->cfg.eval_warps;
+  refresh_job_set(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->h_jobs = hj;
   ctx->h_blocks = hb;
@@ -694,10 +842,112 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   return AKMC_OK;
 }
 
+AKMC_API akmc_status akmc_admit_job(akmc_ctx* ctx, const akmc_job_config* cfg, const uint8_t* occ, int64_t n_sites,
+                                    int32_t* job_id) {
+  if (!ctx || !cfg || !occ) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_admit_job needs a prepared context (akmc_add_job before it)");
+  if (ctx->max_edge <= 0) return fail(ctx, AKMC_ESTATE, "the context was created without room for admitted jobs (max_jobs)");
+  CK(cudaSetDevice(ctx->cfg.device));
+  HostJob j;
+  akmc_status st = check_job(ctx, cfg, occ, n_sites, j);
+  if (st != AKMC_OK) return st;
+  if (max_block_edge(j) > ctx->max_edge)
+    return fail(ctx, AKMC_EINVAL, "domain blocks larger than the context's max_block_edge (" +
+                                      std::to_string(ctx->max_edge) + " cells); use more blocks");
+  int32_t slot = -1;
+  for (size_t k = 0; k < ctx->jobs.size() && slot < 0; ++k)
+    if (!ctx->jobs[k].live) slot = static_cast<int32_t>(k);
+  if (slot < 0 && static_cast<int32_t>(ctx->jobs.size()) >= ctx->cap_jobs)
+    return fail(ctx, AKMC_EBUSY, "no free job slot (max_jobs " + std::to_string(ctx->cap_jobs) + ")");
+  j.block0 = take_range(ctx->free_blocks, j.nblocks);
+  if (j.block0 < 0) return fail(ctx, AKMC_EBUSY, "no room for the job's domain blocks (max_blocks)");
+  j.vac0 = take_range(ctx->free_vac, static_cast<int32_t>(j.nvac));
+  if (j.vac0 < 0) {
+    give_range(ctx->free_blocks, j.block0, j.nblocks);
+    return fail(ctx, AKMC_EBUSY, "no room for the job's vacancies (max_vacancies)");
+  }
+  const size_t npots = ctx->pots.size();
+  int rc = 0;
+  j.pot = find_or_add_pot(ctx, j, &rc);
+  if (j.pot < 0 || rc) {
+    give_range(ctx->free_blocks, j.block0, j.nblocks);
+    give_range(ctx->free_vac, j.vac0, static_cast<int32_t>(j.nvac));
+    if (rc == -2) return fail(ctx, AKMC_ERANGE, "EAM densities can exceed the F table");
+    return fail(ctx, rc ? AKMC_EINVAL : AKMC_EBUSY, rc ? "invalid EAM tables" : "no room for another potential");
+  }
+  if (ctx->pots.size() > npots) {
+    Potential hp;
+    st = upload_pot(ctx, npots, hp);
+    if (st != AKMC_OK) return st;
+    CK(cudaMemcpyAsync(ctx->d_pots + npots, &hp, sizeof(hp), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (slot < 0) {
+    slot = static_cast<int32_t>(ctx->jobs.size());
+    ctx->jobs.emplace_back();
+  }
+  ctx->jobs[static_cast<size_t>(slot)] = std::move(j);
+  HostJob& h = ctx->jobs[static_cast<size_t>(slot)];
+  JobDev J;
+  std::vector<BlockDev> hb(static_cast<size_t>(h.nblocks));
+  std::vector<int32_t> vsite(static_cast<size_t>(h.nvac)), vjob(static_cast<size_t>(h.nvac));
+  st = setup_job(ctx, slot, J, hb.data(), vsite.data(), vjob.data());
+  if (st != AKMC_OK) return st;
+  CK(cudaMemcpyAsync(ctx->d_jobs + slot, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks + h.block0, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  if (h.nvac) {
+    CK(cudaMemcpyAsync(ctx->d_vac_site + h.vac0, vsite.data(), vsite.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_vac_job + h.vac0, vjob.data(), vjob.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (h.has_eam) {
+    const int e = launch_init_rho(h.d_occ, h.d_rho, 2 * static_cast<int32_t>(h.cfg.box[0]),
+                                  static_cast<int32_t>(h.cfg.box[1]), static_cast<int32_t>(h.cfg.box[2]),
+                                  ctx->d_pots + h.pot, ctx->d_geo, ctx->d_status, ctx->stream);
+    if (e) return fail(ctx, AKMC_ECUDA, std::string("init rho: ") + cuda_name(e));
+  }
+  ctx->h_jobs[static_cast<size_t>(slot)] = J;
+  std::copy(hb.begin(), hb.end(), ctx->h_blocks.begin() + h.block0);
+  refresh_job_set(ctx);
+  drop_job_set_caches(ctx);
+  CK(cudaStreamSynchronize(ctx->stream));  // the host records leave scope
+  if (job_id) *job_id = slot;
+  return AKMC_OK;
+}
+
+AKMC_API akmc_status akmc_retire_job(akmc_ctx* ctx, int32_t job) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size()) || !ctx->jobs[static_cast<size_t>(job)].live)
+    return AKMC_ENOTFOUND;
+  CK(cudaSetDevice(ctx->cfg.device));
+  HostJob& h = ctx->jobs[static_cast<size_t>(job)];
+  const JobDev J = free_job_record();
+  const std::vector<BlockDev> hb(static_cast<size_t>(h.nblocks), free_block_record());
+  CK(cudaMemcpyAsync(ctx->d_jobs + job, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_blocks + h.block0, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  if (h.nvac) CK(cudaMemsetAsync(ctx->d_vac_job + h.vac0, 0xff, static_cast<size_t>(h.nvac) * 4, ctx->stream));
+  dfree(ctx->stream, h.d_occ);
+  dfree(ctx->stream, h.d_rho);
+  h.d_occ = nullptr;
+  h.d_rho = nullptr;
+  ctx->h_jobs[static_cast<size_t>(job)] = J;
+  std::copy(hb.begin(), hb.end(), ctx->h_blocks.begin() + h.block0);
+  give_range(ctx->free_blocks, h.block0, h.nblocks);
+  give_range(ctx->free_vac, h.vac0, static_cast<int32_t>(h.nvac));
+  h.live = false;
+  h.occ.clear();
+  h.occ.shrink_to_fit();
+  refresh_job_set(ctx);
+  drop_job_set_caches(ctx);
+  CK(cudaStreamSynchronize(ctx->stream));  // the host records leave scope
+  return AKMC_OK;
+}
+
 AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8_t* occ, int64_t n_sites) {
   if (!ctx || !occ) return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_sites != j.nsites) return fail(ctx, AKMC_EINVAL, "n_sites does not match the job");
   CK(cudaSetDevice(ctx->cfg.device));
@@ -720,7 +970,7 @@ AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8
 
 AKMC_API akmc_status akmc_snapshot_size(akmc_ctx* ctx, int32_t job, int64_t* bytes) {
   if (!ctx || !bytes) return AKMC_EINVAL;
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   *bytes = snapshot_bytes(ctx->jobs[static_cast<size_t>(job)]);
   return AKMC_OK;
 }
@@ -729,7 +979,7 @@ AKMC_API akmc_status akmc_save_snapshot(akmc_ctx* ctx, int32_t job, uint8_t* buf
   if (!ctx || !buf || !written) return AKMC_EINVAL;
   *written = 0;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   const int64_t need = snapshot_bytes(j);
   if (capacity < need) return fail(ctx, AKMC_EINVAL, "snapshot needs " + std::to_string(need) + " bytes");
@@ -788,7 +1038,7 @@ AKMC_API akmc_status akmc_save_snapshot(akmc_ctx* ctx, int32_t job, uint8_t* buf
 AKMC_API akmc_status akmc_restore_snapshot(akmc_ctx* ctx, int32_t job, const uint8_t* buf, int64_t n) {
   if (!ctx || !buf) return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   SnapHeader h{};
   if (n < static_cast<int64_t>(sizeof(h))) return fail(ctx, AKMC_EINVAL, "not a snapshot: too short");
@@ -844,7 +1094,7 @@ static akmc_status build_rho_tables(akmc_ctx* ctx) {
   std::vector<int64_t> tile0{0};
   for (size_t k = 0; k < ctx->jobs.size(); ++k) {
     const HostJob& j = ctx->jobs[k];
-    if (!j.has_eam) continue;
+    if (!j.has_eam || !j.live) continue;
     const int64_t sx = 2 * j.cfg.box[0], sy = j.cfg.box[1], sz = j.cfg.box[2];
     eam_jobs.push_back(static_cast<int32_t>(k));
     tile0.push_back(tile0.back() + ((sx + 31) / 32) * ((sy + 7) / 8) * ((sz + 3) / 4));
@@ -872,6 +1122,10 @@ static akmc_status setup_jobs_load(akmc_ctx* ctx) {
   int64_t off = 0;
   for (size_t k = 0; k < ctx->jobs.size(); ++k) {
     const HostJob& j = ctx->jobs[k];
+    if (!j.live) {  // a retired slot: no sites, and no vacancies expected
+      want.push_back(0);
+      continue;
+    }
     for (int64_t s0 = 0; s0 < j.nsites; s0 += kChunk) {
       SiteChunk c{};
       c.job = static_cast<int32_t>(k);
@@ -969,11 +1223,12 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
       e0 = ctx->ev[0];
       e1 = ctx->ev[1];
     }
-    // each block runs n_rounds (fewer if its job ends); jobs with a hop budget stop at each
-    // time-step boundary, so their launches run at most to the next one (one more launch for
-    // a job that starts between boundaries)
+    // each block runs n_rounds (fewer if its job ends); the blocks of a multi-block job with a
+    // hop budget stop at each time-step boundary, where k_flow_finalize checks the job's hops,
+    // so those launches run at most to the next one (one more launch for a job that starts
+    // between boundaries).  A single-block job's budget is checked inside the launch.
     bool budget = false;
-    for (const auto& j : ctx->jobs) budget = budget || j.cfg.hop_budget > 0;
+    for (const auto& j : ctx->jobs) budget = budget || (j.live && j.cfg.hop_budget > 0 && j.nblocks > 1);
     {
       const int e = launch_flow_begin(a, n_rounds, ctx->stream);
       if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
@@ -1142,7 +1397,7 @@ AKMC_API akmc_status akmc_run(akmc_ctx* ctx, int64_t max_rounds) {
 
 AKMC_API akmc_status akmc_get_job_state(akmc_ctx* ctx, int32_t job, akmc_job_state* st) {
   if (!ctx || !st) return AKMC_EINVAL;
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   std::memset(st, 0, sizeof(*st));
   st->n_blocks = j.nblocks;
@@ -1187,7 +1442,7 @@ AKMC_API akmc_status akmc_get_job_states(akmc_ctx* ctx, akmc_job_state* out, int
 
 AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out, int64_t n_sites) {
   if (!ctx || !out) return AKMC_EINVAL;
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_sites != j.nsites) return AKMC_EINVAL;
   if (!ctx->prepared) {
@@ -1201,7 +1456,7 @@ AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out
 
 AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int64_t n_sites) {
   if (!ctx || !out) return AKMC_EINVAL;
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_sites != j.nsites || !j.has_eam) return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
@@ -1212,7 +1467,7 @@ AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int6
 
 AKMC_API akmc_status akmc_get_block_clocks(akmc_ctx* ctx, int32_t job, double* evo, int64_t* hops, int32_t n_blocks) {
   if (!ctx || !evo || !hops) return AKMC_EINVAL;
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_blocks != j.nblocks) return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
@@ -1272,7 +1527,7 @@ AKMC_API akmc_status akmc_get_counters(akmc_ctx* ctx, int64_t* out8) {
 
 static akmc_status api_step(akmc_ctx* ctx, int32_t job, int32_t sector_id, int32_t mode, double u) {
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   if (ctx->jobs[static_cast<size_t>(job)].nblocks != 1)
     return fail(ctx, AKMC_EINVAL, "the per-hop entry points drive single-domain jobs");
   if (sector_id < 0 || sector_id > 7) return fail(ctx, AKMC_EINVAL, "sector id in [0, 7]");
@@ -1346,7 +1601,7 @@ AKMC_API akmc_status akmc_job_cluster_stats(akmc_ctx* ctx, int32_t job, int64_t*
   if (!ctx || !isolated_cu || hist_len < 0 || hist_len > AKMC_CLUSTER_MAX_BINS || (hist_len > 0 && !hist))
     return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  if (job < 0 || job >= static_cast<int32_t>(ctx->jobs.size())) return AKMC_ENOTFOUND;
+  if (!live_job(ctx, job)) return AKMC_ENOTFOUND;
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   CK(cudaSetDevice(ctx->cfg.device));
   if (ctx->cl_sites < j.nsites) {

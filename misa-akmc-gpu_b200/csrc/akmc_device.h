@@ -122,7 +122,7 @@ struct RoundArgs {
   unsigned long long* counters;  // hops, evaluations, rounds, blocks, n_act sum, staged sites, written sites, -
   int64_t hop_cap;
   // asynchronous round schedule (k_flow)
-  int32_t* lease;               // per block: 0 free, 1 held by a thread or CTA
+  unsigned long long* fstate;   // per block: rounds completed << 1, | 1 while a thread or CTA holds it
   unsigned long long* vclaim;   // per block: slots of vslot taken
   unsigned long long* vvalid;   // per block: slots of vslot holding a vacancy id
   int32_t* vslot;               // per block: kFlowSlots ids of the vacancies in its area
@@ -131,6 +131,8 @@ struct RoundArgs {
   int32_t* flow_done;           // per energy kind: blocks that reached their target
   int64_t flow_rounds;          // rounds this launch adds to every unfinished block
   int64_t flow_sweep_limit;     // sweeps per CTA before the launch gives up (kErrTimeout)
+  int32_t flow_take;            // rounds with vacancies a CTA takes per sweep (0: all it found)
+  int32_t eval_warps;           // CTA shape of the hop kernels: 8 or 4 evaluator warps
   // per-hop entry points
   int32_t api_job, api_sector;
   double api_u;
@@ -145,7 +147,7 @@ struct RoundArgs {
 // Kernel launchers (akmc_kernels.cu).
 size_t hop_smem_bytes(int max_region_sites);
 int configure_hop_smem(size_t smem);
-int hop_ctas_per_sm();  // CTAs of the hop kernels the register budget allows per SM
+int hop_ctas_per_sm(int eval_warps);  // CTAs of the hop kernels the register budget allows per SM
 // ev0/ev1 (cudaEvent_t or null) are recorded around the hop kernel.
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1);
 // Collects the vacancies of one job's lattice into its slice of the vacancy table and sets

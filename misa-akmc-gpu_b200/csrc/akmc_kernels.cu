@@ -28,16 +28,31 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kStageRows = 4;  // rows of the staged region each warp has in flight
 enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };  // energy kinds, one kernel instance each
-// CTA shape: kEvalWarps warps evaluate the 8 jump directions (warp w takes jumps w, w +
-// kEvalWarps, ...), one more warp controls the hop loop.
-constexpr int kEvalWarps = 8;
-constexpr int kJumpsPerWarp = 8 / kEvalWarps;
-constexpr int kThreads = 32 * (kEvalWarps + 1);
-constexpr int kCtl = 32 * kEvalWarps;  // control thread: first lane of the control warp
-static_assert(8 % kEvalWarps == 0, "whole jump directions per warp");
-// CTAs per SM the register budget is cut for: two 5-warp CTAs fit (10 warps, at most 3 per SM
-// partition), two 9-warp ones would cut a thread to 96 registers.
-constexpr int kCtasPerSm = kEvalWarps <= 4 ? 2 : 1;
+// CTA shape: W warps evaluate the 8 jump directions (warp w takes jumps w, w + W, ...), one
+// more warp controls the hop loop.  The hop kernels are built for W = 8 (one jump per warp) and
+// W = 4 (two jumps per warp, two CTAs per SM); a context picks one (akmc_context_config).
+template <int W>
+struct Shape {
+  static_assert(8 % W == 0, "whole jump directions per warp");
+  static constexpr int kEvalWarps = W;
+  static constexpr int kJumpsPerWarp = 8 / W;
+  static constexpr int kThreads = 32 * (W + 1);
+  static constexpr int kCtl = 32 * W;  // control thread: first lane of the control warp
+  // CTAs per SM the register budget is cut for: two 5-warp CTAs fit (10 warps, at most 3 per SM
+  // partition), two 9-warp ones would cut a thread to 96 registers.
+  static constexpr int kCtasPerSm = W <= 4 ? 2 : 1;
+};
+constexpr int kMaxThreads = Shape<8>::kThreads;
+// The shape's constants under their short names inside a kernel or device function of shape W.
+#define AKMC_SHAPE(W)                                         \
+  constexpr int kEvalWarps = Shape<W>::kEvalWarps;            \
+  constexpr int kJumpsPerWarp = Shape<W>::kJumpsPerWarp;      \
+  constexpr int kThreads = Shape<W>::kThreads;                \
+  constexpr int kCtl = Shape<W>::kCtl;                        \
+  (void)kEvalWarps;                                           \
+  (void)kJumpsPerWarp;                                        \
+  (void)kThreads;                                             \
+  (void)kCtl
 
 __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >= m ? v - m : v); }
 
@@ -135,7 +150,7 @@ struct Smem {
   uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
   // asynchronous schedule (k_flow)
   int8_t flow_lag[8][27];
-  int32_t flow_cand[kThreads];
+  int32_t flow_cand[kMaxThreads];
   int32_t flow_ncand, flow_stop, flow_progress, flow_more;
   int32_t fv[kFlowSlots], fslot[kFlowSlots], fnv;  // the sector's vacancies and their slots
   // device counters summed per CTA and added once when the kernel ends (per-round atomics on
@@ -225,7 +240,9 @@ __device__ __forceinline__ uint8_t* occ_of(int32_t* rho_s, int nreg) {
   return reinterpret_cast<uint8_t*>(rho_s) + ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15));
 }
 
+template <int W>
 __device__ void load_tables(Smem& sm, const Potential& P, const Geometry& G, const Region& R, int kind) {
+  AKMC_SHAPE(W);
   const bool eam = kind != kPairBond;
   const int tid = threadIdx.x;
   if (tid < 25) {
@@ -466,15 +483,17 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
 #endif
 
 // The hop loop of one block's active sector (or one per-hop API step), CTA-collective.
+// round_now is the block's round (its completed rounds), read by the caller.
 // The evaluator warps evaluate rates (warp w: jumps w, w + kEvalWarps, ...) and refresh
 // densities; the control warp keeps the ordered vacancy list, selects, performs the occupancy
 // swap and runs the clock.
 // vlist holds the ids of the cnt_in vacancies inside the sector (any order).  Returns
 // false, uniformly, when the sector's clock is already past its window: nothing ran and
 // the vacancy arrays of sm were not filled.
-template <int KIND>
+template <int KIND, int W>
 __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s,
-                          const int32_t* vlist, int cnt_in) {
+                          const int32_t* vlist, int cnt_in, int64_t round_now) {
+  AKMC_SHAPE(W);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const bool evaluator = warp < kEvalWarps;
@@ -490,7 +509,6 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const bool eam = KIND != kPairBond;
   // the block record, the lattice and the vacancy table are read at L2 (__ldcg): under the
   // asynchronous schedule another SM may have written them since this SM last looked
-  const int64_t round_now = __ldcg(&B.round);
   const int sec = a.mode == kModeRound ? sector_of_round(round_now) : a.api_sector;
   double thr = 0.0;
   if (a.mode == kModeRound) {
@@ -532,7 +550,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
   }
   if (need_tab) {
-    load_tables(sm, P, *a.geo, R, KIND);
+    load_tables<W>(sm, P, *a.geo, R, KIND);
     if (tid == 0) {
       sm.tab_key[0] = tab0;
       sm.tab_key[1] = tab1;
@@ -1021,15 +1039,16 @@ __device__ void dispatch_block(const RoundArgs& a, int gb, uint8_t* smem) {
   carve(smem, R.n, sm, occ_s, rho_s);
   const int32_t* vl = a.blk_list + static_cast<int64_t>(gb) * kMaxV;
   const int cnt = min(B.cnt, kMaxV);
-  if (J.model == AKMC_MODEL_PAIRBOND) run_block<kPairBond>(a, gb, *sm, occ_s, rho_s, vl, cnt);
-  else if (J.precision == AKMC_FP32C) run_block<kEam32>(a, gb, *sm, occ_s, rho_s, vl, cnt);
-  else run_block<kEam64>(a, gb, *sm, occ_s, rho_s, vl, cnt);
+  if (J.model == AKMC_MODEL_PAIRBOND) run_block<kPairBond, 8>(a, gb, *sm, occ_s, rho_s, vl, cnt, B.round);
+  else if (J.precision == AKMC_FP32C) run_block<kEam32, 8>(a, gb, *sm, occ_s, rho_s, vl, cnt, B.round);
+  else run_block<kEam64, 8>(a, gb, *sm, occ_s, rho_s, vl, cnt, B.round);
 }
 
 __global__ void k_bucket(RoundArgs a) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= a.nvac) return;
   const int j = a.vac_job[v];
+  if (j < 0) return;  // a free entry of the vacancy table (a context with room for admitted jobs)
   const JobDev& J = a.jobs[j];
   if (J.done) return;
   if (a.mode != kModeRound && j != a.api_job) return;
@@ -1076,7 +1095,9 @@ __device__ void init_cta_smem(uint8_t* smem) {
 }
 
 // Adds the CTA's counters (summed by the control thread) to the device counters; CTA-wide.
+template <int W>
 __device__ void cta_flush(const RoundArgs& a, uint8_t* smem) {
+  AKMC_SHAPE(W);
   Smem* sm = reinterpret_cast<Smem*>(smem);
   __syncthreads();
   if (threadIdx.x == kCtl) {
@@ -1094,8 +1115,8 @@ __device__ __forceinline__ int job_kind(const JobDev& J) {
 
 // One kernel per energy kind, so each holds only its own hop loop (instruction-cache
 // footprint); items of other kinds are left to their kernel.
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_hop(RoundArgs a) {
+template <int KIND, int W>
+__global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_hop(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int na = *a.n_active;
   if (static_cast<int>(blockIdx.x) >= na) return;
@@ -1110,9 +1131,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_hop(RoundArgs a) {
     uint8_t* occ_s;
     int32_t* rho_s;
     carve(smem, R.n, sm, occ_s, rho_s);
-    run_block<KIND>(a, gb, *sm, occ_s, rho_s, a.blk_list + static_cast<int64_t>(gb) * kMaxV, min(B.cnt, kMaxV));
+    run_block<KIND, W>(a, gb, *sm, occ_s, rho_s, a.blk_list + static_cast<int64_t>(gb) * kMaxV, min(B.cnt, kMaxV),
+                       B.round);
   }
-  cta_flush(a, smem);
+  cta_flush<W>(a, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1129,32 +1151,28 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_hop(RoundArgs a) {
 // k_flow is persistent.  Each sweep a thread takes one block: while the block's next
 // round is ready and its sector holds no vacancy, the thread runs that round alone (the
 // clock jumps to the window, sublattice.inl:108-112); a ready round with vacancies is
-// handed to the CTA, which runs the hop loop for it.  A block is held with a lease (an
-// atomic flag) while anything works on it, and nothing waits while holding a lease.
+// handed to the CTA, which runs the hop loop for it.  A block is held with a lease while
+// anything works on it, and nothing waits while holding a lease.  The lease and the block's
+// completed rounds share one 64-bit word (fstate = rounds << 1 | leased): one compare-and-swap
+// reads the round and takes the lease, and one store after a fence publishes the rounds run
+// and frees the lease together.  B.round is refreshed from the word when the launch ends.
+// A single-block job's rounds depend on nothing else, so the CTA that ran one runs the next
+// straight away (its hop budget is checked here, at each time-step boundary).
 
-__device__ __forceinline__ int64_t ld_acquire64(const int64_t* p) {
-  int64_t v;
-  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ int64_t ld_relaxed64(const int64_t* p) {
-  int64_t v;
-  // no memory clobber: a relaxed load orders nothing; the fence after it does
-  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
-  return v;
-}
 // Release/acquire fence at GPU scope (lighter than the sequentially consistent __threadfence).
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-__device__ __forceinline__ void st_release32(int32_t* p, int32_t v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ void st_release64(int64_t* p, int64_t v) {
-  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
 }
 
 // Rounds back to the latest earlier round of the neighbour at offset (dx, dy, dz) whose
@@ -1195,7 +1213,7 @@ __device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, in
 #pragma unroll
   for (int o = 0; o < 27; ++o) {
     const int k = lag[ph][o];
-    if (k) ok &= ld_relaxed64(&a.blocks[flow_neighbour(J, local_id, o)].round) >= r - k + 1;
+    if (k) ok &= static_cast<int64_t>(ld_relaxed_u64(&a.fstate[flow_neighbour(J, local_id, o)]) >> 1) >= r - k + 1;
   }
   if (ok) fence_acq_rel();
   return ok;
@@ -1240,33 +1258,62 @@ __device__ void flow_give(const RoundArgs& a, int o, int v) {
   atomicOr(a.status, kErrVacOverflow);
 }
 
-// Publishes round r of block B as complete.  The release is cumulative: writes of other
-// threads of the CTA that a barrier ordered before this call are released too.
-__device__ __forceinline__ void flow_publish(const RoundArgs& a, BlockDev& B, int64_t r, int kind) {
+// Publishes the block's completed rounds (rn) and keeps (keep = 1) or frees the lease, with
+// one store after a fence.  The fence is cumulative: writes of other threads of the CTA that a
+// barrier ordered before this call are released too.  `reached`: this lease holder moved the
+// block onto its target (each block is counted once).
+__device__ __forceinline__ void flow_publish(const RoundArgs& a, int gb, int64_t rn, int keep, bool reached,
+                                             int kind) {
   fence_acq_rel();
-  st_release64(&B.round, r + 1);
-  if (r + 1 == B.target) atomicAdd(&a.flow_done[kind], 1);
+  st_relaxed_u64(&a.fstate[gb], (static_cast<unsigned long long>(rn) << 1) | static_cast<unsigned long long>(keep));
+  if (reached) atomicAdd(&a.flow_done[kind], 1);
 }
 
-// Lease held, one thread: runs the block's ready rounds whose sectors hold no vacancy (the
-// clock jumps to the window, sublattice.inl:108-112), up to 64 in one batch.  The neighbours'
-// round counters are read once, all 27 loads in flight together: a round is ready when that
-// snapshot already covers it, and the vacancy slots read after the snapshot hold every vacancy
-// those rounds can see (a round that could bring one into such a sector overlaps it, so it is
-// in the snapshot).  Returns true when it stops at a ready round with vacancies, false when the
-// next round is not ready or the target is reached.
+// The block's target for this launch, read by its lease holder at L2 (a previous holder on
+// another SM may have moved it).  A single-block job with a hop budget ends at the end of the
+// first time step at which its hops reached the budget, so once they have, its target moves
+// down to the next boundary at or after rn (never below rn).
+__device__ __forceinline__ int64_t flow_target(BlockDev& B, const JobDev& J, int64_t rn) {
+  int64_t t = __ldcg(&B.target);
+  if (J.nblocks == 1 && J.hop_budget > 0 && __ldcg(&B.hops) >= J.hop_budget) {
+    const int64_t b = (rn + 7) & ~static_cast<int64_t>(7);
+    if (b < t) {
+      t = b;
+      B.target = t;
+    }
+  }
+  return t;
+}
+
+// Lease held, one thread, the block at round r0: runs the block's ready rounds whose sectors
+// hold no vacancy (the clock jumps to the window, sublattice.inl:108-112), up to 64 in one
+// batch, and leaves the block's round in *rn (the caller publishes it).  The neighbours' round
+// counters are read once, all 27 loads in flight together: a round is ready when that snapshot
+// already covers it, and the vacancy slots read after the snapshot hold every vacancy those
+// rounds can see (a round that could bring one into such a sector overlaps it, so it is in the
+// snapshot).  Returns true when it stops at a ready round with vacancies, false when the next
+// round is not ready or the target is reached.  *reached: this call moved the block onto its
+// target (by running rounds, or by a budget moving the target down to r0); false for a block
+// that was at its target already (a stale sweep read).
 __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, int gb, const int8_t (*lag)[27],
-                             int kind, int* progress) {
-  const int64_t r0 = ld_relaxed64(&B.round);
-  const int64_t target = B.target;
-  if (r0 >= target) return false;
+                             int64_t r0, int64_t* rn, bool* reached) {
+  *rn = r0;
+  *reached = false;
+  const int64_t t_old = __ldcg(&B.target);
+  if (r0 >= t_old) return false;
+  const int64_t target = flow_target(B, J, r0);
+  if (r0 >= target) {
+    *reached = true;
+    return false;
+  }
   const int n0 = J.nb[0], n1 = J.nb[1], n2 = J.nb[2], block0 = J.block0, lid = B.local_id;
   const int bx = lid % n0, by = (lid / n0) % n1, bz = lid / (n0 * n1);
   int64_t P[27];
 #pragma unroll
   for (int o = 0; o < 27; ++o) {
     const int y = block0 + wrapb(bx + o % 3 - 1, n0) + n0 * (wrapb(by + (o / 3) % 3 - 1, n1) + n1 * wrapb(bz + o / 9 - 1, n2));
-    P[o] = y == gb ? INT64_MAX : ld_relaxed64(&a.blocks[y].round);  // the block itself never holds it back
+    // the block itself never holds it back
+    P[o] = y == gb ? INT64_MAX : static_cast<int64_t>(ld_relaxed_u64(&a.fstate[y]) >> 1);
   }
   fence_acq_rel();
   double evo[8];
@@ -1316,21 +1363,21 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
   if (r > r0) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) B.evo[k] = evo[k];
-    flow_publish(a, B, r - 1, kind);
-    *progress = 1;
   }
+  *rn = r;
+  *reached = r == target;
   return stop_full;
 }
 
-// Rounds with vacancies a CTA takes per sweep, and rounds of one block it runs back to back
-// while the next one is ready.  Measured on the 256^3 lattice and the 512 batched boxes: taking
-// every ready round found, one round per block at a time, beats taking one per sweep (others
-// left to idle CTAs) and beats chaining up to 8 rounds of one block.
-constexpr int kFlowTake = kThreads;
-constexpr int kFlowChain = 1;
-
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
+// Rounds with vacancies a CTA takes per sweep: a.flow_take (0: every ready round its threads
+// found).  Measured on the 256^3 lattice and the 512 batched boxes: taking every ready round
+// found, one round per block at a time, beats taking one per sweep (others left to idle CTAs)
+// and beats chaining up to 8 rounds of one block of a multi-block job.  Single-block jobs chain:
+// their next round waits for nothing.
+template <int KIND, int W>
+__global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_flow(RoundArgs a) {
+  AKMC_SHAPE(W);
+  const int kFlowTake = a.flow_take > 0 && a.flow_take < kThreads ? a.flow_take : kThreads;
   extern __shared__ __align__(16) uint8_t smem[];
   Smem* sm0 = reinterpret_cast<Smem*>(smem);
   const int tid = threadIdx.x;
@@ -1369,23 +1416,25 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
       int gb = cursor + tid;
       if (gb >= nb) gb -= nb;
       BlockDev& B = a.blocks[gb];
-      const JobDev& J = a.jobs[B.job];
-      const int64_t r = ld_relaxed64(&B.round);
-      if (job_kind(J) == KIND && r < B.target && *reinterpret_cast<volatile int*>(&a.lease[gb]) == 0 &&
-          flow_ready(a, J, B.local_id, r, sm0->flow_lag) && atomicCAS(&a.lease[gb], 0, 1) == 0) {
+      const int bj = B.job;
+      const JobDev& J = a.jobs[bj < 0 ? 0 : bj];
+      const unsigned long long w = ld_relaxed_u64(&a.fstate[gb]);
+      const int64_t r = static_cast<int64_t>(w >> 1);
+      if (bj >= 0 && !(w & 1ull) && job_kind(J) == KIND && r < B.target && flow_ready(a, J, B.local_id, r, sm0->flow_lag) &&
+          atomicCAS(&a.fstate[gb], w, w | 1ull) == w) {
         fence_acq_rel();
-        bool keep = false;
-        if (flow_advance(a, B, J, gb, sm0->flow_lag, KIND, &sm0->flow_progress)) {
+        int64_t rn = r;
+        int keep = 0;
+        bool reached = false;
+        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &rn, &reached)) {
           const int i = atomicAdd(&sm0->flow_ncand, 1);
           if (i < kFlowTake) {
             sm0->flow_cand[i] = gb;
-            keep = true;
+            keep = 1;
           }
         }
-        if (!keep) {
-          fence_acq_rel();
-          atomicExch(&a.lease[gb], 0);
-        }
+        if (rn > r) sm0->flow_progress = 1;
+        flow_publish(a, gb, rn, keep, reached, KIND);
       }
     }
     __syncthreads();
@@ -1398,8 +1447,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
     }
 #endif
 
-    // the hop loop for each round handed over, then for the block's next rounds while they
-    // are ready (empty ones in between run on thread 0)
+    // the hop loop for each round handed over; a single-block job's next rounds follow while
+    // the launch's target allows (empty ones in between run on thread 0)
     const int ncand = min(sm0->flow_ncand, kFlowTake);
     for (int c = 0; c < ncand; ++c) {
       const int gb = sm0->flow_cand[c];
@@ -1412,7 +1461,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
         // the thread that found this round ready read the neighbours' round counters and then
         // fenced (an acquire), and a CTA barrier followed: every thread's reads come after the
         // rounds it waits for (shared data is read at L2)
-        const int64_t r = ld_acquire64(&B.round);
+        const int64_t r = static_cast<int64_t>(ld_acquire_u64(&a.fstate[gb]) >> 1);
         const int sec = sector_of_round(r);
         Region R;
         make_region(B, J, sec, R);
@@ -1441,7 +1490,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
           tw = clock64();
         }
 #endif
-        const bool ran = run_block<KIND>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt);
+        const bool ran = run_block<KIND, W>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt, r);
 #ifdef AKMC_PHASE_PROFILE
         if (tid == 0) tw = clock64();
 #endif
@@ -1468,22 +1517,22 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
 #ifdef AKMC_FLOW_PROFILE
           const long long q0 = clock64();
 #endif
-          flow_publish(a, B, r, KIND);
-          sm->flow_progress = 1;
+          // round r ran (it was below the target when handed over)
+          int64_t rn = r + 1;
+          bool more = false, reached = rn >= __ldcg(&B.target);
+          if (!reached && J.nblocks == 1) {
+            // a single-block job: its next rounds wait for nothing, so keep the lease and run on
+            more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, &rn, &reached);
+          }
 #ifdef AKMC_FLOW_PROFILE
           const long long q1 = clock64();
 #endif
-          // keep the lease for the block's next round with vacancies, if it is ready now
-          const bool more = link + 1 < kFlowChain && flow_advance(a, B, J, gb, sm0->flow_lag, KIND, &sm->flow_progress);
-#ifdef AKMC_FLOW_PROFILE
-          const long long q2 = clock64();
-#endif
+          sm->flow_progress = 1;
           sm->flow_more = more;
-          if (!more) st_release32(&a.lease[gb], 0);  // after the round's release: ordered behind it
+          flow_publish(a, gb, rn, more ? 1 : 0, reached, KIND);
 #ifdef AKMC_FLOW_PROFILE
           atomicAdd(a.counters + 20, static_cast<unsigned long long>(q1 - q0));
-          atomicAdd(a.counters + 21, static_cast<unsigned long long>(q2 - q1));
-          atomicAdd(a.counters + 22, static_cast<unsigned long long>(clock64() - q2));
+          atomicAdd(a.counters + 21, static_cast<unsigned long long>(clock64() - q1));
           atomicAdd(a.counters + 23, static_cast<unsigned long long>(q0 - tw));
 #endif
         }
@@ -1504,7 +1553,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_flow(RoundArgs a) {
     cursor += kThreads;
     if (cursor >= nb) cursor %= nb;
   }
-  cta_flush(a, smem);
+  cta_flush<W>(a, smem);
 #if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE)
   if (tid == 0) {  // scheduler profile: [12] sweep cycles, [13] hop-loop cycles, [14] sweeps, [15] full rounds
     atomicAdd(a.counters + 20, static_cast<unsigned long long>(t_sweep));
@@ -1521,27 +1570,33 @@ __global__ void k_flow_prep(RoundArgs a) {
   const int gb = blockIdx.x * blockDim.x + threadIdx.x;
   if (gb >= a.nblocks) return;
   BlockDev& B = a.blocks[gb];
+  B.cnt = 0;
+  a.vclaim[gb] = 0;
+  a.vvalid[gb] = 0;
+  a.vcount[gb] = 0;
+  if (B.job < 0) {  // a free block slot: nothing to run
+    B.target = B.round;
+    a.fstate[gb] = static_cast<unsigned long long>(B.round) << 1;
+    return;
+  }
   const JobDev& J = a.jobs[B.job];
-  // up to flow_rounds of the block's remaining rounds; a job with a hop budget stops at its next
-  // time-step boundary, where k_flow_finalize checks the budget
+  // up to flow_rounds of the block's remaining rounds; a multi-block job with a hop budget
+  // stops at its next time-step boundary, where k_flow_finalize checks the budget (a
+  // single-block job's budget is checked by the kernel)
   int64_t L = B.remaining < a.flow_rounds ? B.remaining : a.flow_rounds;
-  if (J.hop_budget > 0 && L > 8 - (B.round & 7)) L = 8 - (B.round & 7);
+  if (J.hop_budget > 0 && J.nblocks > 1 && L > 8 - (B.round & 7)) L = 8 - (B.round & 7);
   int64_t t = B.done ? B.round : B.round + L;
   if (J.max_rounds > 0 && t > J.max_rounds) t = J.max_rounds > B.round ? J.max_rounds : B.round;
   B.remaining -= t - B.round;
   B.target = t;
-  B.cnt = 0;
-  a.lease[gb] = 0;
-  a.vclaim[gb] = 0;
-  a.vvalid[gb] = 0;
-  a.vcount[gb] = 0;
+  a.fstate[gb] = static_cast<unsigned long long>(B.round) << 1;
   if (t > B.round) atomicAdd(&a.flow_need[job_kind(J)], 1);
 }
 
 // Per vacancy: into the slots of the block whose area holds it.
 __global__ void k_flow_slots(RoundArgs a) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= a.nvac) return;
+  if (v >= a.nvac || a.vac_job[v] < 0) return;
   const JobDev& J = a.jobs[a.vac_job[v]];
   const int o = owner_block(J, a.vac_site[v]);
   const int slot = atomicAdd(&a.vcount[o], 1);
@@ -1560,8 +1615,10 @@ __global__ void k_flow_finalize(RoundArgs a) {
   if (gb == 0) atomicAdd(a.counters + 2, static_cast<unsigned long long>(a.flow_rounds));
   if (gb >= a.nblocks) return;
   BlockDev& B = a.blocks[gb];
-  JobDev& J = a.jobs[B.job];
   B.cnt = 0;
+  B.round = static_cast<int64_t>(a.fstate[gb] >> 1);
+  if (B.job < 0) return;
+  JobDev& J = a.jobs[B.job];
   // J.hops holds the launch's hops (added when k_flow ended); all blocks of a budget job stop
   // at the same time-step boundary
   const int done = (J.max_rounds > 0 && B.round >= J.max_rounds) ||
@@ -1581,9 +1638,10 @@ __global__ void k_finalize(RoundArgs a) {
   }
   if (gb >= a.nblocks) return;
   BlockDev& B = a.blocks[gb];
-  JobDev& J = a.jobs[B.job];
   const int had = B.cnt;
   B.cnt = 0;
+  if (B.job < 0) return;  // a free block slot
+  JobDev& J = a.jobs[B.job];
   // J.done is only written here, by the job's block 0, so other blocks read their own flag
   if (B.done) return;
   if (had == 0) {  // no vacancy in the sector: total = 0, sector_time = threshold (sublattice.inl:108-112)
@@ -1605,7 +1663,7 @@ __global__ void k_finalize(RoundArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) k_api_block(RoundArgs a) {
+__global__ void __launch_bounds__(Shape<8>::kThreads, 1) k_api_block(RoundArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const JobDev& J = a.jobs[a.api_job];
   if (*a.n_active == 0) {  // no vacancy in the sector
@@ -1622,7 +1680,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_api_block(RoundArgs a) {
   }
   init_cta_smem(smem);
   dispatch_block(a, J.block0, smem);
-  cta_flush(a, smem);
+  cta_flush<8>(a, smem);
 }
 __global__ void k_api_reset(RoundArgs a) {
   const JobDev& J = a.jobs[a.api_job];
@@ -1828,13 +1886,27 @@ size_t hop_smem_bytes(int max_region_sites) {
          static_cast<size_t>(max_region_sites) + 16;
 }
 
+template <int W>
+void launch_hops(const RoundArgs& a, int hop_grid, size_t smem, cudaStream_t st) {
+  constexpr int T = Shape<W>::kThreads;
+  if (a.kind_mask & (1 << kEam64)) k_hop<kEam64, W><<<hop_grid, T, smem, st>>>(a);
+  if (a.kind_mask & (1 << kEam32)) k_hop<kEam32, W><<<hop_grid, T, smem, st>>>(a);
+  if (a.kind_mask & (1 << kPairBond)) k_hop<kPairBond, W><<<hop_grid, T, smem, st>>>(a);
+}
+template <int W>
+void launch_flows(const RoundArgs& a, int grid, size_t smem, cudaStream_t st) {
+  constexpr int T = Shape<W>::kThreads;
+  if (a.kind_mask & (1 << kEam64)) k_flow<kEam64, W><<<grid, T, smem, st>>>(a);
+  if (a.kind_mask & (1 << kEam32)) k_flow<kEam32, W><<<grid, T, smem, st>>>(a);
+  if (a.kind_mask & (1 << kPairBond)) k_flow<kPairBond, W><<<grid, T, smem, st>>>(a);
+}
+
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a.nvac > 0) k_bucket<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
   if (ev0) cudaEventRecord(static_cast<cudaEvent_t>(ev0), st);
-  if (a.kind_mask & (1 << kEam64)) k_hop<kEam64><<<hop_grid, kThreads, smem, st>>>(a);
-  if (a.kind_mask & (1 << kEam32)) k_hop<kEam32><<<hop_grid, kThreads, smem, st>>>(a);
-  if (a.kind_mask & (1 << kPairBond)) k_hop<kPairBond><<<hop_grid, kThreads, smem, st>>>(a);
+  if (a.eval_warps == 4) launch_hops<4>(a, hop_grid, smem, st);
+  else launch_hops<8>(a, hop_grid, smem, st);
   if (ev1) cudaEventRecord(static_cast<cudaEvent_t>(ev1), st);
   k_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
@@ -1843,7 +1915,7 @@ int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, vo
 int launch_api(const RoundArgs& a, size_t smem, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (a.nvac > 0) k_bucket<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
-  k_api_block<<<1, kThreads, smem, st>>>(a);
+  k_api_block<<<1, Shape<8>::kThreads, smem, st>>>(a);
   k_api_reset<<<1, 1, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
 }
@@ -1865,30 +1937,27 @@ int launch_flow(const RoundArgs& a, int grid, size_t smem, void* stream, void* e
   k_flow_prep<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   if (a.nvac > 0) k_flow_slots<<<(a.nvac + 127) / 128, 128, 0, st>>>(a);
   if (ev0) cudaEventRecord(static_cast<cudaEvent_t>(ev0), st);
-  if (a.kind_mask & (1 << kEam64)) k_flow<kEam64><<<grid, kThreads, smem, st>>>(a);
-  if (a.kind_mask & (1 << kEam32)) k_flow<kEam32><<<grid, kThreads, smem, st>>>(a);
-  if (a.kind_mask & (1 << kPairBond)) k_flow<kPairBond><<<grid, kThreads, smem, st>>>(a);
+  if (a.eval_warps == 4) launch_flows<4>(a, grid, smem, st);
+  else launch_flows<8>(a, grid, smem, st);
   if (ev1) cudaEventRecord(static_cast<cudaEvent_t>(ev1), st);
   k_flow_finalize<<<(a.nblocks + 127) / 128, 128, 0, st>>>(a);
   return static_cast<int>(cudaGetLastError());
 }
 
-int hop_ctas_per_sm() { return kCtasPerSm; }
+int hop_ctas_per_sm(int eval_warps) { return eval_warps == 4 ? Shape<4>::kCtasPerSm : Shape<8>::kCtasPerSm; }
 
 int configure_hop_smem(size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(k_hop<kEam64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_hop<kEam32>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_hop<kPairBond>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  const void* flows[] = {reinterpret_cast<const void*>(k_flow<kEam64>),
-                         reinterpret_cast<const void*>(k_flow<kEam32>),
-                         reinterpret_cast<const void*>(k_flow<kPairBond>)};
-  for (const void* f : flows)
+  const void* kernels[] = {
+      reinterpret_cast<const void*>(k_hop<kEam64, 8>),     reinterpret_cast<const void*>(k_hop<kEam32, 8>),
+      reinterpret_cast<const void*>(k_hop<kPairBond, 8>),  reinterpret_cast<const void*>(k_hop<kEam64, 4>),
+      reinterpret_cast<const void*>(k_hop<kEam32, 4>),     reinterpret_cast<const void*>(k_hop<kPairBond, 4>),
+      reinterpret_cast<const void*>(k_flow<kEam64, 8>),    reinterpret_cast<const void*>(k_flow<kEam32, 8>),
+      reinterpret_cast<const void*>(k_flow<kPairBond, 8>), reinterpret_cast<const void*>(k_flow<kEam64, 4>),
+      reinterpret_cast<const void*>(k_flow<kEam32, 4>),    reinterpret_cast<const void*>(k_flow<kPairBond, 4>),
+      reinterpret_cast<const void*>(k_api_block)};
+  cudaError_t e = cudaSuccess;
+  for (const void* f : kernels)
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e != cudaSuccess) return static_cast<int>(e);
-  e = cudaFuncSetAttribute(k_api_block, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   return static_cast<int>(e);
 }
 

@@ -1,18 +1,16 @@
 // akmc_server.cpp -- job server over the context API of include/akmc.h.
 //
-// Jobs queue in arrival order and are admitted oldest first, or smallest hop budget first.  Each lane (a host thread with its own context, hence its own
-// CUDA stream) takes the queued jobs that fit the device-memory budget as one batch and runs
-// them together in chunks of rounds.  A job's result is published, and its memory returned to
-// the budget, as soon as that job is done.  When an eighth of a batch has finished and queued
-// jobs fit, the lane refills: the running jobs are saved as restart snapshots, the context is
-// rebuilt with them and the newly admitted jobs, and the snapshots are restored, so every
-// job's trajectory is exactly the one it has alone.  A lane also refills, after 8 chunks, when
-// at least as many jobs wait as it runs.  A lane whose live jobs are all single-block boxes, with
-// none queued, runs them round by round in chunks 8 times longer: those jobs are the small boxes
-// with large hop budgets that end a run, latency bound, and the dependency-driven schedule's
-// launches (at most a time step each for budget jobs) cost more than their rounds; single-block
-// jobs keep one another's pace in lockstep.  Both schedules give the same trajectory.  Lanes overlap on the GPU.  All shared state is under one mutex; the device work
-// runs outside it.
+// Jobs queue in arrival order and are admitted oldest first, or smallest hop budget first.
+// Each lane is a host thread with one context (hence one CUDA stream) for its whole life,
+// created with room for many jobs (akmc_context_config.max_jobs).  Between chunks of rounds the
+// lane admits queued jobs that fit the device-memory budget and the context's room
+// (akmc_admit_job), runs one chunk of rounds of every live job, and publishes each job that is
+// done -- its lattice read back, its slots and memory freed (akmc_retire_job) -- while the
+// others keep running.  So a job's lattice, density cache, vacancies and random streams stay in
+// device memory from admission to its end, and its trajectory is exactly the one it has alone.
+// With nothing queued, a chunk is kIdleChunks times longer (the queue is checked after every
+// chunk, so a job arriving then waits at most one chunk).  Lanes overlap on the GPU.  All shared
+// state is under one mutex; the device work runs outside it.
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -31,9 +29,12 @@
 
 namespace {
 
-// Chunks of a batch's tail (single-block jobs only, empty queue): this many times the
-// configured length.
-constexpr int64_t kTailChunks = 8;
+// With no job queued, chunks are this many times the configured length.
+constexpr int64_t kIdleChunks = 4;
+// Room of a lane's context: domain blocks and vacancies held at once, the largest block edge.
+constexpr int64_t kLaneBlocks = 1 << 14;
+constexpr int64_t kLaneVacancies = 1 << 18;
+constexpr int32_t kLaneBlockEdge = 24;
 
 struct SJob {
   int64_t ticket = 0;
@@ -45,7 +46,7 @@ struct SJob {
   int state = 0;  // 0 queued, 1 running, 2 done
   akmc_job_result res{};
   std::vector<uint8_t> out;
-  std::vector<uint8_t> snap;  // restart snapshot while the job moves to a rebuilt context
+  int32_t slot = -1;  // its job id in the lane's context while it runs
 };
 
 // Device bytes a job holds: occupancy, density cache, block records and lists, vacancies.
@@ -68,11 +69,12 @@ struct akmc_server {
   int64_t running = 0;  // jobs in running batches
   bool stopping = false;
   std::vector<std::thread> lanes;
-  // profile, summed over lanes (under the mutex): seconds building contexts (create, add,
-  // prepare, restore), running chunks (rounds and the job-state read), reading results, and
-  // waiting for work; chunks run, live jobs summed over chunks, contexts built
+  // profile, summed over lanes (under the mutex): seconds changing the lanes' job sets
+  // (creating the contexts, admitting and retiring jobs), running chunks (rounds and the
+  // job-state read), reading results, and waiting for work; chunks run, live jobs summed over
+  // chunks, contexts built
   double t_build = 0, t_run = 0, t_publish = 0, t_wait = 0;
-  double t_add = 0, t_prepare = 0, t_restore = 0, t_save = 0;  // parts of t_build
+  double t_admit = 0, t_create = 0, t_retire = 0;  // parts of t_build
   int64_t n_chunks = 0, n_live = 0, n_builds = 0;
   void add_time(double& slot, std::chrono::steady_clock::time_point since) {
     const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - since).count();
@@ -95,8 +97,6 @@ struct akmc_server {
       std::memcpy(j->res.error, msg, sizeof(msg));
       j->res.finish_s = now();
       j->state = 2;
-      j->snap.clear();
-      j->snap.shrink_to_fit();
       --running;
       held -= j->bytes;
     }
@@ -121,149 +121,166 @@ struct akmc_server {
     return !queue.empty() && held + (*next_locked())->bytes <= cfg.budget_bytes;
   }
 
-  // Under the lock: moves queued jobs that fit into `live`.
-  void take_locked(std::vector<std::shared_ptr<SJob>>& live) {
-    while (fits_locked() && static_cast<int32_t>(live.size()) < cfg.max_batch_jobs) {
-      const auto it = next_locked();
-      auto j = *it;
-      queue.erase(it);
-      j->state = 1;
-      j->res.start_s = now();
-      held += j->bytes;
-      ++running;
-      live.push_back(j);
-    }
+  // Under the lock: the next queued job that fits the budget, moved to running.
+  std::shared_ptr<SJob> take_one_locked() {
+    if (stopping || !fits_locked()) return nullptr;
+    const auto it = next_locked();
+    auto j = *it;
+    queue.erase(it);
+    j->state = 1;
+    j->res.start_s = now();
+    held += j->bytes;
+    ++running;
+    return j;
+  }
+  // Under the lock: a job taken but not admitted (the context is full) goes back to the front.
+  void put_back_locked(const std::shared_ptr<SJob>& j) {
+    j->state = 0;
+    held -= j->bytes;
+    --running;
+    queue.push_front(j);
   }
 
-  // Runs `live` until every job is done, refilling from the queue on the way.
-  void run_batch(std::vector<std::shared_ptr<SJob>>& live) {
-    while (!live.empty()) {
-      auto tb = std::chrono::steady_clock::now();
-      akmc_context_config cc{};
-      cc.device = cfg.device;
-      cc.graph_rounds = cfg.chunk_rounds;
-      akmc_ctx* ctx = nullptr;
-      akmc_status st = akmc_create(&cc, &ctx);
-      if (st != AKMC_OK) {
-        for (auto& j : live) publish(j, st);
-        live.clear();
-        return;
+  // One lane: a context for the lane's life, jobs admitted and retired between chunks.
+  void lane() {
+    auto tc = std::chrono::steady_clock::now();
+    akmc_context_config cc{};
+    cc.device = cfg.device;
+    cc.graph_rounds = cfg.chunk_rounds;
+    cc.max_jobs = cfg.max_batch_jobs;
+    cc.max_block_edge = kLaneBlockEdge;
+    cc.max_blocks = kLaneBlocks;
+    cc.max_vacancies = kLaneVacancies;
+    akmc_ctx* ctx = nullptr;
+    akmc_status st = akmc_create(&cc, &ctx);
+    if (st == AKMC_OK) st = akmc_prepare(ctx);
+    add_time(t_create, tc);
+    add_time(t_build, tc);
+    {
+      std::lock_guard<std::mutex> lk(m);
+      ++n_builds;
+    }
+    std::vector<std::shared_ptr<SJob>> slots;  // by job id of the context
+    std::vector<akmc_job_state> js;
+    size_t live = 0;
+    if (st != AKMC_OK) {  // no context: every job this lane takes fails with the reason
+      for (;;) {
+        std::shared_ptr<SJob> j;
+        {
+          std::unique_lock<std::mutex> lk(m);
+          cv_work.wait(lk, [&] { return stopping || fits_locked(); });
+          if (stopping) break;
+          j = take_one_locked();
+        }
+        if (j) publish(j, st, ctx);
       }
-      auto tpart = std::chrono::steady_clock::now();
-      std::vector<std::shared_ptr<SJob>> in;  // jobs of this context, by job id
-      for (auto& j : live) {
+      if (ctx) akmc_destroy(ctx);
+      return;
+    }
+    for (;;) {
+      // admit what fits (budget and room), oldest (or smallest budget) first
+      auto ta = std::chrono::steady_clock::now();
+      while (st == AKMC_OK) {
+        std::shared_ptr<SJob> j;
+        {
+          std::lock_guard<std::mutex> lk(m);
+          if (static_cast<int32_t>(live) >= cfg.max_batch_jobs) break;
+          j = take_one_locked();
+        }
+        if (!j) break;
         akmc_job_config c = j->cfg;
         c.eam = j->has_eam ? &j->eam : nullptr;
         int32_t id = -1;
-        const akmc_status s = akmc_add_job(ctx, &c, j->occ.data(), static_cast<int64_t>(j->occ.size()), &id);
-        if (s != AKMC_OK) publish(j, s, ctx);
-        else in.push_back(j);
-      }
-      add_time(t_add, tpart);
-      tpart = std::chrono::steady_clock::now();
-      if (!in.empty()) st = akmc_prepare(ctx);
-      add_time(t_prepare, tpart);
-      tpart = std::chrono::steady_clock::now();
-      for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k)
-        if (!in[k]->snap.empty())
-          st = akmc_restore_snapshot(ctx, static_cast<int32_t>(k), in[k]->snap.data(),
-                                     static_cast<int64_t>(in[k]->snap.size()));
-      add_time(t_restore, tpart);
-      add_time(t_build, tb);
-      {
-        std::lock_guard<std::mutex> lk(m);
-        ++n_builds;
-      }
-      std::vector<bool> over(in.size(), false);
-      std::vector<akmc_job_state> js(in.size());
-      size_t left = in.size(), finished = 0, chunks_here = 0;
-      const size_t refill_after = std::max<size_t>(1, in.size() / 8);
-      bool refill = false;
-      while (st == AKMC_OK && left > 0 && !refill) {
-        auto tr = std::chrono::steady_clock::now();
-        bool tail = chunks_here > 0;  // job states known
-        for (size_t k = 0; tail && k < in.size(); ++k) tail = over[k] || js[k].n_blocks == 1;
-        if (tail) {
+        const akmc_status s = akmc_admit_job(ctx, &c, j->occ.data(), static_cast<int64_t>(j->occ.size()), &id);
+        if (s == AKMC_EBUSY && live > 0) {  // no room until a running job ends
           std::lock_guard<std::mutex> lk(m);
-          tail = queue.empty();
+          put_back_locked(j);
+          break;
         }
-        st = akmc_set_round_schedule(ctx, tail ? AKMC_SCHEDULE_ROUNDS : AKMC_SCHEDULE_AUTO);
-        if (st == AKMC_OK) st = akmc_run_rounds(ctx, tail ? kTailChunks * cfg.chunk_rounds : cfg.chunk_rounds);
-        if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(in.size()));
-        add_time(t_run, tr);
-        {
-          std::lock_guard<std::mutex> lk(m);
-          ++n_chunks;
-          n_live += static_cast<int64_t>(left);
-        }
-        auto tp = std::chrono::steady_clock::now();
-        for (size_t k = 0; st == AKMC_OK && k < in.size(); ++k) {
-          if (over[k] || !js[k].done) continue;
-          auto& j = in[k];
-          j->out.resize(j->occ.size());
-          st = akmc_get_occupancy(ctx, static_cast<int32_t>(k), j->out.data(), static_cast<int64_t>(j->out.size()));
-          if (st != AKMC_OK) break;
-          j->res.hops = js[k].hops;
-          j->res.rounds = js[k].round;
-          j->res.n_blocks = js[k].n_blocks;
-          publish(j, AKMC_OK);
-          over[k] = true;
-          --left;
-          ++finished;
-        }
-        add_time(t_publish, tp);
-        ++chunks_here;
-        if (st == AKMC_OK && left > 0) {
-          // refill when an eighth of the batch is done, or when at least as many jobs wait as
-          // run (a small early batch of long jobs must not hold the queue back)
-          std::lock_guard<std::mutex> lk(m);
-          const bool grow = queue.size() >= left && chunks_here >= 8;
-          refill = !stopping && fits_locked() && static_cast<int32_t>(left) < cfg.max_batch_jobs &&
-                   (finished >= refill_after || grow);
-        }
-      }
-      live.clear();
-      tb = std::chrono::steady_clock::now();
-      for (size_t k = 0; k < in.size(); ++k) {
-        if (over[k]) continue;
-        if (st != AKMC_OK) {
-          publish(in[k], st, ctx);
+        if (s != AKMC_OK) {
+          publish(j, s, ctx);
           continue;
         }
-        // carried into the next context
-        int64_t n = 0;
-        st = akmc_snapshot_size(ctx, static_cast<int32_t>(k), &n);
-        if (st == AKMC_OK) {
-          in[k]->snap.resize(static_cast<size_t>(n));
-          int64_t w = 0;
-          st = akmc_save_snapshot(ctx, static_cast<int32_t>(k), in[k]->snap.data(), n, &w);
-        }
-        if (st != AKMC_OK) publish(in[k], st, ctx);
-        else live.push_back(in[k]);
+        j->slot = id;
+        if (static_cast<size_t>(id) >= slots.size()) slots.resize(static_cast<size_t>(id) + 1);
+        slots[static_cast<size_t>(id)] = j;
+        ++live;
       }
-      add_time(t_save, tb);
-      akmc_destroy(ctx);
-      add_time(t_build, tb);
-      if (!live.empty()) {
-        std::lock_guard<std::mutex> lk(m);
-        take_locked(live);
+      add_time(t_admit, ta);
+      add_time(t_build, ta);
+      if (st != AKMC_OK) {  // the lane's context failed: its jobs fail, the lane stops
+        for (auto& j : slots)
+          if (j) publish(j, st, ctx);
+        break;
       }
-    }
-  }
-
-  void lane() {
-    for (;;) {
-      std::vector<std::shared_ptr<SJob>> live;
-      {
+      if (live == 0) {
         const auto tw = std::chrono::steady_clock::now();
         std::unique_lock<std::mutex> lk(m);
         cv_work.wait(lk, [&] { return stopping || fits_locked(); });
         t_wait += std::chrono::duration<double>(std::chrono::steady_clock::now() - tw).count();
-        if (stopping) return;
-        take_locked(live);
+        if (stopping) break;
+        continue;
       }
-      run_batch(live);
+      // one chunk of rounds of every live job
+      auto tr = std::chrono::steady_clock::now();
+      bool idle = false;
+      {
+        std::lock_guard<std::mutex> lk(m);
+        idle = queue.empty();
+      }
+      st = akmc_run_rounds(ctx, idle ? kIdleChunks * cfg.chunk_rounds : cfg.chunk_rounds);
+      js.resize(slots.size());
+      if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(js.size()));
+      add_time(t_run, tr);
+      {
+        std::lock_guard<std::mutex> lk(m);
+        ++n_chunks;
+        n_live += static_cast<int64_t>(live);
+      }
+      // publish and retire the jobs that are done
+      auto tp = std::chrono::steady_clock::now();
+      for (size_t k = 0; st == AKMC_OK && k < slots.size(); ++k) {
+        auto& j = slots[k];
+        if (!j || !js[k].done) continue;
+        j->out.resize(j->occ.size());
+        st = akmc_get_occupancy(ctx, static_cast<int32_t>(k), j->out.data(), static_cast<int64_t>(j->out.size()));
+        if (st != AKMC_OK) break;
+        j->res.hops = js[k].hops;
+        j->res.rounds = js[k].round;
+        j->res.n_blocks = js[k].n_blocks;
+        {
+          const size_t nb = static_cast<size_t>(js[k].n_blocks);
+          std::vector<double> evo(8 * nb);
+          std::vector<int64_t> bh(nb);
+          st = akmc_get_block_clocks(ctx, static_cast<int32_t>(k), evo.data(), bh.data(), js[k].n_blocks);
+          if (st != AKMC_OK) break;
+          uint64_t h = 0xCBF29CE484222325ull;
+          auto mix = [&h](const void* p, size_t n) {
+            const unsigned char* b = static_cast<const unsigned char*>(p);
+            for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001B3ull;
+          };
+          for (size_t b = 0; b < nb; ++b) {
+            mix(evo.data() + 8 * b, 8 * sizeof(double));
+            mix(&bh[b], sizeof(int64_t));
+          }
+          j->res.clocks_fnv = h;
+        }
+        auto tt = std::chrono::steady_clock::now();
+        st = akmc_retire_job(ctx, static_cast<int32_t>(k));
+        add_time(t_retire, tt);
+        add_time(t_build, tt);
+        publish(j, st == AKMC_OK ? AKMC_OK : st, ctx);
+        j = nullptr;
+        --live;
+      }
+      add_time(t_publish, tp);
+      if (st != AKMC_OK) {
+        for (auto& j : slots)
+          if (j) publish(j, st, ctx);
+        break;
+      }
     }
+    if (ctx) akmc_destroy(ctx);
   }
 };
 
@@ -311,8 +328,11 @@ AKMC_API akmc_status akmc_server_submit(akmc_server* s, const akmc_job_config* c
   if (!s || !cfg || !occ || !ticket) return AKMC_EINVAL;
   *ticket = 0;
   if (cfg->hop_budget <= 0 && cfg->max_rounds <= 0) return AKMC_EINVAL;  // the job would never end
-  for (int d = 0; d < 3; ++d)
+  for (int d = 0; d < 3; ++d) {
     if (cfg->box[d] < 8 || cfg->box[d] > (1 << 20)) return AKMC_EINVAL;
+    const int64_t nb = cfg->blocks[d] > 0 ? cfg->blocks[d] : 1;
+    if ((cfg->box[d] + nb - 1) / nb > kLaneBlockEdge) return AKMC_EINVAL;  // blocks larger than a lane takes
+  }
   if (n_sites != 2 * cfg->box[0] * cfg->box[1] * cfg->box[2]) return AKMC_EINVAL;
   if (cfg->energy_model == AKMC_MODEL_EAM && !cfg->eam) return AKMC_EINVAL;
   auto j = std::make_shared<SJob>();
@@ -385,10 +405,10 @@ AKMC_API akmc_status akmc_server_profile(akmc_server* s, double* seconds8, int64
   seconds8[1] = s->t_run;
   seconds8[2] = s->t_publish;
   seconds8[3] = s->t_wait;
-  seconds8[4] = s->t_add;
-  seconds8[5] = s->t_prepare;
-  seconds8[6] = s->t_restore;
-  seconds8[7] = s->t_save;
+  seconds8[4] = s->t_admit;
+  seconds8[5] = s->t_create;
+  seconds8[6] = s->t_retire;
+  seconds8[7] = 0.0;
   counts3[0] = s->n_chunks;
   counts3[1] = s->n_live;
   counts3[2] = s->n_builds;

@@ -130,6 +130,12 @@ class ContextConfig(C.Structure):
         ("event_log_capacity", C.c_int64),
         ("hop_cap_per_round", C.c_int64),
         ("flow_sweep_limit", C.c_int64),
+        ("max_jobs", C.c_int32),
+        ("max_block_edge", C.c_int32),
+        ("max_blocks", C.c_int64),
+        ("max_vacancies", C.c_int64),
+        ("eval_warps", C.c_int32),
+        ("flow_take", C.c_int32),
     ]
 
 
@@ -154,6 +160,7 @@ class JobResult(C.Structure):
         ("status", C.c_int32),
         ("n_blocks", C.c_int32),
         ("error", C.c_char * 128),
+        ("clocks_fnv", C.c_uint64),
     ]
 
 
@@ -206,6 +213,8 @@ SIGNATURES = {
     "akmc_destroy": (C.c_int, [_vp]),
     "akmc_add_job": (C.c_int, [_vp, C.POINTER(JobConfig), _vp, _i64, C.POINTER(_i32)]),
     "akmc_prepare": (C.c_int, [_vp]),
+    "akmc_admit_job": (C.c_int, [_vp, C.POINTER(JobConfig), _vp, _i64, C.POINTER(_i32)]),
+    "akmc_retire_job": (C.c_int, [_vp, _i32]),
     "akmc_run_rounds": (C.c_int, [_vp, _i64]),
     "akmc_run_rounds_noalloc": (C.c_int, [_vp, _i64]),
     "akmc_set_round_schedule": (C.c_int, [_vp, _i32]),
@@ -381,7 +390,11 @@ class Engine:
     """One akmc_ctx: a set of jobs advanced together on one GPU."""
 
     def __init__(self, device=0, stream=None, event_log_capacity=0, graph_rounds=32, hop_cap_per_round=0,
-                 flow_sweep_limit=0):
+                 flow_sweep_limit=0, max_jobs=0, max_block_edge=0, max_blocks=0, max_vacancies=0, eval_warps=0,
+                 flow_take=0):
+        """max_jobs > 0 leaves room for jobs admitted after prepare (admit_job): that many jobs,
+        max_blocks domain blocks and max_vacancies vacancies held at once, blocks of at most
+        max_block_edge cells."""
         cfg = ContextConfig()
         cfg.device = device
         cfg.graph_rounds = graph_rounds
@@ -389,6 +402,12 @@ class Engine:
         cfg.event_log_capacity = event_log_capacity
         cfg.hop_cap_per_round = hop_cap_per_round
         cfg.flow_sweep_limit = flow_sweep_limit
+        cfg.max_jobs = max_jobs
+        cfg.max_block_edge = max_block_edge
+        cfg.max_blocks = max_blocks
+        cfg.max_vacancies = max_vacancies
+        cfg.eval_warps = eval_warps
+        cfg.flow_take = flow_take
         h = C.c_void_p()
         _check(lib().akmc_create(C.byref(cfg), C.byref(h)))
         self.h = h
@@ -423,6 +442,21 @@ class Engine:
 
     def prepare(self):
         self._ck(lib().akmc_prepare(self.h))
+
+    def admit_job(self, cfg, occ):
+        """akmc_admit_job: a job added to the prepared, running context; returns its slot id."""
+        occ = np.ascontiguousarray(occ, np.uint8)
+        jid = C.c_int32(-1)
+        self._ck(lib().akmc_admit_job(self.h, C.byref(cfg), _ptr(occ), occ.size, C.byref(jid)))
+        while len(self.jobs) <= jid.value:
+            self.jobs.append(None)
+        self.jobs[jid.value] = (cfg, occ.size)
+        return jid.value
+
+    def retire_job(self, job):
+        """akmc_retire_job: frees the job's slots; its id may be given out again."""
+        self._ck(lib().akmc_retire_job(self.h, job))
+        self.jobs[job] = None
 
     def run_rounds(self, n):
         self._ck(lib().akmc_run_rounds(self.h, n))
@@ -517,7 +551,7 @@ class Engine:
 
     def occupancies(self, out=None):
         """akmc_get_occupancies: every job's lattice, back to back in job order (into `out`)."""
-        n = sum(j[1] for j in self.jobs)
+        n = sum(j[1] for j in self.jobs if j is not None)
         if out is None:
             out = np.empty(n, np.uint8)
         elif out.dtype != np.uint8 or out.size != n or not out.flags["C_CONTIGUOUS"]:
@@ -593,11 +627,23 @@ class Engine:
 
 def _result(r):
     return dict(hops=r.hops, rounds=r.rounds, submit_s=r.submit_s, start_s=r.start_s, finish_s=r.finish_s,
-                status=r.status, n_blocks=r.n_blocks, error=r.error.decode(errors="replace"))
+                status=r.status, n_blocks=r.n_blocks, error=r.error.decode(errors="replace"),
+                clocks_fnv=r.clocks_fnv)
+
+
+def clocks_fnv(evo, hops):
+    """The job result's clocks_fnv of block clocks evo[nblocks][8] (FP64) and hops[nblocks]."""
+    h = 0xCBF29CE484222325
+    for b in range(len(hops)):
+        data = np.ascontiguousarray(evo[b], np.float64).tobytes() + np.int64(hops[b]).tobytes()
+        for x in data:
+            h = ((h ^ x) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
 
 
 class Server:
-    """akmc_server: queued jobs run in batches by worker lanes, results as each job ends."""
+    """akmc_server: queued jobs admitted into the lanes' running contexts as room frees up,
+    results as each job ends."""
 
     def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0, order=0):
         cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds, order)
@@ -634,12 +680,12 @@ class Server:
         return _result(r), out
 
     def profile(self):
-        """akmc_server_profile: lane seconds (build, run, publish, wait) and counts."""
+        """akmc_server_profile: lane seconds (job-set changes, run, publish, wait) and counts."""
         t = np.zeros(8, np.float64)
         c = np.zeros(3, np.int64)
         _check(lib().akmc_server_profile(self.h, _ptr(t), _ptr(c)))
         return dict(build_s=float(t[0]), run_s=float(t[1]), publish_s=float(t[2]), wait_s=float(t[3]),
-                    add_s=float(t[4]), prepare_s=float(t[5]), restore_s=float(t[6]), save_s=float(t[7]),
+                    admit_s=float(t[4]), create_s=float(t[5]), retire_s=float(t[6]),
                     chunks=int(c[0]), mean_batch=float(c[1]) / max(1, int(c[0])), builds=int(c[2]))
 
     def stats(self):

@@ -188,6 +188,46 @@ def test_hop_budgets_under_both_schedules(ak, schedule):
         assert eng.job_state(1)["round"] == 93
 
 
+def test_single_block_budget_jobs_under_flow(ak):
+    # single-block jobs run their rounds back to back in one CTA under the dependency-driven
+    # schedule, and the kernel itself stops each at the first time-step boundary at which its
+    # hops reached its budget; a multi-block job without budget shares the launches.  Each job
+    # must equal the oracle, budgets and rounds alike, over calls that end between boundaries.
+    kws = [dict(box=(16, 16, 16), model=po.MODEL_EAM, precision=po.FP32C, alloy=QUATERNARY, n_vacancies=4,
+                temperature=600.0, seed=41),
+           dict(box=(20, 20, 20), model=po.MODEL_EAM, n_vacancies=6, seed=42),
+           dict(box=(18, 17, 16), model=po.MODEL_PAIRBOND, alloy=QUATERNARY, n_vacancies=5, seed=43),
+           dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=40,
+                temperature=563.0, seed=44)]
+    budgets = [300, 700, 150, 0]
+    calls = (37, 100, 63, 5)
+    with ak.Engine(event_log_capacity=1 << 20) as eng:
+        eng.set_round_schedule(ak.SCHEDULE_FLOW)
+        oracles = [oracle_job(**kw) for kw in kws]
+        for kw, o, b in zip(kws, oracles, budgets):
+            dkw = {key: kw[key] for key in ("box", "blocks", "model", "precision", "seed", "temperature") if key in kw}
+            device_job(eng, o, hop_budget=b, **dkw)
+        eng.prepare()
+        assert eng.round_schedule() == ak.SCHEDULE_FLOW
+        for n in calls:
+            eng.run_rounds(n)
+        eng.sync()
+        total = sum(calls)
+        for o, b in zip(oracles, budgets):
+            if b:
+                o.run(b, total)
+            else:
+                o.run_rounds(total)
+        ev = eng.events()
+        for k, (o, b) in enumerate(zip(oracles, budgets)):
+            check_job(eng, o, k, ev)
+            st = eng.job_state(k)
+            if b:
+                assert st["done"] and st["round"] % 8 == 0 and st["hops"] >= b and st["round"] < total, st
+            else:
+                assert st["round"] == total
+
+
 def test_schedule_switch_between_calls(ak):
     # the job server switches a context between the two schedules from one chunk to the next:
     # the trajectory must not notice.  A budget job (it stops at a time-step boundary inside the
