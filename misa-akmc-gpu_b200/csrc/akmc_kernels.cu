@@ -75,9 +75,11 @@ struct Region {
 
 // The staged region of a block's sector: the sector and a 2-cell halo.  Rows are staged
 // whole by the bulk-copy unit when the job allows it (J.bulk: rows of a multiple of 16 sites,
-// 16-byte aligned arrays, shared memory sized for the wider rows) and the region does not
-// wrap in x: each row is rounded out to 16-site boundaries, so every copy starts on a 16-byte
-// boundary of its lattice row and ends inside it.
+// 16-byte aligned arrays, shared memory sized for the wider rows): each row's span is rounded
+// out to 16-site boundaries from its unwrapped origin R.ox (which may lie before the row or run
+// past its end: the sector never wraps, its halo may), so every copy starts on a 16-byte
+// boundary.  A span that crosses the row's end (or starts before it) is copied as two pieces,
+// each inside the row; the span must not be longer than the row.
 __device__ __forceinline__ void make_region(const BlockDev& B, const JobDev& J, int sec, Region& R) {
   for (int d = 0; d < 3; ++d) {
     const int half = (B.c1[d] - B.c0[d]) / 2;
@@ -99,14 +101,18 @@ __device__ __forceinline__ void make_region(const BlockDev& B, const JobDev& J, 
   R.xo = 0;
   R.bulk = 0;
   R.bo = R.br = 0;
-  if (J.bulk && R.ox >= 0 && R.ox + R.LX <= J.sx) {
-    const int x0 = R.ox & ~15;
-    R.xo = R.ox - x0;
-    R.ox = x0;
-    R.LX = (R.LXt + 14 + 15) & ~15;  // one pitch for every alignment: tables stay valid
-    R.bo = (R.xo + R.LXt + 15) & ~15;
-    R.br = (R.xo + R.LXt + 3) & ~3;
-    R.bulk = 1;
+  if (J.bulk) {
+    const int x0 = R.ox & ~15;  // rounds down, negative origins included
+    const int xo = R.ox - x0;
+    const int bo = (xo + R.LXt + 15) & ~15;
+    if (bo <= J.sx) {
+      R.xo = xo;
+      R.ox = x0;
+      R.LX = (R.LXt + 14 + 15) & ~15;  // one pitch for every alignment: tables stay valid
+      R.bo = bo;
+      R.br = (xo + R.LXt + 3) & ~3;
+      R.bulk = 1;
+    }
   }
   R.hx = R.slo[0] - R.ox / 2;
   R.n = R.LX * R.LY * R.LZ;
@@ -127,12 +133,16 @@ struct Smem {
   int32_t d2[6];
   int32_t jl[2][8][kJumpN];     // int16 local offset | (s*8+t) << 16
   int32_t rl[2][8][kRefreshN];  // packed (dx, dy, dz) | (s*8+t) << 24
-  int32_t vidx[kMaxV], vloc[kMaxV], vlid[kMaxV], ord[kMaxV];
-  int16_t vcx[kMaxV], vcy[kMaxV], vcz[kMaxV];  // local coordinates (x in doubled sites)
-  int32_t vgx[kMaxV], vgy[kMaxV], vgz[kMaxV];  // global coordinates
-  uint8_t vact[kMaxV];          // vacancy still inside the active sector
-  uint8_t vavb[kMaxV][8];       // jump b of vacancy k available (target is an atom)
-  double rates[kMaxV][8];
+  int32_t vidx[kMaxV];          // vacancy table index of record k
+  // Vacancy records in two sets: a hop selected from set c writes set c ^ 1 (see run_block).
+  int32_t vloc[2][kMaxV], vlid[2][kMaxV];               // local site, global site id
+  int16_t vcx[2][kMaxV], vcy[2][kMaxV], vcz[2][kMaxV];  // local coordinates (x in doubled sites)
+  int32_t vgx[2][kMaxV], vgy[2][kMaxV], vgz[2][kMaxV];  // global coordinates
+  uint8_t vact[2][kMaxV];       // vacancy still inside the active sector
+  int32_t ord[2][kMaxV];        // the active vacancies in z-y-x order (ascending site id)
+  int32_t nord[2];
+  uint8_t vX[2][kMaxV][8];      // code of jump b's target atom (0: the target is a vacancy)
+  double rates[2][kMaxV][8];
   // F-table window, two planes: FP64 (c0, c1) x kFWin then (c2, c3) x kFWin;
   // FP32 (hi, lo, c1, c2) x kFWin then c3 x kFWin
   alignas(16) unsigned char fwin[kFWin * 32];
@@ -141,12 +151,12 @@ struct Smem {
   uint32_t mbar_phase, mbst_phase;
   int32_t win_pot;                             // potential (and precision) the window holds
   int32_t tab_key[2];                          // potential, kind and region strides the tables hold
-  // hop-loop control, written by thread 0 between barriers
-  double pre[kMaxV * 8];   // running sums of the ordered rates
-  double ctl_u, ctl_unext, ctl_expected;
-  int32_t ctl_from, ctl_to;
-  int32_t ctl_ksel, ctl_bsel, ctl_stop, ctl_ok, ctl_s, ctl_X, ctl_next_stop, ctl_hop, ctl_n8;
-  int32_t ctl_gx, ctl_gy, ctl_gz, ctl_qx, ctl_qy, ctl_qz, ctl_pos;
+  // hop-loop control, written by the control thread, in slots of the iteration parity
+  double ctl_u[2];         // the selection's uniform, drawn ahead
+  int32_t ctl_stop[2];     // the sector's window is reached (or the hop cap): no more selections
+  uint64_t xsn[2][4];      // selection stream after the uniform drawn ahead
+  int32_t ctl_ok;          // the region's copies arrived
+  int32_t fin;             // record set that holds the block's vacancies after run_block
   uint64_t xs[4], xt[4];  // the block's selection / residence-time streams while it runs
   // asynchronous schedule (k_flow)
   int8_t flow_lag[8][27];
@@ -158,7 +168,6 @@ struct Smem {
   unsigned long long acc[6];  // counters 0 (hops), 1, 3, 4, 5, 6
   int32_t acc_job;
   unsigned long long acc_job_hops;
-  uint64_t xsn[4];        // selection stream after the uniform drawn ahead
 };
 
 // --- bulk copy global -> shared with an mbarrier (cp.async.bulk, TMA unit) -----------
@@ -329,19 +338,19 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
   return c;
 }
 
-// Rates of vacancy k, all 8 jumps, CTA-collective (no barrier inside; the caller
-// synchronises before the rates are read).  Warp b evaluates jump b.
+// Rates of vacancy k of record set `set`, all 8 jumps, CTA-collective (no barrier inside; the
+// caller synchronises before the rates are read).  Warp b evaluates jump b.
 //  pair-bond: lanes 0..3 run the four bond counts of VacRatesSolver::deltaE
 //             (vacancy_rates_solver.cpp:45-116), each summed in the reference order;
 //  EAM:       lane q sums sites i = q, q+32, q+64 of the jump's list; the 32 partials
 //             merge by a xor butterfly (16, 8, 4, 2, 1), then the moving atom's own
 //             embedding change is added.
 template <int KIND>
-__device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_s, int k, int b, const FTab& FT,
-                             const JobC& jc, const int32_t (&jr)[2][3], double* de_out) {
+__device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int32_t* rho_s, int k, int b,
+                             const FTab& FT, const JobC& jc, const int32_t (&jr)[2][3], double* de_out) {
   const int lane = threadIdx.x & 31;
   const int q = lane;
-  const int l = sm.vloc[k];
+  const int l = sm.vloc[set][k];
   const int p = l & 1;
   const int tl = l + sm.d1[p][b];
   const uint8_t Xc = occ_s[tl];
@@ -443,8 +452,8 @@ __device__ void eval_vacancy(Smem& sm, const uint8_t* occ_s, const int32_t* rho_
     }
   }
   if (q == 0) {
-    sm.rates[k][b] = avail ? arrhenius(jc.nu, jc.kT, Xc, dE) : 0.0;
-    sm.vavb[k][b] = avail ? 1 : 0;
+    sm.rates[set][k][b] = avail ? arrhenius(jc.nu, jc.kT, Xc, dE) : 0.0;
+    sm.vX[set][k][b] = avail ? Xc : 0;
     if (de_out) de_out[k * 8 + b] = avail ? dE : 0.0;  // akmc_calculate only
   }
   if (KIND == kEam64) EVAL_T(3);
@@ -611,14 +620,27 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
   } else {
     // the bulk-copy unit moves whole rows: R.bo occupancy bytes and R.br densities from the
-    // row's 16-site boundary R.ox, into shared rows of pitch R.LX; thread t issues row t
+    // row's 16-site boundary R.ox (unwrapped), into shared rows of pitch R.LX; thread t issues
+    // row t.  A span that leaves the row [0, sx) at either end goes in two pieces: sites
+    // [R.ox, cut) to shared [0, cut - R.ox) and the rest from the other end of the row.
     asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
+    const int sx = jc.sx;
     for (int row = tid; row < nrows; row += kThreads) {
       const int ly = row % R.LY, lz = row / R.LY;
       const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
-      const int64_t base = static_cast<int64_t>(jc.sx) * (gy + static_cast<int64_t>(jc.sy) * gz) + R.ox;
-      bulk_copy(occ_s + R.LX * row, jc.occ + base, static_cast<uint32_t>(R.bo), &sm.mbar_st);
-      if (eam) bulk_copy(rho_s + R.LX * row, jc.rho + base, 4u * static_cast<uint32_t>(R.br), &sm.mbar_st);
+      const int64_t rb = static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(jc.sy) * gz);
+#pragma unroll
+      for (int arr = 0; arr < 2; ++arr) {
+        if (arr == 1 && !eam) break;
+        const int len = arr == 0 ? R.bo : R.br;  // sites of the span
+        const int es = arr == 0 ? 1 : 4;          // bytes per site
+        uint8_t* dst = arr == 0 ? occ_s + R.LX * row : reinterpret_cast<uint8_t*>(rho_s + R.LX * row);
+        const uint8_t* src = arr == 0 ? jc.occ + rb : reinterpret_cast<const uint8_t*>(jc.rho + rb);
+        const int n1 = R.ox < 0 ? -R.ox : min(len, sx - R.ox);  // sites up to the row's end
+        const int a1 = R.ox < 0 ? R.ox + sx : R.ox;              // row position of the first piece
+        bulk_copy(dst, src + static_cast<int64_t>(es) * a1, static_cast<uint32_t>(es * n1), &sm.mbar_st);
+        if (len > n1) bulk_copy(dst + es * n1, src, static_cast<uint32_t>(es * (len - n1)), &sm.mbar_st);
+      }
     }
   }
   AKMC_STAGE_T(2);
@@ -632,15 +654,15 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     const int z = t / jc.sy;
     const int lx = X - R.ox, ly = y - R.oy, lz = z - R.oz;
     sm.vidx[tid] = v;
-    sm.vloc[tid] = lx + R.LX * (ly + R.LY * lz);
-    sm.vlid[tid] = s;
-    sm.vcx[tid] = static_cast<int16_t>(lx);
-    sm.vcy[tid] = static_cast<int16_t>(ly);
-    sm.vcz[tid] = static_cast<int16_t>(lz);
-    sm.vgx[tid] = X;
-    sm.vgy[tid] = y;
-    sm.vgz[tid] = z;
-    sm.vact[tid] = 1;
+    sm.vloc[0][tid] = lx + R.LX * (ly + R.LY * lz);
+    sm.vlid[0][tid] = s;
+    sm.vcx[0][tid] = static_cast<int16_t>(lx);
+    sm.vcy[0][tid] = static_cast<int16_t>(ly);
+    sm.vcz[0][tid] = static_cast<int16_t>(lz);
+    sm.vgx[0][tid] = X;
+    sm.vgy[0][tid] = y;
+    sm.vgz[0][tid] = z;
+    sm.vact[0][tid] = 1;
   }
   __syncthreads();
   AKMC_STAGE_T(3);
@@ -649,19 +671,25 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     // z-y-x scan order of ABVIModel::calcRates = ascending site id inside a sector
     for (int i = 0; i < cnt; ++i) {
       int j = i;
-      while (j > 0 && sm.vlid[sm.ord[j - 1]] > sm.vlid[i]) {
-        sm.ord[j] = sm.ord[j - 1];
+      while (j > 0 && sm.vlid[0][sm.ord[0][j - 1]] > sm.vlid[0][i]) {
+        sm.ord[0][j] = sm.ord[0][j - 1];
         --j;
       }
-      sm.ord[j] = i;
+      sm.ord[0][j] = i;
     }
+    sm.nord[0] = cnt;
+    uint64_t x[4];
     for (int i = 0; i < 4; ++i) {
-      sm.xs[i] = __ldcg(&B.xs[i]);
+      x[i] = __ldcg(&B.xs[i]);
+      sm.xs[i] = x[i];
       sm.xt[i] = __ldcg(&B.xt[i]);
     }
-    sm.ctl_next_stop = 0;
-    sm.ctl_hop = 0;
+    // the first selection's uniform, drawn ahead; the stream moves on only if a selection uses it
+    sm.ctl_u[0] = a.mode == kModeRound ? uniform_co(x) : 0.0;
+    for (int i = 0; i < 4; ++i) sm.xsn[0][i] = x[i];
+    sm.ctl_stop[0] = 0;
     sm.ctl_ok = 1;
+    sm.fin = 0;
     if (need_win) {
       if (mbar_wait(&sm.mbar, sm.mbar_phase)) {
         sm.mbar_phase ^= 1u;
@@ -698,299 +726,284 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       jr[jj][0][u] = in ? sm.jl[0][b][i] : 0;
       jr[jj][1][u] = in ? sm.jl[1][b][i] : 0;
     }
+  double* const de_out = a.mode == kModeCalc ? a.api_de : nullptr;
+  const int D = eam ? 4 : 3;  // a hop changes the rates of vacancies within D cells of its origin
 
-  // The 78 exact density deltas of the hop just performed (ABVIModel::perform's lattice
-  // change seen by the density cache), in shared memory and through to global memory.
-  auto refresh = [&](int i) {
-    const int s = sm.ctl_s, bsel = sm.ctl_bsel;
-    const int p = s & 1;
-    const int X = species_index(static_cast<uint8_t>(sm.ctl_X));
-    const int32_t e = sm.rl[p][bsel][i];
-    const int j = s + local_delta(e, R);
-    const int32_t v = rho_s[j] + sm.dfq[X * 64 + rshells(e)];
-    rho_s[j] = v;
-    const int gx = wrap1(sm.ctl_gx + unpack_dx(e), jc.sx), gy = wrap1(sm.ctl_gy + unpack_dy(e), jc.sy),
-              gz = wrap1(sm.ctl_gz + unpack_dz(e), jc.sz);
-    jc.rho[gx + jc.sx * (gy + jc.sy * gz)] = v;  // site ids fit in int32 (checked at akmc_add_job)
-  };
+  // first evaluation: every vacancy of the sector, into record set 0
+  if (evaluator) {
+    for (int k = 0; k < cnt; ++k) {
+#pragma unroll
+      for (int jj = 0; jj < kJumpsPerWarp; ++jj)
+        eval_vacancy<KIND>(sm, 0, occ_s, rho_s, k, warp + kEvalWarps * jj, FT, jc, jr[jj], de_out);
+    }
+  }
+  __syncthreads();
+  AKMC_PHASE(2);
 
-  // Hop loop, two CTA barriers per hop:
-  //  (E) the evaluator warps refresh the densities of the hop just performed, then evaluate the
-  //      vacancies it made dirty; the control warp counts them, moves the hopped vacancy
-  //      in the ordered list, runs the clock of the hop, decides whether the sector is
-  //      done and draws the next selection uniform ahead of time;
-  //  (S) the control warp forms the ordered total, selects the next hop and performs it
-  //      on the occupancy and the vacancy record.
-  // Clock and counters live in the control thread's registers.
+  // Hop loop, one CTA barrier per hop.  The vacancy records, the ordered list, the rates and the
+  // jump targets come in two sets: a hop selected from set c writes set n = c ^ 1, which the next
+  // hop reads, so no write of a hop meets a read of the same hop.  Every warp selects for itself
+  // (the ordered sum and the scan are deterministic: every warp finds the same hop), then:
+  //  - the evaluator warps perform it (occupancy swap, the 78 density deltas, set n), meet at a
+  //    named barrier, and evaluate the vacancies the hop made dirty into set n;
+  //  - the control warp runs the hop's clock, writes its event, decides whether the sector's
+  //    window is reached and draws the next selection's uniform, into the control slots of the
+  //    next iteration (indexed by iteration parity).
+  // A selection that finds no jump (u * total reached no running sum) advances the clock only and
+  // keeps set c.
   const int64_t hop0 = __ldcg(&B.hops);
   int64_t nh = 0, nact_sum = 0, evals = cnt;
-  int nord = cnt, nact_last = 0;
-  double sector_time = 0.0, total_last = 0.0;
-  bool clock_due = false;  // a selection with a positive total happened since the last clock
-  const int D = eam ? 4 : 3;
-  bool first = true;
-  double* const de_out = a.mode == kModeCalc ? a.api_de : nullptr;
-  // vacancies to evaluate: all active ones on the first pass, then those within D cells
-  // of the last hop's origin (every warp derives the same set)
-  auto dirty_mask = [&](int base) -> unsigned {
-    const int k = base + lane;
-    bool d = false;
-    if (k < cnt && sm.vact[k]) {
-      d = first || (abs((sm.vcx[k] >> 1) - sm.ctl_qx) <= D && abs(sm.vcy[k] - sm.ctl_qy) <= D &&
-                    abs(sm.vcz[k] - sm.ctl_qz) <= D);
-    }
-    return __ballot_sync(kFull, d);
+  double sector_time = 0.0;
+  int c = 0;   // record set of the current selection
+  int it = 0;  // iteration parity: control slots
+  // vacancy k of record set `set` lies within D cells of the cell (qx, qy, qz) and in the sector
+  auto dirty = [&](int set, int k, int qx, int qy, int qz) -> bool {
+    return sm.vact[set][k] && abs((sm.vcx[set][k] >> 1) - qx) <= D && abs(sm.vcy[set][k] - qy) <= D &&
+           abs(sm.vcz[set][k] - qz) <= D;
   };
   while (true) {
-    const bool hopped = !first && sm.ctl_hop;
-    if (evaluator) {
-      if (eam && hopped) {
-        if (tid < kRefreshN) refresh(tid);
-        asm volatile("bar.sync 1, %0;" ::"n"(kCtl) : "memory");  // the evaluator warps only
-      }
-      if (first || hopped) {
-        for (int base = 0; base < cnt; base += 32) {
-          unsigned m = dirty_mask(base);
-          while (m) {
-            const int k = base + __ffs(m) - 1;
-            m &= m - 1;
+    if (sm.ctl_stop[it]) break;
+    const int n = c ^ 1;
+    const int nord = sm.nord[c];
+    // [1] selection: lane 0 of every warp forms the ordered total (ABVIModel::calcRates,
+    // kmc.cpp:68-115), then runs the same running sums again to the first one above u * total
+    // (ABVIModel::select, kmc.cpp:242-309).  Jumps onto a vacancy hold 0.0, which leaves a
+    // positive sum unchanged.
+    int isel = -1, stop = 0;
+    double total = 0.0, u = 0.0;
+    if (lane == 0) {
+      for (int i = 0; i < nord; ++i) {
+        const double* r = sm.rates[c][sm.ord[c][i]];
 #pragma unroll
-            for (int jj = 0; jj < kJumpsPerWarp; ++jj)
-              eval_vacancy<KIND>(sm, occ_s, rho_s, k, warp + kEvalWarps * jj, FT, jc, jr[jj], de_out);
-          }
-        }
+        for (int bb = 0; bb < 8; ++bb) total += r[bb];
       }
-    } else {  // control warp
-      int nd = 0;
-      if (hopped)
-        for (int base = 0; base < cnt; base += 32) nd += __popc(dirty_mask(base));
-      if (lane == 0) {
-        if (hopped) {
-          // the hopped vacancy leaves its place in the ordered list and re-enters at its
-          // new site id if it is still inside the sector
-          const int ksel = sm.ctl_ksel;
-          for (int i = sm.ctl_pos; i + 1 < nord; ++i) sm.ord[i] = sm.ord[i + 1];
-          --nord;
-          if (sm.vact[ksel]) {
-            const int32_t key = sm.vlid[ksel];
-            int j = nord;
-            while (j > 0 && sm.vlid[sm.ord[j - 1]] > key) {
-              sm.ord[j] = sm.ord[j - 1];
-              --j;
-            }
-            sm.ord[j] = ksel;
-            ++nord;
-          }
-          evals += nd;
-          nact_sum += nact_last;
-          ++nh;
-        }
-        if (clock_due) {
-          clock_due = false;
-          int stop = 0;
-          const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
-          const double dt = -port_log(u2) / total_last;
-          sector_time += dt;
-          if (hopped && a.log_cap > 0) {
-            const unsigned long long slot = atomicAdd(a.log_count, 1ull);
-            if (slot < static_cast<unsigned long long>(a.log_cap)) {
-              akmc_event* e = a.log + slot;
-              e->round = round_now;
-              e->hop = hop0 + nh - 1;
-              e->from_site = sm.ctl_from;
-              e->to_site = sm.ctl_to;
-              e->block = B.local_id;
-              e->species = sm.ctl_X;
-              e->u = sm.ctl_u;
-              e->total = total_last;
-              e->dt = dt;
-              e->n_act = nact_last;
-              e->n_dirty = nd;
-              e->job = B.job;
-              e->reserved = 0;
-            } else {
-              atomicOr(a.status, kErrLogOverflow);
+      if (a.mode == kModeCalc) {
+        stop = 1;
+      } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
+        stop = 2;
+      } else {
+        u = a.mode == kModeSelectPerform ? a.api_u : sm.ctl_u[it];
+        const double expected = u * total;  // ModelAdapter::selectAndPerform
+        double acc = 0.0;
+        for (int i = 0; i < nord && isel < 0; ++i) {
+          const double* r = sm.rates[c][sm.ord[c][i]];
+          for (int bb = 0; bb < 8; ++bb) {
+            acc += r[bb];
+            if (acc > expected) {
+              isel = i * 8 + bb;
+              break;
             }
           }
-          if (!(sector_time < thr)) stop = 1;
-          if (nh >= a.hop_cap) {
-            atomicOr(a.status, kErrHopCap);
-            stop = 1;
-          }
-          sm.ctl_next_stop = stop;
-        }
-        if (a.mode == kModeRound && !sm.ctl_next_stop) {
-          // the next selection's uniform, committed only if a selection consumes it
-          uint64_t x[4] = {sm.xs[0], sm.xs[1], sm.xs[2], sm.xs[3]};
-          sm.ctl_unext = uniform_co(x);
-          for (int i = 0; i < 4; ++i) sm.xsn[i] = x[i];
         }
       }
     }
-    __syncthreads();  // (E) rates, list and the clock decision visible
-    AKMC_PHASE(first ? 2 : 5);
-    first = false;
-    if (sm.ctl_next_stop) break;
-    if (warp == kEvalWarps) {
-      if (lane == 0) {
-        // ordered total; the running sums are kept: they are the selection scan's
-        // accumulator values (ABVIModel::select, kmc.cpp:242-309) in the same order.
-        // Unavailable jumps hold 0.0, and adding 0.0 leaves a positive sum unchanged.
-        double total = 0.0;
-        int n8 = 0;
-        for (int i = 0; i < nord; ++i) {
-          const double* r = sm.rates[sm.ord[i]];
-#pragma unroll
-          for (int bb = 0; bb < 8; ++bb) {
-            total += r[bb];
-            sm.pre[n8 + bb] = total;
-          }
-          n8 += 8;
-        }
-        int stop = 0;
-        double u = 0.0, expected = 0.0;
-        if (a.mode == kModeCalc) {
+    isel = __shfl_sync(kFull, isel, 0);
+    stop = __shfl_sync(kFull, stop, 0);
+    if (stop) {
+      if (tid == kCtl) {
+        if (stop == 1) {  // akmc_calculate: the sector's vacancies with their jump rates
           *a.api_total = total;
-          // the sector's vacancies with their jump rates (ΔE is written by the evaluators)
           for (int i = 0; i < cnt; ++i) {
-            a.api_sites[i] = sm.vact[i] ? sm.vlid[i] : -1;
-            for (int bb = 0; bb < 8; ++bb) a.api_rates[i * 8 + bb] = sm.rates[i][bb];
+            a.api_sites[i] = sm.vact[c][i] ? sm.vlid[c][i] : -1;
+            for (int bb = 0; bb < 8; ++bb) a.api_rates[i * 8 + bb] = sm.rates[c][i][bb];
           }
           *a.api_count = cnt;
-          stop = 1;
-        } else if (total == 0.0 || fabs(total) < DBL_EPSILON) {  // sublattice.inl:108-112
+        } else {
           if (a.mode == kModeSelectPerform) {
             a.api_event->from_site = -1;
             a.api_event->total = total;
           }
           sector_time = thr;
-          stop = 1;
-        } else {
-          if (a.mode == kModeSelectPerform) {
-            u = a.api_u;
-          } else {
-            u = sm.ctl_unext;
-            for (int i = 0; i < 4; ++i) sm.xs[i] = sm.xsn[i];
-          }
-          expected = u * total;  // ModelAdapter::selectAndPerform
-          clock_due = a.mode == kModeRound;
-          total_last = total;
-          nact_last = nord;
         }
-        sm.ctl_u = u;
-        sm.ctl_expected = expected;
-        sm.ctl_n8 = stop ? 0 : n8;
-        sm.ctl_stop = stop;
       }
-      __syncwarp();
-      // first running sum above u * total, 32 entries per step
-      const int n8 = sm.ctl_n8;
-      const double expected = sm.ctl_expected;
-      int isel = -1;
-      for (int base = 0; base < n8 && isel < 0; base += 32) {
-        const int i = base + lane;
-        const unsigned m = __ballot_sync(kFull, i < n8 && sm.pre[i] > expected);
-        if (m) isel = base + __ffs(m) - 1;
+      break;
+    }
+    // the selected jump: vacancy ksel of set c, direction bsel, atom X
+    const bool hop = isel >= 0;
+    const int ksel = hop ? sm.ord[c][isel >> 3] : 0, bsel = hop ? (isel & 7) : 0;
+    const int s = sm.vloc[c][ksel];
+    const int p = s & 1;
+    const int X = hop ? sm.vX[c][ksel][bsel] : 0;
+    const int32_t wg = sm.w1[p][bsel];
+    const int qx = sm.vcx[c][ksel] >> 1, qy = sm.vcy[c][ksel], qz = sm.vcz[c][ksel];
+    const int nlx = sm.vcx[c][ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
+    const bool nact = (nlx >> 1) >= R.hx && (nlx >> 1) < R.hx + R.w[0] && nly >= 2 && nly < 2 + R.w[1] &&
+                      nlz >= 2 && nlz < 2 + R.w[2];
+    const int sX = sm.vgx[c][ksel], sY = sm.vgy[c][ksel], sZ = sm.vgz[c][ksel];
+    const int ngx = wrap1(sX + unpack_dx(wg), jc.sx), ngy = wrap1(sY + unpack_dy(wg), jc.sy),
+              ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
+    const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
+    if (evaluator) {
+      if (hop) {
+        // [2] perform (ABVIModel::perform, kmc.cpp:358-396) on the staged region, written
+        // through, and set n: items 0..77 the density deltas, 78 the occupancy swap, 79 the
+        // ordered list, then one record and 8 rates per vacancy
+        const int nitems = kRefreshN + 2 + 9 * cnt;
+        for (int i = tid; i < nitems; i += kCtl) {
+          if (i < kRefreshN) {
+            if (eam) {
+              const int32_t e = sm.rl[p][bsel][i];
+              const int j = s + local_delta(e, R);
+              const int32_t v = rho_s[j] + sm.dfq[species_index(static_cast<uint8_t>(X)) * 64 + rshells(e)];
+              rho_s[j] = v;
+              const int gx = wrap1(sX + unpack_dx(e), jc.sx), gy = wrap1(sY + unpack_dy(e), jc.sy),
+                        gz = wrap1(sZ + unpack_dz(e), jc.sz);
+              jc.rho[gx + jc.sx * (gy + jc.sy * gz)] = v;  // site ids fit in int32 (checked at akmc_add_job)
+            }
+          } else if (i == kRefreshN) {
+            occ_s[s + sm.d1[p][bsel]] = kV;
+            occ_s[s] = static_cast<uint8_t>(X);
+            jc.occ[to_g] = kV;
+            jc.occ[sm.vlid[c][ksel]] = static_cast<uint8_t>(X);
+          } else if (i == kRefreshN + 1) {
+            // the hopped vacancy leaves its place in the ordered list and re-enters at its new
+            // site id if it is still inside the sector
+            const int pos = isel >> 3;
+            int m = 0;
+            for (int q = 0; q < nord; ++q)
+              if (q != pos) sm.ord[n][m++] = sm.ord[c][q];
+            if (nact) {
+              int j = m;
+              while (j > 0 && sm.vlid[c][sm.ord[n][j - 1]] > to_g) {
+                sm.ord[n][j] = sm.ord[n][j - 1];
+                --j;
+              }
+              sm.ord[n][j] = ksel;
+              ++m;
+            }
+            sm.nord[n] = m;
+          } else if (i < kRefreshN + 2 + cnt) {
+            const int k = i - kRefreshN - 2;
+            if (k == ksel) {
+              sm.vloc[n][k] = s + sm.d1[p][bsel];
+              sm.vlid[n][k] = to_g;
+              sm.vcx[n][k] = static_cast<int16_t>(nlx);
+              sm.vcy[n][k] = static_cast<int16_t>(nly);
+              sm.vcz[n][k] = static_cast<int16_t>(nlz);
+              sm.vgx[n][k] = ngx;
+              sm.vgy[n][k] = ngy;
+              sm.vgz[n][k] = ngz;
+              sm.vact[n][k] = nact ? 1 : 0;
+            } else {
+              sm.vloc[n][k] = sm.vloc[c][k];
+              sm.vlid[n][k] = sm.vlid[c][k];
+              sm.vcx[n][k] = sm.vcx[c][k];
+              sm.vcy[n][k] = sm.vcy[c][k];
+              sm.vcz[n][k] = sm.vcz[c][k];
+              sm.vgx[n][k] = sm.vgx[c][k];
+              sm.vgy[n][k] = sm.vgy[c][k];
+              sm.vgz[n][k] = sm.vgz[c][k];
+              sm.vact[n][k] = sm.vact[c][k];
+            }
+          } else {
+            // rates of vacancy q / 8, jump q % 8 carried over; the dirty ones are overwritten below
+            const int q = i - kRefreshN - 2 - cnt;
+            (&sm.rates[n][0][0])[q] = (&sm.rates[c][0][0])[q];
+            (&sm.vX[n][0][0])[q] = (&sm.vX[c][0][0])[q];
+          }
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(kCtl) : "memory");  // the evaluator warps only
+        // [3] + [4] the vacancies within D cells of the hop's origin, evaluated into set n
+        for (int base = 0; base < cnt; base += 32) {
+          const int k = base + lane;
+          unsigned m = __ballot_sync(kFull, k < cnt && dirty(n, k, qx, qy, qz));
+          while (m) {
+            const int kk = base + __ffs(m) - 1;
+            m &= m - 1;
+#pragma unroll
+            for (int jj = 0; jj < kJumpsPerWarp; ++jj)
+              eval_vacancy<KIND>(sm, n, occ_s, rho_s, kk, warp + kEvalWarps * jj, FT, jc, jr[jj], nullptr);
+          }
+        }
+      }
+    } else {  // control warp: the hop's clock and event, the next iteration's decision and uniform
+      int nd = 0;
+      if (hop) {
+        // the dirty count, from set c with the hopped vacancy at its new cell
+        for (int base = 0; base < cnt; base += 32) {
+          const int k = base + lane;
+          const bool d = k < cnt && (k == ksel ? nact : dirty(c, k, qx, qy, qz));
+          nd += __popc(__ballot_sync(kFull, d));
+        }
       }
       if (lane == 0) {
-        sm.ctl_hop = isel >= 0;
-        if (isel >= 0) {
-          // ABVIModel::perform (kmc.cpp:358-396) on the staged region, written through
-          const int ksel = sm.ord[isel >> 3], bsel = isel & 7;
-          const int s = sm.vloc[ksel];
-          const int p = s & 1;
-          const int tl = s + sm.d1[p][bsel];
-          const uint8_t Xc = occ_s[tl];
-          const int32_t wg = sm.w1[p][bsel];
-          const int sX = sm.vgx[ksel], sY = sm.vgy[ksel], sZ = sm.vgz[ksel];
-          const int ngx = wrap1(sX + unpack_dx(wg), jc.sx), ngy = wrap1(sY + unpack_dy(wg), jc.sy),
-                    ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
-          const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
-          const int32_t from_g = sm.vlid[ksel];
-          occ_s[tl] = kV;
-          occ_s[s] = Xc;
-          jc.occ[to_g] = kV;
-          jc.occ[from_g] = Xc;
-          sm.ctl_ksel = ksel;
-          sm.ctl_bsel = bsel;
-          sm.ctl_pos = isel >> 3;
-          sm.ctl_s = s;
-          sm.ctl_X = Xc;
-          sm.ctl_from = from_g;
-          sm.ctl_to = to_g;
-          sm.ctl_gx = sX;
-          sm.ctl_gy = sY;
-          sm.ctl_gz = sZ;
-          // move the vacancy: local coordinates by the jump offset, no division needed
-          const int qx = sm.vcx[ksel] >> 1, qy = sm.vcy[ksel], qz = sm.vcz[ksel];
-          const int nlx = sm.vcx[ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
-          sm.ctl_qx = qx;
-          sm.ctl_qy = qy;
-          sm.ctl_qz = qz;
-          sm.vcx[ksel] = static_cast<int16_t>(nlx);
-          sm.vcy[ksel] = static_cast<int16_t>(nly);
-          sm.vcz[ksel] = static_cast<int16_t>(nlz);
-          sm.vloc[ksel] = tl;
-          sm.vlid[ksel] = to_g;
-          sm.vgx[ksel] = ngx;
-          sm.vgy[ksel] = ngy;
-          sm.vgz[ksel] = ngz;
-          const int cx = nlx >> 1;
-          sm.vact[ksel] =
-              cx >= R.hx && cx < R.hx + R.w[0] && nly >= 2 && nly < 2 + R.w[1] && nlz >= 2 && nlz < 2 + R.w[2];
-        } else if (!sm.ctl_stop && a.mode == kModeSelectPerform) {  // u * total reached no event
+        const int nx = it ^ 1;
+        int nstop = 0;
+        if (a.mode == kModeSelectPerform) {  // the per-hop entry point stops after one selection
           akmc_event* e = a.api_event;
           e->round = 0;
           e->hop = hop0;
-          e->from_site = -1;
-          e->to_site = -1;
+          e->from_site = hop ? sm.vlid[c][ksel] : -1;
+          e->to_site = hop ? to_g : -1;
           e->block = B.local_id;
-          e->species = 0;
-          e->u = sm.ctl_u;
-          e->total = total_last;
+          e->species = X;
+          e->u = u;
+          e->total = total;
           e->dt = 0.0;
           e->n_act = nord;
-          e->n_dirty = 0;
-          e->job = B.job;
-          e->reserved = 0;
-          sm.ctl_stop = 1;
-        }
-      }
-      if (a.mode == kModeSelectPerform && isel >= 0) {  // the per-hop entry point stops here
-        __syncwarp();
-        int nd = 0;
-        for (int base = 0; base < cnt; base += 32) nd += __popc(dirty_mask(base));
-        if (lane == 0) {
-          akmc_event* e = a.api_event;
-          e->round = 0;
-          e->hop = hop0;
-          e->from_site = sm.ctl_from;
-          e->to_site = sm.ctl_to;
-          e->block = B.local_id;
-          e->species = sm.ctl_X;
-          e->u = sm.ctl_u;
-          e->total = total_last;
-          e->dt = 0.0;
-          e->n_act = nact_last;
           e->n_dirty = nd;
           e->job = B.job;
           e->reserved = 0;
-          nh = 1;
-          evals += nd;
-          nact_sum += nact_last;
-          sm.ctl_stop = 1;
+          if (hop) {
+            nh = 1;
+            evals += nd;
+            nact_sum += nord;
+          }
+          nstop = 1;
+        } else {
+          // the selection used the uniform drawn ahead: the stream moves on
+          for (int i = 0; i < 4; ++i) sm.xs[i] = sm.xsn[it][i];
+          const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
+          const double dt = -port_log(u2) / total;
+          sector_time += dt;
+          if (hop) {
+            ++nh;
+            evals += nd;
+            nact_sum += nord;
+            if (a.log_cap > 0) {
+              const unsigned long long slot = atomicAdd(a.log_count, 1ull);
+              if (slot < static_cast<unsigned long long>(a.log_cap)) {
+                akmc_event* e = a.log + slot;
+                e->round = round_now;
+                e->hop = hop0 + nh - 1;
+                e->from_site = sm.vlid[c][ksel];
+                e->to_site = to_g;
+                e->block = B.local_id;
+                e->species = X;
+                e->u = u;
+                e->total = total;
+                e->dt = dt;
+                e->n_act = nord;
+                e->n_dirty = nd;
+                e->job = B.job;
+                e->reserved = 0;
+              } else {
+                atomicOr(a.status, kErrLogOverflow);
+              }
+            }
+          }
+          if (!(sector_time < thr)) nstop = 1;
+          if (nh >= a.hop_cap) {
+            atomicOr(a.status, kErrHopCap);
+            nstop = 1;
+          }
+          if (!nstop) {  // the next selection's uniform, committed only if a selection uses it
+            uint64_t x[4] = {sm.xs[0], sm.xs[1], sm.xs[2], sm.xs[3]};
+            sm.ctl_u[nx] = uniform_co(x);
+            for (int i = 0; i < 4; ++i) sm.xsn[nx][i] = x[i];
+          }
         }
+        sm.ctl_stop[nx] = nstop;
       }
     }
-    __syncthreads();  // (S) selection, lattice and vacancy record updated
-    AKMC_PHASE(3);
-    if (sm.ctl_stop) {
-      if (eam && sm.ctl_hop && tid < kRefreshN) refresh(tid);  // the per-hop entry point's hop
-      break;
-    }
+    __syncthreads();  // set n (or c), the clock's decision and the next uniform visible
+    AKMC_PHASE(5);
+    if (hop) c = n;
+    it ^= 1;
   }
   __syncthreads();
   AKMC_PHASE(6);
+  if (tid == 0) sm.fin = c;  // every thread holds the same c
   if (a.mode == kModeCalc) return true;
   if (tid == kCtl) {
     if (a.mode == kModeRound) {
@@ -1016,7 +1029,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.acc[5] += static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2));
   }
   // the lattice was written through at every hop; only the vacancy positions remain
-  if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[tid];
+  if (tid < cnt) a.vac_site[sm.vidx[tid]] = sm.vlid[c][tid];
   return true;
 }
 
@@ -1500,10 +1513,11 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         if (ran && tid < cnt) {
           // a vacancy still inside the block's area keeps its owner; only one that left it
           // needs the owner lookup
-          const int cx = sm->vgx[tid] >> 1, cy = sm->vgy[tid], cz = sm->vgz[tid];
+          const int f = sm->fin;
+          const int cx = sm->vgx[f][tid] >> 1, cy = sm->vgy[f][tid], cz = sm->vgz[f][tid];
           const bool inside = cx >= B.c0[0] && cx < B.c1[0] && cy >= B.c0[1] && cy < B.c1[1] && cz >= B.c0[2] &&
                               cz < B.c1[2];
-          const int o = inside ? gb : owner_block(J, sm->vlid[tid]);
+          const int o = inside ? gb : owner_block(J, sm->vlid[f][tid]);
           if (o != gb) {
             flow_give(a, o, sm->vidx[tid]);
             const unsigned long long bit = 1ull << sm->fslot[tid];

@@ -120,6 +120,18 @@ def test_uneven_blocks_and_odd_edges(ak):
     eng.close()
 
 
+@pytest.mark.parametrize("model,prec", [(po.MODEL_EAM, po.FP64), (po.MODEL_PAIRBOND, po.FP64)])
+def test_single_domain_24_cubed_wrapped_bulk_staging(ak, model, prec):
+    # rows of 48 sites: every sector's halo wraps in x, and each staged row goes in two bulk copies
+    eng, (o,) = run_pair(ak, 320, [dict(box=(24, 24, 24), model=model, precision=prec, alloy=QUATERNARY,
+                                        n_vacancies=12, temperature=563.0, seed=17)])
+    assert o.hops > 500
+    check_job(eng, o, 0, eng.events())
+    if model == po.MODEL_EAM:
+        assert np.array_equal(eng.rho(0), o.rho())
+    eng.close()
+
+
 @pytest.mark.parametrize("schedule", [1, 2])
 def test_uneven_blocks_with_bulk_staging(ak, schedule):
     # rows of 80 sites (a multiple of 16): regions that do not wrap in x are staged by bulk

@@ -1,15 +1,18 @@
 """The bulk-copy staging geometry, checked on the CPU for every block and sector of the box and
 block layouts the host accepts.
 
-The hop kernels stage a sector region (the sector plus a 2-cell halo) by one bulk copy per row
-and array when the lattice rows hold a multiple of 16 sites and the region does not wrap in x
-(make_region in csrc/akmc_kernels.cu); the host sizes shared memory for the widest such region
-(region_sites in csrc/akmc_api.cu).  A bulk copy wants a 16-byte aligned source, destination and
-size, and must stay inside the lattice array.  This test restates that geometry and checks, for
-each copy: alignment of the row start in both arrays (occupancy bytes, int32 densities), sizes
-that are multiples of 16 bytes, an end inside the lattice row, a shared-memory row pitch that
-holds the copy and keeps every row 16-byte aligned, a layout within the host's sizing, a
-transaction count within the mbarrier's limit, and the x halo the hop loop uses for its
+The hop kernels stage a sector region (the sector plus a 2-cell halo) by bulk copies of whole
+rows when the lattice rows hold a multiple of 16 sites (make_region and the staging in
+csrc/akmc_kernels.cu): each row's span is rounded out to 16-site boundaries from the region's
+unwrapped origin, and a span that runs past the row's end, or starts before it (the halo of a
+sector on the box's face in x), goes in two pieces, one from each end of the row.  The host sizes
+shared memory for the widest region (region_sites in csrc/akmc_api.cu).  A bulk copy wants a
+16-byte aligned source, destination and size, and must stay inside the lattice array.  This test
+restates that geometry and checks, for each piece: alignment in both arrays (occupancy bytes,
+int32 densities), sizes that are multiples of 16 bytes, a place inside the lattice row, pieces
+of one row that cover disjoint sites and land where the unwrapped span puts them, a shared-memory
+row pitch that holds the span and keeps every row 16-byte aligned, a layout within the host's
+sizing, a transaction count within the mbarrier's limit, and the x halo the hop loop uses for its
 "still inside the sector" test.
 """
 import itertools
@@ -58,17 +61,28 @@ def regions(n, nb):
                     w.append(half)
             R = dict(ox=2 * (slo[0] - 2), LX=2 * (w[0] + 4), LY=w[1] + 4, LZ=w[2] + 4, bulk=False)
             R["LXt"], R["xo"] = R["LX"], 0
-            if sx % 16 == 0 and R["ox"] >= 0 and R["ox"] + R["LX"] <= sx:
-                x0 = R["ox"] & ~15
+            x0 = R["ox"] & ~15  # Python's & rounds negative origins down too
+            bo = (R["ox"] - x0 + R["LXt"] + 15) & ~15
+            if sx % 16 == 0 and bo <= sx:
                 R["xo"] = R["ox"] - x0
                 R["ox"] = x0
                 R["LX"] = (R["LXt"] + 14 + 15) & ~15
-                R["bo"] = (R["xo"] + R["LXt"] + 15) & ~15
+                R["bo"] = bo
                 R["br"] = (R["xo"] + R["LXt"] + 3) & ~3
                 R["bulk"] = True
             R["hx"] = slo[0] - R["ox"] // 2
             R["n"] = R["LX"] * R["LY"] * R["LZ"]
             yield (bx, by, bz), sec, R
+
+
+def pieces(ox, length, sx):
+    """The bulk copies of one row's span of `length` sites from the unwrapped origin ox, as the
+    staging issues them: (row position, sites, shared position)."""
+    n1 = -ox if ox < 0 else min(length, sx - ox)
+    out = [(ox + sx if ox < 0 else ox, n1, 0)]
+    if length > n1:
+        out.append((0, length - n1, n1))
+    return out
 
 
 LAYOUTS = [(n, nb) for n in (8, 16, 17, 20, 24, 25, 31, 32, 40, 47, 48, 56, 64, 96)
@@ -90,13 +104,17 @@ def test_every_bulk_copy_is_aligned_and_in_bounds(n, nb):
             continue
         n_bulk += 1
         ox, LX, bo, br = R["ox"], R["LX"], R["bo"], R["br"]
-        # sources: every row starts at a multiple of sx (a multiple of 16 sites), plus ox
-        assert sx % 16 == 0 and ox % 16 == 0
-        assert (4 * ox) % 16 == 0
-        # sizes, ends inside the lattice row
-        assert bo % 16 == 0 and (4 * br) % 16 == 0
-        assert 0 <= ox and ox + bo <= sx and ox + br <= sx
-        # shared rows: the pitch holds both copies and the region, and keeps rows aligned
+        assert sx % 16 == 0 and ox % 16 == 0 and -16 <= ox < sx
+        for length, es in ((bo, 1), (br, 4)):  # occupancy bytes, int32 densities
+            for piece_at, piece_len, dst in pieces(ox, length, sx):
+                # every row starts at a multiple of sx (a multiple of 16 sites)
+                assert (es * piece_at) % 16 == 0 and (es * piece_len) % 16 == 0 and (es * dst) % 16 == 0
+                assert 0 <= piece_at and piece_at + piece_len <= sx and piece_len > 0
+                # the piece holds the sites the unwrapped span puts at shared positions dst..
+                assert (ox + dst) % sx == piece_at
+            got = sorted(x for a, m, _ in pieces(ox, length, sx) for x in range(a, a + m))
+            assert got == sorted((ox + k) % sx for k in range(length)) and len(set(got)) == length
+        # shared rows: the pitch holds both spans and the region, and keeps rows aligned
         assert LX % 16 == 0 and bo <= LX and br <= LX and R["xo"] + R["LXt"] <= LX
         assert R["n"] % 2 == 0
         # the mbarrier's transaction count
@@ -105,6 +123,20 @@ def test_every_bulk_copy_is_aligned_and_in_bounds(n, nb):
         assert n_bulk > 0
 
 
-def test_256_cubed_stages_fifteen_of_sixteen_rounds_by_bulk_copies():
-    flags = [R["bulk"] for _, _, R in regions(256, 16)]
-    assert sum(flags) * 16 == len(flags) * 15
+def test_256_cubed_stages_every_round_by_bulk_copies():
+    # rows of 512 sites: regions on the box's faces in x go in two pieces per row
+    regs = [R for _, _, R in regions(256, 16)]
+    assert all(R["bulk"] for R in regs)
+    wrapped = [R for R in regs if R["ox"] < 0 or R["ox"] + R["bo"] > 512]
+    assert len(wrapped) * 16 == len(regs)
+
+
+@pytest.mark.parametrize("n", [24, 32, 40, 48])
+def test_single_block_boxes_with_16_site_rows_stage_by_bulk_copies(n):
+    # one block: every sector's halo wraps in x
+    assert all(R["bulk"] for _, _, R in regions(n, 1))
+
+
+def test_a_span_longer_than_the_row_stays_on_row_loads():
+    # a 16-cell box: rows of 32 sites, but the 24-site region rounds out to a 48-site span
+    assert not any(R["bulk"] for _, _, R in regions(16, 1))
