@@ -79,6 +79,7 @@ struct akmc_ctx {
   int32_t* d_api_count = nullptr;
   size_t smem = 0;
   int hop_grid = 0;
+  int grid_sms = 0, grid_fit = 1, grid_resident = 1;  // SMs, CTAs per SM by shared memory / by registers
   RoundArgs args{};
   cudaGraphExec_t graph = nullptr;
   cudaGraph_t graph_def = nullptr;
@@ -603,17 +604,34 @@ void give_range(std::vector<std::pair<int32_t, int32_t>>& fr, int32_t at, int32_
   fr.swap(m);
 }
 
-// Energy kinds present, and whether AUTO may pick the dependency-driven schedule: more than one
-// block slot, and every live job's block areas start with at most 32 vacancies.
+// Energy kinds present; whether AUTO may pick the dependency-driven schedule (more than one
+// block in use, and every live job's block areas start with at most 32 vacancies); and the
+// extent of the tables the kernels walk: every slot below the highest one in use (free slots
+// below it are skipped by the kernels), so a context with room for many jobs pays only for the
+// ones it holds; the launch grids follow.
 void refresh_job_set(akmc_ctx* ctx) {
   int mask = 0, area = 0;
-  for (const auto& j : ctx->jobs) {
+  int32_t hb = 0, hv = 0, hj = 0, live_blocks = 0;
+  for (size_t k = 0; k < ctx->jobs.size(); ++k) {
+    const auto& j = ctx->jobs[k];
     if (!j.live) continue;
     mask |= 1 << (j.cfg.energy_model == AKMC_MODEL_PAIRBOND ? 0 : (j.cfg.precision == AKMC_FP32C ? 2 : 1));
     area = std::max(area, j.area_max);
+    hb = std::max(hb, j.block0 + j.nblocks);
+    hv = std::max(hv, j.vac0 + static_cast<int32_t>(j.nvac));
+    hj = static_cast<int32_t>(k) + 1;
+    live_blocks += j.nblocks;
   }
-  ctx->args.kind_mask = mask;
-  ctx->flow_ok = area <= kFlowSlots / 2 && ctx->cap_blocks > 1;
+  RoundArgs& a = ctx->args;
+  a.kind_mask = mask;
+  a.nblocks = std::max(hb, 1);  // block slot 0 is free when nothing is held: every kernel skips it
+  a.nvac = hv;
+  a.njobs = std::max(hj, 1);
+  ctx->nblocks = a.nblocks;
+  ctx->nvac = a.nvac;
+  ctx->hop_grid = std::max(1, std::min(a.nblocks, ctx->grid_sms * ctx->grid_fit));
+  ctx->flow_grid = std::max(1, std::min(a.nblocks, ctx->grid_sms * ctx->grid_resident));
+  ctx->flow_ok = area <= kFlowSlots / 2 && live_blocks > 1;
 }
 
 // After the job set changed: the captured round graph and the whole-context transfer tables
@@ -693,8 +711,6 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   ctx->cap_vac = std::max<int32_t>(nv, room ? static_cast<int32_t>(std::min<int64_t>(ctx->cfg.max_vacancies, INT32_MAX)) : 0);
   if (room && (ctx->cap_blocks < 1 || ctx->cap_vac < 1)) return fail(ctx, AKMC_EINVAL, "max_blocks and max_vacancies must be > 0");
   ctx->cap_pots = static_cast<int32_t>(ctx->pots.size()) + (room ? 16 : 0);
-  ctx->nblocks = ctx->cap_blocks;
-  ctx->nvac = ctx->cap_vac;
   int dev_smem = 0;
   CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
   // bulk staging where its wider rows fit, else row loads everywhere
@@ -718,8 +734,9 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   const int fit = std::max(1, std::min(2, static_cast<int>(smem_sm / (ctx->smem + 1024))));
   const int resident = std::min(fit, hop_ctas_per_sm(ctx->cfg.eval_warps));
   const int32_t cb = ctx->cap_blocks;
-  ctx->hop_grid = std::max(1, std::min(cb, sms * fit));
-  ctx->flow_grid = std::max(1, std::min(cb, sms * resident));
+  ctx->grid_sms = sms;
+  ctx->grid_fit = fit;
+  ctx->grid_resident = resident;
 
   // geometry and potentials
   Geometry geo;

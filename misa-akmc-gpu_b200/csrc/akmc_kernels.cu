@@ -1170,7 +1170,8 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_ho
 // reads the round and takes the lease, and one store after a fence publishes the rounds run
 // and frees the lease together.  B.round is refreshed from the word when the launch ends.
 // A single-block job's rounds depend on nothing else, so the CTA that ran one runs the next
-// straight away (its hop budget is checked here, at each time-step boundary).
+// straight away when it holds no other round of the sweep (its hop budget is checked here, at
+// each time-step boundary).
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;
@@ -1534,8 +1535,9 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           // round r ran (it was below the target when handed over)
           int64_t rn = r + 1;
           bool more = false, reached = rn >= __ldcg(&B.target);
-          if (!reached && J.nblocks == 1) {
+          if (!reached && J.nblocks == 1 && c + 1 == ncand) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
+            // -- when no other round this CTA took in the sweep is waiting for it
             more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, &rn, &reached);
           }
 #ifdef AKMC_FLOW_PROFILE
