@@ -197,8 +197,9 @@ AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
  * ROUNDS: every block finishes round r before any starts r+1 (SubLattice::startTimeLoop,
  * sublattice.inl:61-179, with the blocks as MPI ranks).  FLOW: a block's round waits only
  * for the neighbour rounds whose staged regions (sector plus a 2-cell halo) overlap it, so
- * blocks with few hops run ahead; results are identical to ROUNDS.  Under FLOW, jobs with a
- * hop budget advance one time step per launch.  AUTO (default): FLOW when the context holds
+ * blocks with few hops run ahead; results are identical to ROUNDS.  Under FLOW a job's hop
+ * budget is checked inside the launch: the blocks of a multi-block budget job wait for one
+ * another at each time-step boundary.  AUTO (default): FLOW when the context holds
  * more than one domain block and every block area starts with at most 32 vacancies, else
  * ROUNDS.  akmc_run_rounds_noalloc always runs ROUNDS. */
 enum { AKMC_SCHEDULE_AUTO = 0, AKMC_SCHEDULE_ROUNDS = 1, AKMC_SCHEDULE_FLOW = 2 };

@@ -1240,18 +1240,14 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
       e0 = ctx->ev[0];
       e1 = ctx->ev[1];
     }
-    // each block runs n_rounds (fewer if its job ends); the blocks of a multi-block job with a
-    // hop budget stop at each time-step boundary, where k_flow_finalize checks the job's hops,
-    // so those launches run at most to the next one (one more launch for a job that starts
-    // between boundaries).  A single-block job's budget is checked inside the launch.
-    bool budget = false;
-    for (const auto& j : ctx->jobs) budget = budget || (j.live && j.cfg.hop_budget > 0 && j.nblocks > 1);
+    // each block runs n_rounds (fewer if its job ends: hop budgets are checked by the kernel at
+    // time-step boundaries), up to 1024 per launch
     {
       const int e = launch_flow_begin(a, n_rounds, ctx->stream);
       if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
     }
-    const int64_t per = budget ? 8 : 1024;
-    const int64_t launches = (n_rounds + per - 1) / per + (budget ? 1 : 0);
+    const int64_t per = 1024;
+    const int64_t launches = (n_rounds + per - 1) / per;
     for (int64_t k = 0; k < launches; ++k) {
       a.flow_rounds = per;
       const int e = launch_flow(a, ctx->flow_grid, ctx->smem, ctx->stream, e0, e1);

@@ -86,6 +86,8 @@ struct BlockDev {
   int32_t done;          // the job finished at or before this block's last round
   int64_t target;        // asynchronous schedule: round this launch runs the block up to
   int64_t remaining;     // asynchronous schedule: rounds of the akmc_run_rounds call still to run
+  int64_t hops_at[2];    // asynchronous schedule: hops when the block reached time-step boundary b,
+                         // in slot (b / 8) & 1 (a multi-block job's hop budget is checked there)
 };
 
 enum : uint32_t {

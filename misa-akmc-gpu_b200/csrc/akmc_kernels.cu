@@ -1221,6 +1221,25 @@ __device__ __forceinline__ int flow_neighbour(const JobDev& J, int local_id, int
 // Whether round r of the block may run.  The neighbours' round counters are read with
 // relaxed loads, all in flight at once, and a fence follows a positive answer (the acquire
 // pattern): the writes of the rounds waited for become visible to this thread.
+// A multi-block job with a hop budget ends at the end of the first time step at which the hops
+// of all its blocks reach the budget, so its round b at a time-step boundary (b = 8, 16, ...)
+// runs only once every block of the job has reached b; the blocks' hops at b (hops_at, written
+// when each reached b) then decide.  Blocks of the job are thus never a whole time step apart,
+// and the two hops_at slots never hold a boundary someone still reads.  Returns 0 while a block
+// is behind, 1 to run round b, 2 when the job ends at b.
+__device__ int budget_gate(const RoundArgs& a, const JobDev& J, int64_t b) {
+  if (J.hop_budget <= 0 || J.nblocks == 1 || b == 0 || (b & 7)) return 1;
+  bool all = true;
+  for (int k = 0; k < J.nblocks; ++k)
+    all &= static_cast<int64_t>(ld_relaxed_u64(&a.fstate[J.block0 + k]) >> 1) >= b;
+  if (!all) return 0;
+  fence_acq_rel();  // the hops_at written before those rounds were published
+  const int slot = static_cast<int>((b >> 3) & 1);
+  int64_t sum = 0;
+  for (int k = 0; k < J.nblocks; ++k) sum += __ldcg(&a.blocks[J.block0 + k].hops_at[slot]);
+  return sum >= J.hop_budget ? 2 : 1;
+}
+
 __device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, int64_t r, const int8_t (*lag)[27]) {
   const int ph = static_cast<int>(r & 7);
   bool ok = true;
@@ -1229,6 +1248,7 @@ __device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, in
     const int k = lag[ph][o];
     if (k) ok &= static_cast<int64_t>(ld_relaxed_u64(&a.fstate[flow_neighbour(J, local_id, o)]) >> 1) >= r - k + 1;
   }
+  if (ok && budget_gate(a, J, r) == 0) ok = false;  // (a job that ends at r is taken, to mark it)
   if (ok) fence_acq_rel();
   return ok;
 }
@@ -1347,6 +1367,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
   }
   const int64_t last = min(target, r0 + 64);
   const double window = J.window;
+  const int64_t hops = __ldcg(&B.hops);  // empty rounds add none
   int64_t r = r0;
   bool stop_full = false;
   while (r < last) {
@@ -1358,6 +1379,12 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
       if (k && P[o] < r - k + 1) ok = false;
     }
     if (!ok) break;
+    const int g = budget_gate(a, J, r);
+    if (g == 0) break;
+    if (g == 2) {  // the job ends at this boundary: the block's target moves down to it
+      B.target = r;
+      break;
+    }
     const int sec = sector_of_round(r);
     if ((occ_sec >> sec) & 1u) {
       stop_full = true;
@@ -1373,13 +1400,14 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
 #pragma unroll
     for (int k = 0; k < 8; ++k) evo[k] = k == sec ? ne : evo[k];
     ++r;
+    if ((r & 7) == 0) B.hops_at[(r >> 3) & 1] = hops;
   }
   if (r > r0) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) B.evo[k] = evo[k];
   }
   *rn = r;
-  *reached = r == target;
+  *reached = r == __ldcg(&B.target);
   return stop_full;
 }
 
@@ -1534,6 +1562,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
 #endif
           // round r ran (it was below the target when handed over)
           int64_t rn = r + 1;
+          if ((rn & 7) == 0) B.hops_at[(rn >> 3) & 1] = __ldcg(&B.hops);
           bool more = false, reached = rn >= __ldcg(&B.target);
           if (!reached && J.nblocks == 1 && c + 1 == ncand) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
@@ -1596,11 +1625,10 @@ __global__ void k_flow_prep(RoundArgs a) {
     return;
   }
   const JobDev& J = a.jobs[B.job];
-  // up to flow_rounds of the block's remaining rounds; a multi-block job with a hop budget
-  // stops at its next time-step boundary, where k_flow_finalize checks the budget (a
-  // single-block job's budget is checked by the kernel)
+  // up to flow_rounds of the block's remaining rounds (hop budgets are checked by the kernel,
+  // at time-step boundaries); a block sitting at a boundary records its hops there
   int64_t L = B.remaining < a.flow_rounds ? B.remaining : a.flow_rounds;
-  if (J.hop_budget > 0 && J.nblocks > 1 && L > 8 - (B.round & 7)) L = 8 - (B.round & 7);
+  if ((B.round & 7) == 0) B.hops_at[(B.round >> 3) & 1] = B.hops;
   int64_t t = B.done ? B.round : B.round + L;
   if (J.max_rounds > 0 && t > J.max_rounds) t = J.max_rounds > B.round ? J.max_rounds : B.round;
   B.remaining -= t - B.round;
