@@ -66,8 +66,9 @@ inline bool is_atom(uint8_t code) { return code == kFe || code == kCu || code ==
 // Portable exp / log: the same IEEE operation sequence runs on the host and on
 // the GPU, so rates and clocks agree bit for bit.
 // exp: Cody & Waite argument reduction x = k ln2 + r (ln2 split in a 32-bit
-//      head and a tail), Taylor polynomial of degree 13 for e^r on |r| <= ln2/2,
-//      scaling by 2^k through the exponent field.
+//      head and a tail), Taylor polynomial of degree 13 for e^r on |r| <= ln2/2
+//      as 1 + (r + r^2 T(r)) with the tail T in Estrin's scheme, scaling by 2^k
+//      through the exponent field.
 // log: x = m 2^e with m in [sqrt(1/2), sqrt(2)); log m = 2 atanh(s),
 //      s = (m-1)/(m+1), atanh series to s^25.
 // ---------------------------------------------------------------------------
@@ -96,20 +97,18 @@ double port_exp(double x) {
   const int k = static_cast<int>(kd);
   double r = std::fma(-kd, kLn2Hi, x);
   r = std::fma(-kd, kLn2Lo, r);
-  double p = 0x1.6124613a86d09p-33;      // 1/13!
-  p = std::fma(p, r, 0x1.1eed8eff8d898p-29);  // 1/12!
-  p = std::fma(p, r, 0x1.ae64567f544e4p-26);  // 1/11!
-  p = std::fma(p, r, 0x1.27e4fb7789f5cp-22);  // 1/10!
-  p = std::fma(p, r, 0x1.71de3a556c734p-19);  // 1/9!
-  p = std::fma(p, r, 0x1.a01a01a01a01ap-16);  // 1/8!
-  p = std::fma(p, r, 0x1.a01a01a01a01ap-13);  // 1/7!
-  p = std::fma(p, r, 0x1.6c16c16c16c17p-10);  // 1/6!
-  p = std::fma(p, r, 0x1.1111111111111p-7);   // 1/5!
-  p = std::fma(p, r, 0x1.5555555555555p-5);   // 1/4!
-  p = std::fma(p, r, 0x1.5555555555555p-3);   // 1/3!
-  p = std::fma(p, r, 0.5);
-  p = std::fma(p, r, 1.0);
-  p = std::fma(p, r, 1.0);
+  // e^r = 1 + (r + r^2 T(r)), T(r) = sum of r^(i-2) / i! for i = 2..13 in Estrin's scheme:
+  // pairs (1/i! + r/(i+1)!), then powers r^2, r^4, r^8 (the device runs the same operations)
+  const double r2 = r * r, r4 = r2 * r2, r8 = r4 * r4;
+  const double p23 = std::fma(0x1.5555555555555p-3, r, 0.5);                     // 1/2! + r/3!
+  const double p45 = std::fma(0x1.1111111111111p-7, r, 0x1.5555555555555p-5);    // 1/4!, 1/5!
+  const double p67 = std::fma(0x1.a01a01a01a01ap-13, r, 0x1.6c16c16c16c17p-10);  // 1/6!, 1/7!
+  const double p89 = std::fma(0x1.71de3a556c734p-19, r, 0x1.a01a01a01a01ap-16);  // 1/8!, 1/9!
+  const double p1011 = std::fma(0x1.ae64567f544e4p-26, r, 0x1.27e4fb7789f5cp-22);  // 1/10!, 1/11!
+  const double p1213 = std::fma(0x1.6124613a86d09p-33, r, 0x1.1eed8eff8d898p-29);  // 1/12!, 1/13!
+  const double t0 = std::fma(p45, r2, p23), t1 = std::fma(p89, r2, p67), t2 = std::fma(p1213, r2, p1011);
+  const double T = std::fma(t2, r8, std::fma(t1, r4, t0));
+  const double p = 1.0 + std::fma(r2, T, r);
   return scale_pow2(p, k);
 }
 
