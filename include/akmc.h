@@ -193,6 +193,14 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds);
  * contexts of a device: calls whose rounds overlap on the device race.  Kernel
  * timing mode is not applied. */
 AKMC_API akmc_status akmc_run_rounds_noalloc(akmc_ctx* ctx, int64_t n_rounds);
+/* No reference counterpart.  Up to n_rounds more rounds of every unfinished job, in one launch of
+ * the dependency-driven schedule that takes no new round after max_us microseconds: each job
+ * advances as far as its own rounds allow in that time, so small jobs are not held to the pace
+ * of large ones (the server's chunks).  Jobs end at different rounds; a later call continues
+ * each where it stopped, and the trajectories are the same as with akmc_run_rounds.  Contexts on
+ * the round-by-round schedule run min(n_rounds, graph_rounds) rounds instead.  Asynchronous, as
+ * akmc_run_rounds; akmc_get_job_states tells where each job is. */
+AKMC_API akmc_status akmc_run_for(akmc_ctx* ctx, int64_t n_rounds, int64_t max_us);
 /* Order in which akmc_run_rounds runs the rounds of different domain blocks.
  * ROUNDS: every block finishes round r before any starts r+1 (SubLattice::startTimeLoop,
  * sublattice.inl:61-179, with the blocks as MPI ranks).  FLOW: a block's round waits only
@@ -375,11 +383,12 @@ typedef struct akmc_server_config {
   int32_t lanes;            /* lanes, each with its own context and stream (0: 2) */
   int64_t budget_bytes;     /* device memory the running jobs of all lanes may hold (0: 8 GiB) */
   int32_t max_batch_jobs;   /* jobs one lane runs at once (0: 512) */
-  int32_t chunk_rounds;     /* rounds between admissions and checks for finished jobs (0: 16; 4x
-                               that while nothing is queued) */
+  int32_t chunk_rounds;     /* rounds per chunk of a lane whose context runs round by round (0: 16) */
   int32_t order;            /* admission order of queued jobs: AKMC_SERVE_FIFO (arrival) or
                                AKMC_SERVE_SMALLEST_BUDGET (smallest hop budget first; jobs
                                without a budget last; ties in arrival order) */
+  int32_t chunk_us;         /* wall time of a chunk (akmc_run_for) between admissions and checks
+                               for finished jobs, in microseconds (0: 2000) */
 } akmc_server_config;
 enum { AKMC_SERVE_FIFO = 0, AKMC_SERVE_SMALLEST_BUDGET = 1 };
 typedef struct akmc_job_result {

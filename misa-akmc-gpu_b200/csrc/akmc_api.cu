@@ -1319,6 +1319,24 @@ AKMC_API akmc_status akmc_run_rounds(akmc_ctx* ctx, int64_t n_rounds) {
   return AKMC_OK;
 }
 
+AKMC_API akmc_status akmc_run_for(akmc_ctx* ctx, int64_t n_rounds, int64_t max_us) {
+  if (!ctx) return AKMC_EINVAL;
+  if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
+  if (n_rounds <= 0) return AKMC_OK;
+  if (max_us <= 0) return fail(ctx, AKMC_EINVAL, "max_us must be > 0");
+  const bool flow = ctx->schedule == AKMC_SCHEDULE_FLOW || (ctx->schedule == AKMC_SCHEDULE_AUTO && ctx->flow_ok);
+  if (!flow) return akmc_run_rounds(ctx, std::min<int64_t>(n_rounds, ctx->cfg.graph_rounds));
+  CK(cudaSetDevice(ctx->cfg.device));
+  RoundArgs a = ctx->args;
+  a.mode = kModeRound;
+  a.flow_rounds = n_rounds;
+  a.time_budget_ns = max_us * 1000;
+  int e = launch_flow_begin(a, n_rounds, ctx->stream);
+  if (!e) e = launch_flow(a, ctx->flow_grid, ctx->smem, ctx->stream, nullptr, nullptr);
+  if (e) return fail(ctx, AKMC_ECUDA, std::string("launch: ") + cuda_name(e));
+  return AKMC_OK;
+}
+
 namespace {
 // Per-device address of the fixed round scratch, looked up on the first call with the device current.
 constexpr int kNoAllocDevices = 64;

@@ -88,6 +88,9 @@ struct BlockDev {
   int64_t remaining;     // asynchronous schedule: rounds of the akmc_run_rounds call still to run
   int64_t hops_at[2];    // asynchronous schedule: hops when the block reached time-step boundary b,
                          // in slot (b / 8) & 1 (a multi-block job's hop budget is checked there)
+  int32_t budget_end;    // asynchronous schedule: the hop budget set the block's target (the job
+                         // ends when the block reaches it)
+  int32_t pad2;
 };
 
 enum : uint32_t {
@@ -133,6 +136,7 @@ struct RoundArgs {
   int32_t* flow_done;           // per energy kind: blocks that reached their target
   int64_t flow_rounds;          // rounds this launch adds to every unfinished block
   int64_t flow_sweep_limit;     // sweeps per CTA before the launch gives up (kErrTimeout)
+  int64_t time_budget_ns;       // > 0: the launch takes no new round after this long (akmc_run_for)
   int32_t flow_take;            // rounds with vacancies a CTA takes per sweep (0: all it found)
   int32_t eval_warps;           // CTA shape of the hop kernels: 8 or 4 evaluator warps
   // per-hop entry points

@@ -1178,6 +1178,11 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 // Release/acquire fence at GPU scope (lighter than the sequentially consistent __threadfence).
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
@@ -1314,6 +1319,7 @@ __device__ __forceinline__ int64_t flow_target(BlockDev& B, const JobDev& J, int
     if (b < t) {
       t = b;
       B.target = t;
+      B.budget_end = 1;
     }
   }
   return t;
@@ -1383,6 +1389,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
     if (g == 0) break;
     if (g == 2) {  // the job ends at this boundary: the block's target moves down to it
       B.target = r;
+      B.budget_end = 1;
       break;
     }
     const int sec = sector_of_round(r);
@@ -1430,6 +1437,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
   }
   const int nb = a.nblocks;
   int cursor = static_cast<int>((static_cast<int64_t>(blockIdx.x) * nb) / gridDim.x);
+  const uint64_t t_begin = globaltimer_ns();  // a time-boxed launch takes no new round after its budget
 #ifdef AKMC_PHASE_PROFILE
   long long t_sweep = 0, t_hop = 0, n_sweep = 0, n_full = 0, t0 = 0;
 #endif
@@ -1444,6 +1452,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
       const int done = *reinterpret_cast<volatile int*>(&a.flow_done[KIND]);
       const unsigned st = *reinterpret_cast<volatile unsigned*>(a.status);
       int stop = done >= need || (st & (kErrVacOverflow | kErrRhoRange | kErrHopCap | kErrTimeout)) != 0;
+      if (a.time_budget_ns > 0 && globaltimer_ns() - t_begin >= static_cast<uint64_t>(a.time_budget_ns)) stop = 1;
       if (!stop && sweep >= a.flow_sweep_limit) {  // watchdog; the default 2^24 no launch of <= 1024 rounds needs
         atomicOr(a.status, kErrTimeout);
         stop = 1;
@@ -1564,7 +1573,9 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           int64_t rn = r + 1;
           if ((rn & 7) == 0) B.hops_at[(rn >> 3) & 1] = __ldcg(&B.hops);
           bool more = false, reached = rn >= __ldcg(&B.target);
-          if (!reached && J.nblocks == 1 && c + 1 == ncand) {
+          const bool in_time =
+              a.time_budget_ns <= 0 || globaltimer_ns() - t_begin < static_cast<uint64_t>(a.time_budget_ns);
+          if (!reached && J.nblocks == 1 && c + 1 == ncand && in_time) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
             // -- when no other round this CTA took in the sweep is waiting for it
             more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, &rn, &reached);
@@ -1630,6 +1641,7 @@ __global__ void k_flow_prep(RoundArgs a) {
   int64_t L = B.remaining < a.flow_rounds ? B.remaining : a.flow_rounds;
   if ((B.round & 7) == 0) B.hops_at[(B.round >> 3) & 1] = B.hops;
   int64_t t = B.done ? B.round : B.round + L;
+  B.budget_end = 0;  // a budget that ends the job moves this target down again inside the launch
   if (J.max_rounds > 0 && t > J.max_rounds) t = J.max_rounds > B.round ? J.max_rounds : B.round;
   B.remaining -= t - B.round;
   B.target = t;
@@ -1656,17 +1668,21 @@ __global__ void k_flow_slots(RoundArgs a) {
 // After the flow kernels: job round and done flags as k_finalize leaves them.
 __global__ void k_flow_finalize(RoundArgs a) {
   const int gb = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gb == 0) atomicAdd(a.counters + 2, static_cast<unsigned long long>(a.flow_rounds));
+  if (gb == 0 && a.time_budget_ns <= 0) atomicAdd(a.counters + 2, static_cast<unsigned long long>(a.flow_rounds));
   if (gb >= a.nblocks) return;
   BlockDev& B = a.blocks[gb];
   B.cnt = 0;
   B.round = static_cast<int64_t>(a.fstate[gb] >> 1);
   if (B.job < 0) return;
+  // rounds of the call a time-boxed launch left to run go back to the block's remaining ones
+  if (B.target > B.round) B.remaining += B.target - B.round;
   JobDev& J = a.jobs[B.job];
-  // J.hops holds the launch's hops (added when k_flow ended); all blocks of a budget job stop
-  // at the same time-step boundary
-  const int done = (J.max_rounds > 0 && B.round >= J.max_rounds) ||
-                   (J.hop_budget > 0 && (B.round & 7) == 0 && J.hops >= J.hop_budget);
+  // a hop budget ended the job inside the launch (the block reached the boundary its budget set);
+  // or, when every block ran to the call's target (no time box), the job's hops (J.hops, added
+  // when k_flow ended) reach the budget on a time-step boundary, as the round-by-round finalize
+  // decides
+  const int done = B.done || (J.max_rounds > 0 && B.round >= J.max_rounds) || (B.budget_end && B.round >= B.target) ||
+                   (a.time_budget_ns <= 0 && J.hop_budget > 0 && (B.round & 7) == 0 && J.hops >= J.hop_budget);
   B.done = done;
   if (B.local_id == 0) {
     J.round = B.round;

@@ -8,8 +8,9 @@
 // done -- its lattice read back, its slots and memory freed (akmc_retire_job) -- while the
 // others keep running.  So a job's lattice, density cache, vacancies and random streams stay in
 // device memory from admission to its end, and its trajectory is exactly the one it has alone.
-// With nothing queued, a chunk is kIdleChunks times longer (the queue is checked after every
-// chunk, so a job arriving then waits at most one chunk).  Lanes overlap on the GPU.  All shared
+// A chunk is one time-boxed launch (akmc_run_for, cfg.chunk_us): every live job advances as far
+// as its own rounds allow in that time, so small jobs are not held to the pace of the largest;
+// the queue is checked after every chunk.  Lanes overlap on the GPU.  All shared
 // state is under one mutex; the device work runs outside it.
 #include <algorithm>
 #include <chrono>
@@ -29,8 +30,6 @@
 
 namespace {
 
-// With no job queued, chunks are this many times the configured length.
-constexpr int64_t kIdleChunks = 4;
 // Room of a lane's context: domain blocks and vacancies held at once, the largest block edge.
 constexpr int64_t kLaneBlocks = 1 << 14;
 constexpr int64_t kLaneVacancies = 1 << 18;
@@ -221,14 +220,9 @@ struct akmc_server {
         if (stopping) break;
         continue;
       }
-      // one chunk of rounds of every live job
+      // one chunk: every live job advances as far as it can in cfg.chunk_us
       auto tr = std::chrono::steady_clock::now();
-      bool idle = false;
-      {
-        std::lock_guard<std::mutex> lk(m);
-        idle = queue.empty();
-      }
-      st = akmc_run_rounds(ctx, idle ? kIdleChunks * cfg.chunk_rounds : cfg.chunk_rounds);
+      st = akmc_run_for(ctx, int64_t(1) << 40, cfg.chunk_us);
       js.resize(slots.size());
       if (st == AKMC_OK) st = akmc_get_job_states(ctx, js.data(), static_cast<int32_t>(js.size()));
       add_time(t_run, tr);
@@ -307,6 +301,7 @@ AKMC_API akmc_status akmc_server_create(const akmc_server_config* cfg, akmc_serv
   if (s->cfg.budget_bytes <= 0) s->cfg.budget_bytes = int64_t(8) << 30;
   if (s->cfg.max_batch_jobs <= 0) s->cfg.max_batch_jobs = 512;
   if (s->cfg.chunk_rounds <= 0) s->cfg.chunk_rounds = 16;
+  if (s->cfg.chunk_us <= 0) s->cfg.chunk_us = 2000;
   try {
     for (int i = 0; i < s->cfg.lanes; ++i) s->lanes.emplace_back([s] { s->lane(); });
   } catch (...) {

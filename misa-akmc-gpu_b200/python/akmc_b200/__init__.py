@@ -147,6 +147,7 @@ class ServerConfig(C.Structure):
         ("max_batch_jobs", C.c_int32),
         ("chunk_rounds", C.c_int32),
         ("order", C.c_int32),
+        ("chunk_us", C.c_int32),
     ]
 
 
@@ -215,6 +216,7 @@ SIGNATURES = {
     "akmc_prepare": (C.c_int, [_vp]),
     "akmc_admit_job": (C.c_int, [_vp, C.POINTER(JobConfig), _vp, _i64, C.POINTER(_i32)]),
     "akmc_retire_job": (C.c_int, [_vp, _i32]),
+    "akmc_run_for": (C.c_int, [_vp, _i64, _i64]),
     "akmc_run_rounds": (C.c_int, [_vp, _i64]),
     "akmc_run_rounds_noalloc": (C.c_int, [_vp, _i64]),
     "akmc_set_round_schedule": (C.c_int, [_vp, _i32]),
@@ -453,6 +455,10 @@ class Engine:
         self.jobs[jid.value] = (cfg, occ.size)
         return jid.value
 
+    def run_for(self, n, max_us):
+        """akmc_run_for: up to n more rounds per job, taking no new round after max_us."""
+        self._ck(lib().akmc_run_for(self.h, n, max_us))
+
     def retire_job(self, job):
         """akmc_retire_job: frees the job's slots; its id may be given out again."""
         self._ck(lib().akmc_retire_job(self.h, job))
@@ -645,8 +651,8 @@ class Server:
     """akmc_server: queued jobs admitted into the lanes' running contexts as room frees up,
     results as each job ends."""
 
-    def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0, order=0):
-        cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds, order)
+    def __init__(self, device=0, lanes=0, budget_bytes=0, max_batch_jobs=0, chunk_rounds=0, order=0, chunk_us=0):
+        cfg = ServerConfig(device, lanes, budget_bytes, max_batch_jobs, chunk_rounds, order, chunk_us)
         h = C.c_void_p()
         _check(lib().akmc_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

@@ -240,6 +240,44 @@ def test_single_block_budget_jobs_under_flow(ak):
                 assert st["round"] == total
 
 
+def test_time_boxed_calls_follow_the_oracle(ak):
+    # akmc_run_for: launches that take no new round after 200 us, so every job ends each call at
+    # its own round; repeated until the budget jobs are done and the round-limited ones at their
+    # limit.  A multi-block budget job (its blocks meet at each time-step boundary), single-block
+    # budget jobs, a round-limited multi-block job and a pair-bond job: each equals the oracle.
+    kws = [dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=40,
+                temperature=563.0, seed=61),
+           dict(box=(16, 16, 16), model=po.MODEL_EAM, precision=po.FP32C, alloy=QUATERNARY, n_vacancies=4,
+                temperature=620.0, seed=62),
+           dict(box=(24, 16, 16), blocks=(2, 1, 1), model=po.MODEL_PAIRBOND, alloy=QUATERNARY, n_vacancies=10, seed=63),
+           dict(box=(20, 20, 20), model=po.MODEL_EAM, n_vacancies=6, seed=64)]
+    budgets = [3000, 400, 0, 900]
+    max_rounds = [0, 0, 150, 0]
+    with ak.Engine(event_log_capacity=1 << 20) as eng:
+        oracles = [oracle_job(**kw) for kw in kws]
+        for kw, o, b, m in zip(kws, oracles, budgets, max_rounds):
+            dkw = {key: kw[key] for key in ("box", "blocks", "model", "precision", "seed", "temperature") if key in kw}
+            device_job(eng, o, hop_budget=b, max_rounds=m, **dkw)
+        eng.prepare()
+        eng.set_round_schedule(ak.SCHEDULE_FLOW)
+        calls = 0
+        while not all(st["done"] for st in eng.job_states()):
+            eng.run_for(1 << 20, 200)
+            eng.sync()
+            calls += 1
+            assert calls < 20000
+        assert calls > 3  # the time box cut the runs into several calls
+        for o, b, m in zip(oracles, budgets, max_rounds):
+            if b:
+                o.run(b, 1 << 30)
+            else:
+                o.run_rounds(m)
+        ev = eng.events()
+        for k, o in enumerate(oracles):
+            check_job(eng, o, k, ev)
+            assert eng.job_state(k)["done"]
+
+
 def test_schedule_switch_between_calls(ak):
     # the job server switches a context between the two schedules from one chunk to the next:
     # the trajectory must not notice.  A budget job (it stops at a time-step boundary inside the
