@@ -145,6 +145,37 @@ def test_uneven_blocks_with_bulk_staging(ak, schedule):
     eng.close()
 
 
+@pytest.mark.parametrize("warps,take,schedule", [(4, 0, 1), (4, 0, 2), (8, 1, 2), (4, 4, 2)])
+def test_kernel_shapes_and_takes_give_the_same_trajectories(ak, warps, take, schedule):
+    # the autotuner's knobs: 4 evaluator warps (two jumps each, two CTAs per SM) and the rounds
+    # a CTA takes per sweep must not change a bit of any trajectory
+    jobs = [dict(box=(32, 32, 32), blocks=(2, 2, 2), model=po.MODEL_EAM, alloy=QUATERNARY, n_vacancies=50,
+                 temperature=563.0, seed=71),
+            dict(box=(24, 24, 24), blocks=(2, 1, 1), model=po.MODEL_EAM, precision=po.FP32C, alloy=QUATERNARY,
+                 n_vacancies=12, seed=72),
+            dict(box=(16, 24, 18), model=po.MODEL_PAIRBOND, alloy=QUATERNARY, n_vacancies=9, temperature=500.0,
+                 seed=73),
+            dict(box=(20, 20, 20), model=po.MODEL_EAM, n_vacancies=8, seed=74)]
+    eng = ak.Engine(event_log_capacity=1 << 21, eval_warps=warps, flow_take=take)
+    eng.set_round_schedule(schedule)
+    oracles = []
+    for kw in jobs:
+        o = oracle_job(**kw)
+        dkw = {k: kw[k] for k in ("box", "blocks", "model", "precision", "seed", "temperature") if k in kw}
+        device_job(eng, o, **dkw)
+        oracles.append(o)
+    eng.prepare()
+    for o in oracles:
+        o.run_rounds(120)
+    eng.run_rounds(120)
+    eng.sync()
+    ev = eng.events()
+    for j, o in enumerate(oracles):
+        check_job(eng, o, j, ev)
+    assert np.array_equal(eng.rho(0), oracles[0].rho())
+    eng.close()
+
+
 def test_batched_jobs_of_different_shapes(ak):
     jobs = [
         dict(box=(20, 20, 20), model=po.MODEL_EAM, seed=1, temperature=573.0),
