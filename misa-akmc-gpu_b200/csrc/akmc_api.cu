@@ -94,6 +94,8 @@ struct akmc_ctx {
   unsigned long long* d_vvalid = nullptr;
   int32_t* d_vslot = nullptr;
   int32_t* d_vcount = nullptr;
+  int32_t* d_nbr = nullptr;
+  unsigned int* d_vsec = nullptr;
   int32_t* d_flow = nullptr;  // flow_need[3], flow_done[3]
   // cluster statistics scratch: list, parent, size (one int32 per site of the largest job
   // measured so far), then n_list, the isolated count and the histogram
@@ -171,11 +173,13 @@ void free_device(akmc_ctx* ctx) {
   ctx->ev.clear();
   dfree(ctx->stream, ctx->d_vac_count);
   ctx->d_vac_count = nullptr;
-  void* flow_ptrs[] = {ctx->d_fstate, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vcount, ctx->d_flow};
+  void* flow_ptrs[] = {ctx->d_fstate, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot,
+                       ctx->d_vcount, ctx->d_nbr,    ctx->d_vsec,   ctx->d_flow};
   for (void* p : flow_ptrs) dfree(ctx->stream, p);
   ctx->d_fstate = nullptr;
   ctx->d_vclaim = ctx->d_vvalid = nullptr;
-  ctx->d_vslot = ctx->d_vcount = ctx->d_flow = nullptr;
+  ctx->d_vslot = ctx->d_vcount = ctx->d_nbr = ctx->d_flow = nullptr;
+  ctx->d_vsec = nullptr;
   dfree(ctx->stream, ctx->d_cl);
   dfree(ctx->stream, ctx->d_cl_misc);
   ctx->d_cl = nullptr;
@@ -782,6 +786,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(ctx->stream, &ctx->d_vvalid, ncap));
   CK(dalloc(ctx->stream, &ctx->d_vslot, ncap * kFlowSlots));
   CK(dalloc(ctx->stream, &ctx->d_vcount, ncap));
+  CK(dalloc(ctx->stream, &ctx->d_nbr, ncap * kNbrStride));
+  CK(dalloc(ctx->stream, &ctx->d_vsec, ncap));
   CK(dalloc(ctx->stream, &ctx->d_flow, 6));
   CK(dalloc(ctx->stream, &ctx->d_log_count, 1));
   CK(dalloc(ctx->stream, &ctx->d_api_total, 1));
@@ -847,6 +853,8 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.vvalid = ctx->d_vvalid;
   a.vslot = ctx->d_vslot;
   a.vcount = ctx->d_vcount;
+  a.nbr = ctx->d_nbr;
+  a.vsec = ctx->d_vsec;
   a.flow_need = ctx->d_flow;
   a.flow_done = ctx->d_flow + 3;
   a.flow_take = ctx->cfg.flow_take;

@@ -14,6 +14,7 @@ constexpr int kNoAllocMaxBlocks = AKMC_NOALLOC_MAX_BLOCKS;
 constexpr int kJumpN = 76;                        // |N(s) u N(t)| - 2 sites per jump
 constexpr int kRefreshN = 78;                     // density refresh sites per jump
 constexpr int kShellNb = 58;                      // neighbours within the 5-shell cutoff
+constexpr int kNbrStride = 32;  // words per block of RoundArgs::nbr (one 128-byte line)
 constexpr int kFlowSlots = 64;                    // vacancies held in one domain block's area
 
 // Packed neighbour entry: int8 dX | int8 dy << 8 | int8 dz << 16 | (sh_s | sh_t << 4) << 24,
@@ -132,6 +133,9 @@ struct RoundArgs {
   unsigned long long* vvalid;   // per block: slots of vslot holding a vacancy id
   int32_t* vslot;               // per block: kFlowSlots ids of the vacancies in its area
   int32_t* vcount;              // per block: fill counter while the slots are rebuilt
+  unsigned int* vsec;           // per block: bit s set while a vacancy of its area lies in sector s
+  int32_t* nbr;                 // per block, kNbrStride words: the 27 neighbour blocks (offset
+                                // o = (dz+1)*9 + (dy+1)*3 + dx+1) and a flags word (k_flow_prep)
   int32_t* flow_need;           // per energy kind: blocks with rounds to run in this launch
   int32_t* flow_done;           // per energy kind: blocks that reached their target
   int64_t flow_rounds;          // rounds this launch adds to every unfinished block

@@ -1245,16 +1245,51 @@ __device__ int budget_gate(const RoundArgs& a, const JobDev& J, int64_t b) {
   return sum >= J.hop_budget ? 2 : 1;
 }
 
-__device__ bool flow_ready(const RoundArgs& a, const JobDev& J, int local_id, int64_t r, const int8_t (*lag)[27]) {
-  const int ph = static_cast<int>(r & 7);
+// Flags word of a block's row of RoundArgs::nbr: the energy kind (kNbrFree for a free block
+// slot) and whether the job's hop budget gates its rounds at time-step boundaries (budget_gate).
+constexpr int kNbrFree = 3, kNbrKindMask = 3, kNbrGate = 4;
+
+// The neighbours' completed rounds relative to round r0 (P[o] = rounds - r0, clamped to
+// +-2^30; the block itself never holds it back: 2^30), read with relaxed loads, all in flight at
+// once, from the block's row of the neighbour table.  The caller fences after the loads (an
+// acquire) before it reads what those rounds wrote.  (Relative int32 counts keep the snapshot in
+// 27 registers.)
+constexpr int32_t kAhead = 1 << 30;
+// The block's row of the neighbour table: 27 neighbours and the flags word (y[27]).
+__device__ __forceinline__ void flow_row(const RoundArgs& a, int gb, int (&y)[28]) {
+  const int4* row = reinterpret_cast<const int4*>(a.nbr + static_cast<int64_t>(gb) * kNbrStride);
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    const int4 v = __ldcg(row + q);
+    y[4 * q] = v.x;
+    y[4 * q + 1] = v.y;
+    y[4 * q + 2] = v.z;
+    y[4 * q + 3] = v.w;
+  }
+}
+__device__ __forceinline__ void flow_snapshot(const RoundArgs& a, int gb, const int (&y)[28], int64_t r0,
+                                              int32_t (&P)[27]) {
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    if (y[o] == gb) {
+      P[o] = kAhead;
+    } else {
+      const int64_t d = static_cast<int64_t>(ld_relaxed_u64(&a.fstate[y[o]]) >> 1) - r0;
+      P[o] = static_cast<int32_t>(d > kAhead ? kAhead : (d < -kAhead ? -kAhead : d));
+    }
+  }
+}
+
+// Whether a snapshot relative to r0 lets round r0 + d run (the neighbours' rounds it waits for
+// are complete).
+__device__ __forceinline__ bool flow_ready(const int32_t (&P)[27], int64_t r0, int d, const int8_t (*lag)[27]) {
+  const int ph = static_cast<int>((r0 + d) & 7);
   bool ok = true;
 #pragma unroll
   for (int o = 0; o < 27; ++o) {
     const int k = lag[ph][o];
-    if (k) ok &= static_cast<int64_t>(ld_relaxed_u64(&a.fstate[flow_neighbour(J, local_id, o)]) >> 1) >= r - k + 1;
+    if (k && P[o] < d - k + 1) ok = false;
   }
-  if (ok && budget_gate(a, J, r) == 0) ok = false;  // (a job that ends at r is taken, to mark it)
-  if (ok) fence_acq_rel();
   return ok;
 }
 
@@ -1271,18 +1306,26 @@ __device__ __forceinline__ bool site_in_sector(const BlockDev& B, const JobDev& 
   return true;
 }
 
-// Global block whose area holds site s (the reference's rank split, as k_bucket).
-__device__ __forceinline__ int owner_block(const JobDev& J, int32_t s) {
+// Block whose area holds site s (the reference's rank split, as k_bucket) and the sector of that
+// block the site lies in.
+__device__ __noinline__ int owner_sector(const JobDev& J, int32_t s, int* sec) {
   const int X = s % J.sx;
   const int t = s / J.sx;
   const int c[3] = {X >> 1, t % J.sy, t / J.sy};
   int k[3];
-  for (int d = 0; d < 3; ++d) k[d] = block_of(c[d], J.n[d], J.nb[d]);
+  int q = 0;
+  for (int d = 0; d < 3; ++d) {
+    k[d] = block_of(c[d], J.n[d], J.nb[d]);
+    const int lo = k[d] * (J.n[d] / J.nb[d]) + min(k[d], J.n[d] % J.nb[d]);  // the rank split
+    const int hi = (k[d] + 1) * (J.n[d] / J.nb[d]) + min(k[d] + 1, J.n[d] % J.nb[d]);
+    if (c[d] - lo >= (hi - lo) / 2) q |= 1 << d;
+  }
+  *sec = q;
   return J.block0 + k[0] + J.nb[0] * (k[1] + J.nb[1] * k[2]);
 }
 
 // Puts vacancy v into block o's slots: claim a free slot, write the id, then mark it valid.
-__device__ void flow_give(const RoundArgs& a, int o, int v) {
+__device__ void flow_give(const RoundArgs& a, int o, int v, int osec) {
   for (int tries = 0; tries < 4 * kFlowSlots; ++tries) {
     const unsigned long long m = *reinterpret_cast<volatile unsigned long long*>(&a.vclaim[o]);
     if (m == ~0ull) break;
@@ -1292,6 +1335,7 @@ __device__ void flow_give(const RoundArgs& a, int o, int v) {
     a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
     fence_acq_rel();
     atomicOr(&a.vvalid[o], bit);
+    atomicOr(&a.vsec[o], 1u << osec);
     return;
   }
   atomicOr(a.status, kErrVacOverflow);
@@ -1308,88 +1352,76 @@ __device__ __forceinline__ void flow_publish(const RoundArgs& a, int gb, int64_t
   if (reached) atomicAdd(&a.flow_done[kind], 1);
 }
 
-// The block's target for this launch, read by its lease holder at L2 (a previous holder on
-// another SM may have moved it).  A single-block job with a hop budget ends at the end of the
-// first time step at which its hops reached the budget, so once they have, its target moves
-// down to the next boundary at or after rn (never below rn).
-__device__ __forceinline__ int64_t flow_target(BlockDev& B, const JobDev& J, int64_t rn) {
-  int64_t t = __ldcg(&B.target);
-  if (J.nblocks == 1 && J.hop_budget > 0 && __ldcg(&B.hops) >= J.hop_budget) {
-    const int64_t b = (rn + 7) & ~static_cast<int64_t>(7);
-    if (b < t) {
-      t = b;
-      B.target = t;
-      B.budget_end = 1;
-    }
-  }
-  return t;
-}
-
 // Lease held, one thread, the block at round r0: runs the block's ready rounds whose sectors
 // hold no vacancy (the clock jumps to the window, sublattice.inl:108-112), up to 64 in one
-// batch, and leaves the block's round in *rn (the caller publishes it).  The neighbours' round
-// counters are read once, all 27 loads in flight together: a round is ready when that snapshot
-// already covers it, and the vacancy slots read after the snapshot hold every vacancy those
-// rounds can see (a round that could bring one into such a sector overlaps it, so it is in the
-// snapshot).  Returns true when it stops at a ready round with vacancies, false when the next
+// batch, and leaves the block's round in *rn (the caller publishes it).  A round is ready when
+// the snapshot of the neighbours' round counters (the sweep's, Pin, or one read here with all
+// loads in flight together) already covers it, and the vacancy slots read after the snapshot
+// hold every vacancy those rounds can see (a round that could bring one into such a sector
+// overlaps it, so it is in the snapshot).  Returns true when it stops at a ready round with vacancies, false when the next
 // round is not ready or the target is reached.  *reached: this call moved the block onto its
 // target (by running rounds, or by a budget moving the target down to r0); false for a block
 // that was at its target already (a stale sweep read).
 __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, int gb, const int8_t (*lag)[27],
-                             int64_t r0, int64_t* rn, bool* reached) {
+                             int64_t r0, const int32_t (*Pin)[27], int64_t* rn, bool* reached) {
   *rn = r0;
   *reached = false;
+  // one round of loads, all in flight together: the target, the job's constants, the block's
+  // hops and clocks and its vacancy slots (the lease is held: nothing else writes them but gives)
   const int64_t t_old = __ldcg(&B.target);
+  const int64_t hops = __ldcg(&B.hops);  // empty rounds add none
+  const int nbl = J.nblocks;
+  const int64_t budget = J.hop_budget;
+  const double window = J.window;
+  double evo[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) evo[k] = __ldcg(&B.evo[k]);
+  // sectors holding a vacancy (the slots' sector mask)
+  unsigned occ_sec = __ldcg(&a.vsec[gb]);
   if (r0 >= t_old) return false;
-  const int64_t target = flow_target(B, J, r0);
+  // a single-block job with a hop budget ends at the end of the first time step at which its
+  // hops reached the budget: once they have, its target moves down to the next boundary at or
+  // after r0 (never below r0)
+  int64_t target = t_old;
+  if (nbl == 1 && budget > 0 && hops >= budget) {
+    const int64_t b = (r0 + 7) & ~static_cast<int64_t>(7);
+    if (b < target) {
+      target = b;
+      B.target = b;
+      B.budget_end = 1;
+    }
+  }
   if (r0 >= target) {
     *reached = true;
     return false;
   }
-  const int n0 = J.nb[0], n1 = J.nb[1], n2 = J.nb[2], block0 = J.block0, lid = B.local_id;
-  const int bx = lid % n0, by = (lid / n0) % n1, bz = lid / (n0 * n1);
-  int64_t P[27];
+  // the sweep's snapshot, taken before the lease and fenced after it (rounds only grow, so an
+  // earlier snapshot is a safe one), or a fresh one
+  int32_t P[27];
+  if (Pin) {
 #pragma unroll
-  for (int o = 0; o < 27; ++o) {
-    const int y = block0 + wrapb(bx + o % 3 - 1, n0) + n0 * (wrapb(by + (o / 3) % 3 - 1, n1) + n1 * wrapb(bz + o / 9 - 1, n2));
-    // the block itself never holds it back
-    P[o] = y == gb ? INT64_MAX : static_cast<int64_t>(ld_relaxed_u64(&a.fstate[y]) >> 1);
-  }
-  fence_acq_rel();
-  double evo[8];
+    for (int o = 0; o < 27; ++o) P[o] = (*Pin)[o];
+  } else if (J.nblocks == 1) {  // every neighbour is the block itself: nothing to wait for
 #pragma unroll
-  for (int k = 0; k < 8; ++k) evo[k] = __ldcg(&B.evo[k]);
-  // sectors holding a vacancy
-  unsigned occ_sec = 0;
-  unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
-  const int hx = B.c0[0] + (B.c1[0] - B.c0[0]) / 2, hy = B.c0[1] + (B.c1[1] - B.c0[1]) / 2,
-            hz = B.c0[2] + (B.c1[2] - B.c0[2]) / 2;
-  while (m) {
-    const int slot = __ffsll(static_cast<long long>(m)) - 1;
-    m &= m - 1;
-    const int32_t st = __ldcg(&a.vac_site[__ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + slot])]);
-    const int X = st % J.sx, t = st / J.sx;
-    occ_sec |= 1u << (((X >> 1) >= hx ? 1 : 0) | ((t % J.sy) >= hy ? 2 : 0) | ((t / J.sy) >= hz ? 4 : 0));
+    for (int o = 0; o < 27; ++o) P[o] = kAhead;
+  } else {
+    int y[28];
+    flow_row(a, gb, y);
+    flow_snapshot(a, gb, y, r0, P);
+    fence_acq_rel();
+    occ_sec = __ldcg(&a.vsec[gb]);  // with the vacancies those rounds gave the block
   }
   const int64_t last = min(target, r0 + 64);
-  const double window = J.window;
-  const int64_t hops = __ldcg(&B.hops);  // empty rounds add none
   int64_t r = r0;
   bool stop_full = false;
   while (r < last) {
-    const int ph = static_cast<int>(r & 7);
-    bool ok = true;
-#pragma unroll
-    for (int o = 0; o < 27; ++o) {
-      const int k = lag[ph][o];
-      if (k && P[o] < r - k + 1) ok = false;
-    }
-    if (!ok) break;
+    if (!flow_ready(P, r0, static_cast<int>(r - r0), lag)) break;
     const int g = budget_gate(a, J, r);
     if (g == 0) break;
     if (g == 2) {  // the job ends at this boundary: the block's target moves down to it
       B.target = r;
       B.budget_end = 1;
+      target = r;
       break;
     }
     const int sec = sector_of_round(r);
@@ -1414,7 +1446,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
     for (int k = 0; k < 8; ++k) B.evo[k] = evo[k];
   }
   *rn = r;
-  *reached = r == __ldcg(&B.target);
+  *reached = r == target;  // the lease holder alone moves the target
   return stop_full;
 }
 
@@ -1467,17 +1499,31 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
       int gb = cursor + tid;
       if (gb >= nb) gb -= nb;
       BlockDev& B = a.blocks[gb];
-      const int bj = B.job;
-      const JobDev& J = a.jobs[bj < 0 ? 0 : bj];
+      // one round of loads decides whether to look closer: the block's word, target, job, and its
+      // row of the neighbour table with the flags (energy kind, free slot)
+      int y[28];
+      flow_row(a, gb, y);
       const unsigned long long w = ld_relaxed_u64(&a.fstate[gb]);
+      const int64_t t0 = __ldcg(&B.target);
+      const int bj = __ldcg(&B.job);
       const int64_t r = static_cast<int64_t>(w >> 1);
-      if (bj >= 0 && !(w & 1ull) && job_kind(J) == KIND && r < B.target && flow_ready(a, J, B.local_id, r, sm0->flow_lag) &&
-          atomicCAS(&a.fstate[gb], w, w | 1ull) == w) {
+      int32_t P[27];
+      bool ok = (y[27] & kNbrKindMask) == KIND && !(w & 1ull) && r < t0;
+      if (ok) {  // a second: the neighbours' rounds
+        flow_snapshot(a, gb, y, r, P);
+        ok = flow_ready(P, r, 0, sm0->flow_lag);
+      }
+      // a multi-block job with a hop budget: its round at a time-step boundary waits for the job's
+      // other blocks (a job that ends there is taken, to mark it)
+      if (ok && (y[27] & kNbrGate) && budget_gate(a, a.jobs[bj], r) == 0) ok = false;
+      // the lease, then one fence: the snapshot's and the word's reads become acquires
+      if (ok && atomicCAS(&a.fstate[gb], w, w | 1ull) == w) {
         fence_acq_rel();
+        const JobDev& J = a.jobs[bj];
         int64_t rn = r;
         int keep = 0;
         bool reached = false;
-        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &rn, &reached)) {
+        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &P, &rn, &reached)) {
           const int i = atomicAdd(&sm0->flow_ncand, 1);
           if (i < kFlowTake) {
             sm0->flow_cand[i] = gb;
@@ -1545,6 +1591,9 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
 #ifdef AKMC_PHASE_PROFILE
         if (tid == 0) tw = clock64();
 #endif
+        // the sector's vacancies move: its bit of the block's sector mask goes, and comes back
+        // below for each one still in the block (with the bit of the sector it is in now)
+        if (ran && tid == 0) atomicAnd(&a.vsec[gb], ~(1u << sec));
         __syncthreads();
         // vacancies carried into a neighbour's area change owner (only if the round ran:
         // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
@@ -1555,9 +1604,16 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           const int cx = sm->vgx[f][tid] >> 1, cy = sm->vgy[f][tid], cz = sm->vgz[f][tid];
           const bool inside = cx >= B.c0[0] && cx < B.c1[0] && cy >= B.c0[1] && cy < B.c1[1] && cz >= B.c0[2] &&
                               cz < B.c1[2];
-          const int o = inside ? gb : owner_block(J, sm->vlid[f][tid]);
-          if (o != gb) {
-            flow_give(a, o, sm->vidx[tid]);
+          int osec = 0, o = gb;
+          if (inside)
+            osec = (cx - B.c0[0] >= (B.c1[0] - B.c0[0]) / 2 ? 1 : 0) | (cy - B.c0[1] >= (B.c1[1] - B.c0[1]) / 2 ? 2 : 0) |
+                   (cz - B.c0[2] >= (B.c1[2] - B.c0[2]) / 2 ? 4 : 0);
+          else
+            o = owner_sector(J, sm->vlid[f][tid], &osec);
+          if (o == gb) {
+            atomicOr(&a.vsec[gb], 1u << osec);
+          } else {
+            flow_give(a, o, sm->vidx[tid], osec);
             const unsigned long long bit = 1ull << sm->fslot[tid];
             atomicAnd(&a.vvalid[gb], ~bit);
             fence_acq_rel();
@@ -1578,7 +1634,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           if (!reached && J.nblocks == 1 && c + 1 == ncand && in_time) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
             // -- when no other round this CTA took in the sweep is waiting for it
-            more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, &rn, &reached);
+            more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, nullptr, &rn, &reached);
           }
 #ifdef AKMC_FLOW_PROFILE
           const long long q1 = clock64();
@@ -1630,12 +1686,18 @@ __global__ void k_flow_prep(RoundArgs a) {
   a.vclaim[gb] = 0;
   a.vvalid[gb] = 0;
   a.vcount[gb] = 0;
+  a.vsec[gb] = 0;
+  int32_t* row = a.nbr + static_cast<int64_t>(gb) * kNbrStride;
   if (B.job < 0) {  // a free block slot: nothing to run
     B.target = B.round;
     a.fstate[gb] = static_cast<unsigned long long>(B.round) << 1;
+    for (int o = 0; o < 27; ++o) row[o] = gb;
+    row[27] = kNbrFree;
     return;
   }
   const JobDev& J = a.jobs[B.job];
+  for (int o = 0; o < 27; ++o) row[o] = flow_neighbour(J, B.local_id, o);
+  row[27] = job_kind(J) | (J.hop_budget > 0 && J.nblocks > 1 ? kNbrGate : 0);
   // up to flow_rounds of the block's remaining rounds (hop budgets are checked by the kernel,
   // at time-step boundaries); a block sitting at a boundary records its hops there
   int64_t L = B.remaining < a.flow_rounds ? B.remaining : a.flow_rounds;
@@ -1654,7 +1716,8 @@ __global__ void k_flow_slots(RoundArgs a) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= a.nvac || a.vac_job[v] < 0) return;
   const JobDev& J = a.jobs[a.vac_job[v]];
-  const int o = owner_block(J, a.vac_site[v]);
+  int osec = 0;
+  const int o = owner_sector(J, a.vac_site[v], &osec);
   const int slot = atomicAdd(&a.vcount[o], 1);
   if (slot >= kFlowSlots) {
     atomicOr(a.status, kErrVacOverflow);
@@ -1663,6 +1726,7 @@ __global__ void k_flow_slots(RoundArgs a) {
   a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
   atomicOr(&a.vclaim[o], 1ull << slot);
   atomicOr(&a.vvalid[o], 1ull << slot);
+  atomicOr(&a.vsec[o], 1u << osec);
 }
 
 // After the flow kernels: job round and done flags as k_finalize leaves them.
