@@ -225,7 +225,7 @@ struct JobC {
   double nu, kT;
 };
 
-#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE)
+#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE) && !defined(AKMC_HOP_PROFILE)
 #define EVAL_T(i)                                                                       \
   do {                                                                                  \
     if (threadIdx.x == 0) {                                                             \
@@ -488,6 +488,24 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
 #else
 #define AKMC_STAGE_T(k) \
   do {                \
+  } while (0)
+#endif
+
+// Hop-loop sub-phases (builds with -DAKMC_PHASE_PROFILE -DAKMC_HOP_PROFILE): thread 0 (an
+// evaluator) adds its cycles per stage into counters 16..19, the control thread into 20..22,
+// and counts the iterations in 23.
+#if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE)
+#define HOP_T(k)                                                                                           \
+  do {                                                                                                     \
+    if (threadIdx.x == 0 || threadIdx.x == kCtl) {                                                         \
+      const long long t_ = clock64();                                                                      \
+      atomicAdd(a.counters + (threadIdx.x == 0 ? 16 : 20) + (k), static_cast<unsigned long long>(t_ - thp)); \
+      thp = t_;                                                                                            \
+    }                                                                                                      \
+  } while (0)
+#else
+#define HOP_T(k) \
+  do {           \
   } while (0)
 #endif
 
@@ -761,6 +779,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     return sm.vact[set][k] && abs((sm.vcx[set][k] >> 1) - qx) <= D && abs(sm.vcy[set][k] - qy) <= D &&
            abs(sm.vcz[set][k] - qz) <= D;
   };
+#if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE)
+  long long thp = clock64();
+#endif
   while (true) {
     if (sm.ctl_stop[it]) break;
     const int n = c ^ 1;
@@ -799,6 +820,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
     isel = __shfl_sync(kFull, isel, 0);
     stop = __shfl_sync(kFull, stop, 0);
+    HOP_T(0);
     if (stop) {
       if (tid == kCtl) {
         if (stop == 1) {  // akmc_calculate: the sector's vacancies with their jump rates
@@ -903,6 +925,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           }
         }
         asm volatile("bar.sync 1, %0;" ::"n"(kCtl) : "memory");  // the evaluator warps only
+        HOP_T(1);
         // [3] + [4] the vacancies within D cells of the hop's origin, evaluated into set n
         for (int base = 0; base < cnt; base += 32) {
           const int k = base + lane;
@@ -915,6 +938,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
               eval_vacancy<KIND>(sm, n, occ_s, rho_s, kk, warp + kEvalWarps * jj, FT, jc, jr[jj], nullptr);
           }
         }
+        HOP_T(2);
       }
     } else {  // control warp: the hop's clock and event, the next iteration's decision and uniform
       int nd = 0;
@@ -995,8 +1019,13 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         }
         sm.ctl_stop[nx] = nstop;
       }
+      HOP_T(1);
     }
     __syncthreads();  // set n (or c), the clock's decision and the next uniform visible
+    HOP_T(threadIdx.x == 0 ? 3 : 2);
+#if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE)
+    if (tid == 0) atomicAdd(a.counters + 23, 1ull);
+#endif
     AKMC_PHASE(5);
     if (hop) c = n;
     it ^= 1;
@@ -1470,6 +1499,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
   const int nb = a.nblocks;
   int cursor = static_cast<int>((static_cast<int64_t>(blockIdx.x) * nb) / gridDim.x);
   const uint64_t t_begin = globaltimer_ns();  // a time-boxed launch takes no new round after its budget
+  if (tid == 0) sm0->flow_stop = 0;
 #ifdef AKMC_PHASE_PROFILE
   long long t_sweep = 0, t_hop = 0, n_sweep = 0, n_full = 0, t0 = 0;
 #endif
@@ -1480,19 +1510,18 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
     if (tid == 0) {
       sm0->flow_ncand = 0;
       sm0->flow_progress = 0;
-      const int need = *reinterpret_cast<volatile int*>(&a.flow_need[KIND]);
-      const int done = *reinterpret_cast<volatile int*>(&a.flow_done[KIND]);
-      const unsigned st = *reinterpret_cast<volatile unsigned*>(a.status);
-      int stop = done >= need || (st & (kErrVacOverflow | kErrRhoRange | kErrHopCap | kErrTimeout)) != 0;
-      if (a.time_budget_ns > 0 && globaltimer_ns() - t_begin >= static_cast<uint64_t>(a.time_budget_ns)) stop = 1;
-      if (!stop && sweep >= a.flow_sweep_limit) {  // watchdog; the default 2^24 no launch of <= 1024 rounds needs
-        atomicOr(a.status, kErrTimeout);
-        stop = 1;
-      }
-      sm0->flow_stop = stop;
     }
     __syncthreads();
-    if (sm0->flow_stop) break;
+    if (sm0->flow_stop) break;  // decided during the previous sweep
+    // thread 0 reads the launch's progress and status while the sweep's visits are in flight,
+    // and decides after its own visit whether the CTA stops after this sweep's rounds
+    int need = 0, done = 0;
+    unsigned st = 0;
+    if (tid == 0) {
+      need = *reinterpret_cast<volatile int*>(&a.flow_need[KIND]);
+      done = *reinterpret_cast<volatile int*>(&a.flow_done[KIND]);
+      st = *reinterpret_cast<volatile unsigned*>(a.status);
+    }
 
     // sweep: thread tid looks after block (cursor + tid) mod nb
     if (tid < nb) {
@@ -1533,6 +1562,15 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         if (rn > r) sm0->flow_progress = 1;
         flow_publish(a, gb, rn, keep, reached, KIND);
       }
+    }
+    if (tid == 0) {
+      int stop = done >= need || (st & (kErrVacOverflow | kErrRhoRange | kErrHopCap | kErrTimeout)) != 0;
+      if (a.time_budget_ns > 0 && globaltimer_ns() - t_begin >= static_cast<uint64_t>(a.time_budget_ns)) stop = 1;
+      if (!stop && sweep + 1 >= a.flow_sweep_limit) {  // watchdog; the default 2^24 no launch of <= 1024 rounds needs
+        atomicOr(a.status, kErrTimeout);
+        stop = 1;
+      }
+      sm0->flow_stop = stop;
     }
     __syncthreads();
 #ifdef AKMC_PHASE_PROFILE
@@ -1666,7 +1704,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
     if (cursor >= nb) cursor %= nb;
   }
   cta_flush<W>(a, smem);
-#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE)
+#if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE) && !defined(AKMC_HOP_PROFILE)
   if (tid == 0) {  // scheduler profile: [12] sweep cycles, [13] hop-loop cycles, [14] sweeps, [15] full rounds
     atomicAdd(a.counters + 20, static_cast<unsigned long long>(t_sweep));
     atomicAdd(a.counters + 21, static_cast<unsigned long long>(t_hop));
