@@ -143,6 +143,7 @@ struct Smem {
   int32_t nord[2];
   uint8_t vX[2][kMaxV][8];      // code of jump b's target atom (0: the target is a vacancy)
   double rates[2][kMaxV][8];
+  double presel[kMaxThreads / 32][8];  // per warp: the running sums of the selection's total
   // F-table window, two planes: FP64 (c0, c1) x kFWin then (c2, c3) x kFWin;
   // FP32 (hi, lo, c1, c2) x kFWin then c3 x kFWin
   alignas(16) unsigned char fwin[kFWin * 32];
@@ -315,6 +316,24 @@ __device__ __forceinline__ double F64(const FTab& T, int32_t r) {
   return F64_far(T.g64lo, T.g64hi, T.status, r, p);
 }
 
+// A cell known to lie inside the shared-memory window.
+__device__ __forceinline__ double F64win(const FTab& T, int32_t r) {
+  const int kk = (r >> kRhoCellShift) - T.kw0;
+  const double p = __hiloint2double(0x3FF00000 | ((r & kRhoFracMask) << 3), 0) - 1.0;
+  const double2 lo = reinterpret_cast<const double2*>(T.win)[kk];
+  const double2 hi = reinterpret_cast<const double2*>(T.win)[kFWin + kk];
+  return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
+}
+__device__ __forceinline__ FCell32 cell32win(const FTab& T, int32_t r) {
+  const int kk = (r >> kRhoCellShift) - T.kw0;
+  const float4 a = reinterpret_cast<const float4*>(T.win)[kk];
+  FCell32 c;
+  c.hi = a.x; c.lo = a.y; c.c1 = a.z; c.c2 = a.w;
+  c.c3 = reinterpret_cast<const float*>(T.win + kFWin * 16)[kk];
+  c.pad0 = c.pad1 = c.pad2 = 0.f;
+  return c;
+}
+
 __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
   const int k = r >> kRhoCellShift;
   const unsigned kk = static_cast<unsigned>(k - T.kw0);
@@ -386,27 +405,48 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     const double after = __shfl_down_sync(kFull, pair, 2);
     dE = after - pair;
   } else if (KIND == kEam64) {
-    double acc = 0.0;
+    double acc = 0.0, EX = 0.0;
     const int X = species_index(Xc);
-    // the moving atom's own embedding change; every lane reads the same cells (broadcast),
-    // so its latency overlaps the site loop
-    const double EX = avail ? F64(FT, rho_s[l] - sm.fq1[X]) - F64(FT, rho_s[tl]) : 0.0;
     if (avail) {
+      // gather: this lane's sites (q, q+32, q+64 of the jump's list; lanes 12..31 have two),
+      // their occupancy, densities and shell codes, and the moving atom's own two densities
+      uint8_t o[3];
+      int32_t r0[3], r1[3];
+      int h[3];
+      bool in[3];
 #pragma unroll
-      for (int u = 0; u < 3; ++u) {  // site term (F(r+d) - F(r)) + (phi_s - phi_t)
-        if (q + 32 * u >= kJumpN) break;
-        const int32_t e = p ? jr[1][u] : jr[0][u];
+      for (int u = 0; u < 3; ++u) {
+        in[u] = q + 32 * u < kJumpN;
+        const int32_t e = p ? jr[1][u] : jr[0][u];  // 0 outside the list: the vacancy's own site
         const int j = l + sdelta(e);
-        const int h = jshells(e);
-        const uint8_t o = occ_s[j];
-        const int32_t r = rho_s[j];
-        const double Fa = F64(FT, r + sm.dfq[X * 64 + h]);
-        const double Fb = F64(FT, r);  // independent of Fa: the two overlap
-        if (o != kV) {
-          const int Y = species_index(o);
-          acc += (Fa - Fb) + sm.dphi64[(X * 4 + Y) * 64 + h];
-        }
+        h[u] = jshells(e);
+        o[u] = occ_s[j];
+        r0[u] = rho_s[j];
+        r1[u] = r0[u] + sm.dfq[X * 64 + h[u]];
       }
+      const int32_t rx1 = rho_s[l] - sm.fq1[X], rx0 = rho_s[tl];
+      // every cell inside the shared-memory window (nearly always): one straight run of loads
+      // and polynomials; otherwise the general path, which reads far cells from global memory
+      bool win = static_cast<unsigned>((rx1 >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin) &&
+                 static_cast<unsigned>((rx0 >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin);
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        win = win && (!in[u] || (static_cast<unsigned>((r0[u] >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin) &&
+                                 static_cast<unsigned>((r1[u] >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin)));
+      double t[3];
+      if (win) {
+        EX = F64win(FT, rx1) - F64win(FT, rx0);
+#pragma unroll
+        for (int u = 0; u < 3; ++u) t[u] = in[u] ? F64win(FT, r1[u]) - F64win(FT, r0[u]) : 0.0;
+      } else {
+        EX = F64(FT, rx1) - F64(FT, rx0);
+#pragma unroll
+        for (int u = 0; u < 3; ++u) t[u] = in[u] ? F64(FT, r1[u]) - F64(FT, r0[u]) : 0.0;
+      }
+      // site term (F(r+d) - F(r)) + (phi_s - phi_t), summed in list order
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        if (in[u] && o[u] != kV) acc += t[u] + sm.dphi64[(X * 4 + species_index(o[u])) * 64 + h[u]];
     }
 #pragma unroll
     EVAL_T(0);
@@ -420,21 +460,36 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     acc.c = 0.f;
     const int X = species_index(Xc);
     if (avail) {
+      uint8_t o[3];
+      int32_t r0[3], r1[3];
+      int h[3];
+      bool in[3];
 #pragma unroll
       for (int u = 0; u < 3; ++u) {
-        if (q + 32 * u >= kJumpN) break;
+        in[u] = q + 32 * u < kJumpN;
         const int32_t e = p ? jr[1][u] : jr[0][u];
         const int j = l + sdelta(e);
-        const int h = jshells(e);
-        const uint8_t o = occ_s[j];
-        const int32_t r = rho_s[j];
-        const int32_t r1 = r + sm.dfq[X * 64 + h];
-        const float dF = dF32(cell32(FT, r1), cell32(FT, r), r1, r);
-        if (o != kV) {
-          const int Y = species_index(o);
-          kahan_add(acc, dF + sm.dphi32[(X * 4 + Y) * 64 + h]);
-        }
+        h[u] = jshells(e);
+        o[u] = occ_s[j];
+        r0[u] = rho_s[j];
+        r1[u] = r0[u] + sm.dfq[X * 64 + h[u]];
       }
+      bool win = true;
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        win = win && (!in[u] || (static_cast<unsigned>((r0[u] >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin) &&
+                                 static_cast<unsigned>((r1[u] >> kRhoCellShift) - FT.kw0) < static_cast<unsigned>(kFWin)));
+      float t[3];
+      if (win) {
+#pragma unroll
+        for (int u = 0; u < 3; ++u) t[u] = in[u] ? dF32(cell32win(FT, r1[u]), cell32win(FT, r0[u]), r1[u], r0[u]) : 0.f;
+      } else {
+#pragma unroll
+        for (int u = 0; u < 3; ++u) t[u] = in[u] ? dF32(cell32(FT, r1[u]), cell32(FT, r0[u]), r1[u], r0[u]) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        if (in[u] && o[u] != kV) kahan_add(acc, t[u] + sm.dphi32[(X * 4 + species_index(o[u])) * 64 + h[u]]);
     }
 #pragma unroll
     for (int m = 16; m >= 1; m >>= 1) {
@@ -491,9 +546,10 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
   } while (0)
 #endif
 
-// Hop-loop sub-phases (builds with -DAKMC_PHASE_PROFILE -DAKMC_HOP_PROFILE): thread 0 (an
+// Hop-loop sub-phases (builds with -DAKMC_PHASE_PROFILE -DAKMC_HOP_PROFILE=1): thread 0 (an
 // evaluator) adds its cycles per stage into counters 16..19, the control thread into 20..22,
-// and counts the iterations in 23.
+// and counts the iterations in 23.  With -DAKMC_HOP_PROFILE=2 thread 0's four counters split
+// the perform stage instead (HOP_P).
 #if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE)
 #define HOP_T(k)                                                                                           \
   do {                                                                                                     \
@@ -505,6 +561,25 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
   } while (0)
 #else
 #define HOP_T(k) \
+  do {           \
+  } while (0)
+#endif
+#if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE) && AKMC_HOP_PROFILE == 2
+#define HOP_P(k)                                                                       \
+  do {                                                                                 \
+    if (threadIdx.x == 0) {                                                            \
+      const long long t_ = clock64();                                                  \
+      atomicAdd(a.counters + 16 + (k), static_cast<unsigned long long>(t_ - thp));     \
+      thp = t_;                                                                        \
+    }                                                                                  \
+  } while (0)
+#undef HOP_T
+#define HOP_T(k)                                                                       \
+  do {                                                                                 \
+    if (threadIdx.x == 0) thp = clock64();                                             \
+  } while (0)
+#else
+#define HOP_P(k) \
   do {           \
   } while (0)
 #endif
@@ -787,16 +862,29 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     const int n = c ^ 1;
     const int nord = sm.nord[c];
     // [1] selection: lane 0 of every warp forms the ordered total (ABVIModel::calcRates,
-    // kmc.cpp:68-115), then runs the same running sums again to the first one above u * total
+    // kmc.cpp:68-115), then finds the first of the same running sums above u * total
     // (ABVIModel::select, kmc.cpp:242-309).  Jumps onto a vacancy hold 0.0, which leaves a
-    // positive sum unchanged.
+    // positive sum unchanged.  With one active vacancy (nearly every sector at these
+    // dilutions) the running sums of the total's pass are kept and compared afterwards,
+    // independently of one another, instead of being formed a second time.
     int isel = -1, stop = 0;
     double total = 0.0, u = 0.0;
     if (lane == 0) {
-      for (int i = 0; i < nord; ++i) {
-        const double* r = sm.rates[c][sm.ord[c][i]];
+      constexpr int kPreSel = 1;
+      double* pre = sm.presel[warp];
+      if (nord <= kPreSel) {
+        const double* r = sm.rates[c][sm.ord[c][0]];
 #pragma unroll
-        for (int bb = 0; bb < 8; ++bb) total += r[bb];
+        for (int bb = 0; bb < 8; ++bb) {
+          if (nord) total += r[bb];
+          pre[bb] = total;
+        }
+      } else {
+        for (int i = 0; i < nord; ++i) {
+          const double* r = sm.rates[c][sm.ord[c][i]];
+#pragma unroll
+          for (int bb = 0; bb < 8; ++bb) total += r[bb];
+        }
       }
       if (a.mode == kModeCalc) {
         stop = 1;
@@ -805,14 +893,23 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       } else {
         u = a.mode == kModeSelectPerform ? a.api_u : sm.ctl_u[it];
         const double expected = u * total;  // ModelAdapter::selectAndPerform
-        double acc = 0.0;
-        for (int i = 0; i < nord && isel < 0; ++i) {
-          const double* r = sm.rates[c][sm.ord[c][i]];
-          for (int bb = 0; bb < 8; ++bb) {
-            acc += r[bb];
-            if (acc > expected) {
-              isel = i * 8 + bb;
-              break;
+        if (nord <= kPreSel) {
+          double pv[8 * kPreSel];
+#pragma unroll
+          for (int q = 0; q < 8 * kPreSel; ++q) pv[q] = pre[q];
+#pragma unroll
+          for (int q = 8 * kPreSel - 1; q >= 0; --q)
+            if (q < 8 * nord && pv[q] > expected) isel = q;
+        } else {
+          double acc = 0.0;
+          for (int i = 0; i < nord && isel < 0; ++i) {
+            const double* r = sm.rates[c][sm.ord[c][i]];
+            for (int bb = 0; bb < 8; ++bb) {
+              acc += r[bb];
+              if (acc > expected) {
+                isel = i * 8 + bb;
+                break;
+              }
             }
           }
         }
@@ -855,6 +952,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     const int ngx = wrap1(sX + unpack_dx(wg), jc.sx), ngy = wrap1(sY + unpack_dy(wg), jc.sy),
               ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
     const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
+    HOP_P(0);
     if (evaluator) {
       if (hop) {
         // [2] perform (ABVIModel::perform, kmc.cpp:358-396) on the staged region, written
@@ -924,7 +1022,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
             (&sm.vX[n][0][0])[q] = (&sm.vX[c][0][0])[q];
           }
         }
+        HOP_P(1);
         asm volatile("bar.sync 1, %0;" ::"n"(kCtl) : "memory");  // the evaluator warps only
+        HOP_P(2);
         HOP_T(1);
         // [3] + [4] the vacancies within D cells of the hop's origin, evaluated into set n
         for (int base = 0; base < cnt; base += 32) {
@@ -1023,6 +1123,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
     __syncthreads();  // set n (or c), the clock's decision and the next uniform visible
     HOP_T(threadIdx.x == 0 ? 3 : 2);
+    HOP_P(3);
 #if defined(AKMC_PHASE_PROFILE) && defined(AKMC_HOP_PROFILE)
     if (tid == 0) atomicAdd(a.counters + 23, 1ull);
 #endif
@@ -1222,6 +1323,11 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
   return v;
 }
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
 
 // Rounds back to the latest earlier round of the neighbour at offset (dx, dy, dz) whose
 // region meets this round's (phase = round mod 8), 0 if none ever does.  Per dimension a
@@ -1298,13 +1404,16 @@ __device__ __forceinline__ void flow_row(const RoundArgs& a, int gb, int (&y)[28
 }
 __device__ __forceinline__ void flow_snapshot(const RoundArgs& a, int gb, const int (&y)[28], int64_t r0,
                                               int32_t (&P)[27]) {
+  // only the word's low 32 bits are read (27 registers in flight, not 54): neighbours of one job
+  // are within a few rounds of each other, so the difference taken modulo 2^31 is exact
+  const uint32_t base = static_cast<uint32_t>(r0) & 0x7fffffffu;
 #pragma unroll
   for (int o = 0; o < 27; ++o) {
     if (y[o] == gb) {
       P[o] = kAhead;
     } else {
-      const int64_t d = static_cast<int64_t>(ld_relaxed_u64(&a.fstate[y[o]]) >> 1) - r0;
-      P[o] = static_cast<int32_t>(d > kAhead ? kAhead : (d < -kAhead ? -kAhead : d));
+      const uint32_t lo = ld_relaxed_u32(reinterpret_cast<const unsigned int*>(&a.fstate[y[o]]));
+      P[o] = static_cast<int32_t>(((lo >> 1) - base) << 1) >> 1;  // sign from bit 30
     }
   }
 }
@@ -1631,7 +1740,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
 #endif
         // the sector's vacancies move: its bit of the block's sector mask goes, and comes back
         // below for each one still in the block (with the bit of the sector it is in now)
-        if (ran && tid == 0) atomicAnd(&a.vsec[gb], ~(1u << sec));
+        if (ran && tid == 0) atomicAnd(&a.vsec[gb], ~(1u << sector_of_round(r)));
         __syncthreads();
         // vacancies carried into a neighbour's area change owner (only if the round ran:
         // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
