@@ -93,6 +93,7 @@ struct akmc_ctx {
   unsigned long long* d_vclaim = nullptr;
   unsigned long long* d_vvalid = nullptr;
   int32_t* d_vslot = nullptr;
+  int32_t* d_vsite = nullptr;
   int32_t* d_vcount = nullptr;
   int32_t* d_nbr = nullptr;
   unsigned int* d_vsec = nullptr;
@@ -173,13 +174,14 @@ void free_device(akmc_ctx* ctx) {
   ctx->ev.clear();
   dfree(ctx->stream, ctx->d_vac_count);
   ctx->d_vac_count = nullptr;
-  void* flow_ptrs[] = {ctx->d_fstate, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot,
+  void* flow_ptrs[] = {ctx->d_fstate, ctx->d_vclaim, ctx->d_vvalid, ctx->d_vslot, ctx->d_vsite,
                        ctx->d_vcount, ctx->d_nbr,    ctx->d_vsec,   ctx->d_flow};
   for (void* p : flow_ptrs) dfree(ctx->stream, p);
   ctx->d_fstate = nullptr;
   ctx->d_vclaim = ctx->d_vvalid = nullptr;
   ctx->d_vslot = ctx->d_vcount = ctx->d_nbr = ctx->d_flow = nullptr;
   ctx->d_vsec = nullptr;
+  ctx->d_vsite = nullptr;
   dfree(ctx->stream, ctx->d_cl);
   dfree(ctx->stream, ctx->d_cl_misc);
   ctx->d_cl = nullptr;
@@ -785,6 +787,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(ctx->stream, &ctx->d_vclaim, ncap));
   CK(dalloc(ctx->stream, &ctx->d_vvalid, ncap));
   CK(dalloc(ctx->stream, &ctx->d_vslot, ncap * kFlowSlots));
+  CK(dalloc(ctx->stream, &ctx->d_vsite, ncap * kFlowSlots));
   CK(dalloc(ctx->stream, &ctx->d_vcount, ncap));
   CK(dalloc(ctx->stream, &ctx->d_nbr, ncap * kNbrStride));
   CK(dalloc(ctx->stream, &ctx->d_vsec, ncap));
@@ -852,6 +855,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.vclaim = ctx->d_vclaim;
   a.vvalid = ctx->d_vvalid;
   a.vslot = ctx->d_vslot;
+  a.vsite = ctx->d_vsite;
   a.vcount = ctx->d_vcount;
   a.nbr = ctx->d_nbr;
   a.vsec = ctx->d_vsec;

@@ -132,6 +132,7 @@ struct RoundArgs {
   unsigned long long* vclaim;   // per block: slots of vslot taken
   unsigned long long* vvalid;   // per block: slots of vslot holding a vacancy id
   int32_t* vslot;               // per block: kFlowSlots ids of the vacancies in its area
+  int32_t* vsite;               // per block: their sites (kept with the ids by whoever moves them)
   int32_t* vcount;              // per block: fill counter while the slots are rebuilt
   unsigned int* vsec;           // per block: bit s set while a vacancy of its area lies in sector s
   int32_t* nbr;                 // per block, kNbrStride words: the 27 neighbour blocks (offset

@@ -164,6 +164,11 @@ struct Smem {
   int32_t flow_cand[kMaxThreads];
   int32_t flow_ncand, flow_stop, flow_progress, flow_more;
   int32_t fv[kFlowSlots], fslot[kFlowSlots], fnv;  // the sector's vacancies and their slots
+  int32_t fsite[kFlowSlots];                        // their sites
+  int64_t flow_cr[kMaxThreads], flow_ct[kMaxThreads];  // round and target of each round handed over
+  int64_t cur_r, cur_t;   // the block's round and target for its next chained round
+  int64_t hops_out;       // the block's hop count after run_block
+  double pre_evo;         // the active sector's clock, read while the region's copies fly
   // device counters summed per CTA and added once when the kernel ends (per-round atomics on
   // the same addresses from every CTA queue up); hops of the current job likewise
   unsigned long long acc[6];  // counters 0 (hops), 1, 3, 4, 5, 6
@@ -514,6 +519,38 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
   if (KIND == kEam64) EVAL_T(3);
 }
 
+// Bulk staging of a region (R.bulk): the bulk-copy unit moves whole rows, R.bo occupancy bytes
+// and R.br densities from the row's 16-site boundary R.ox (unwrapped), into shared rows of pitch
+// R.LX; thread t0 + k nt issues row t0 + k nt.  A span that leaves the row [0, sx) at either end
+// goes in two pieces: sites [R.ox, cut) to shared [0, cut - R.ox) and the rest from the other
+// end of the row.  The barrier is armed for the bytes of every row (stage_bytes).
+__device__ __forceinline__ void stage_rows(const Region& R, const uint8_t* occ, const int32_t* rho, int sx, int sy, int sz,
+                                           bool eam, uint8_t* occ_s, int32_t* rho_s, uint64_t* bar, int t0, int nt) {
+  asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
+  const int nrows = R.LY * R.LZ;
+  for (int row = t0; row < nrows; row += nt) {
+    const int ly = row % R.LY, lz = row / R.LY;
+    const int gy = wrap1(R.oy + ly, sy), gz = wrap1(R.oz + lz, sz);
+    const int64_t rb = static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz);
+#pragma unroll
+    for (int arr = 0; arr < 2; ++arr) {
+      if (arr == 1 && !eam) break;
+      const int len = arr == 0 ? R.bo : R.br;  // sites of the span
+      const int es = arr == 0 ? 1 : 4;          // bytes per site
+      uint8_t* dst = arr == 0 ? occ_s + R.LX * row : reinterpret_cast<uint8_t*>(rho_s + R.LX * row);
+      const uint8_t* src = arr == 0 ? occ + rb : reinterpret_cast<const uint8_t*>(rho + rb);
+      const int n1 = R.ox < 0 ? -R.ox : min(len, sx - R.ox);  // sites up to the row's end
+      const int a1 = R.ox < 0 ? R.ox + sx : R.ox;              // row position of the first piece
+      bulk_copy(dst, src + static_cast<int64_t>(es) * a1, static_cast<uint32_t>(es * n1), bar);
+      if (len > n1) bulk_copy(dst + es * n1, src, static_cast<uint32_t>(es * (len - n1)), bar);
+    }
+  }
+}
+// Bytes the bulk staging of region R moves (the barrier's transaction count).
+__device__ __forceinline__ uint32_t stage_bytes(const Region& R, bool eam) {
+  return static_cast<uint32_t>(R.LY * R.LZ) * static_cast<uint32_t>(R.bo + (eam ? 4 * R.br : 0));
+}
+
 // Phase profile (builds with -DAKMC_PHASE_PROFILE): thread 0 accumulates the cycles
 // between consecutive CTA barriers into counters[8 + phase].
 #ifdef AKMC_PHASE_PROFILE
@@ -594,7 +631,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
 // the vacancy arrays of sm were not filled.
 template <int KIND, int W>
 __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, int32_t* rho_s,
-                          const int32_t* vlist, int cnt_in, int64_t round_now) {
+                          const int32_t* vlist, int cnt_in, int64_t round_now, bool flowpre = false) {
   AKMC_SHAPE(W);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -612,11 +649,24 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   // the block record, the lattice and the vacancy table are read at L2 (__ldcg): under the
   // asynchronous schedule another SM may have written them since this SM last looked
   const int sec = a.mode == kModeRound ? sector_of_round(round_now) : a.api_sector;
+  // flowpre (k_flow): the caller issued a bulk region's copies on mbar_st already, and left the
+  // sector's clock (sm.pre_evo), the streams (sm.xs, sm.xt) and the vacancies' sites (sm.fsite)
+  // in shared memory, read while the copies were in flight
   double thr = 0.0;
   if (a.mode == kModeRound) {
     const int64_t step = round_now >> 3;
-    thr = static_cast<double>(step + 1) * J.window - __ldcg(&B.evo[sec]);
-    if (!(0.0 < thr)) return false;  // sector_time stays 0 (sublattice.inl:82)
+    thr = static_cast<double>(step + 1) * J.window - (flowpre ? sm.pre_evo : __ldcg(&B.evo[sec]));
+    if (!(0.0 < thr)) {  // sector_time stays 0 (sublattice.inl:82)
+      if (flowpre && tid == kCtl) {  // copies already issued complete first: the buffer is reused next
+        Region R0;
+        make_region(B, J, sec, R0);
+        if (R0.bulk) {
+          if (mbar_wait(&sm.mbar_st, sm.mbst_phase)) sm.mbst_phase ^= 1u;
+          else atomicOr(a.status, kErrTimeout);
+        }
+      }
+      return false;
+    }
   }
   JobC jc;
   jc.occ = J.occ;
@@ -636,8 +686,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   const int tab0 = J.pot * 4 + KIND, tab1 = R.LX | (R.LY << 16);
   const bool need_tab = sm.tab_key[0] != tab0 || sm.tab_key[1] != tab1;
   const int nrows = R.LY * R.LZ;
-  if (R.bulk && tid == kCtl)  // armed before any copy is issued (after the barrier below)
-    bulk_expect(&sm.mbar_st, static_cast<uint32_t>(nrows) * static_cast<uint32_t>(R.bo + (eam ? 4 * R.br : 0)));
+  if (R.bulk && !flowpre && tid == kCtl)  // armed before any copy is issued (after the barrier below)
+    bulk_expect(&sm.mbar_st, stage_bytes(R, eam));
   __syncthreads();  // every thread has read win_pot and tab_key; the previous item's readers are done
   AKMC_STAGE_T(0);
   if (need_win && tid == kCtl) {
@@ -711,36 +761,14 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         }
       }
     }
-  } else {
-    // the bulk-copy unit moves whole rows: R.bo occupancy bytes and R.br densities from the
-    // row's 16-site boundary R.ox (unwrapped), into shared rows of pitch R.LX; thread t issues
-    // row t.  A span that leaves the row [0, sx) at either end goes in two pieces: sites
-    // [R.ox, cut) to shared [0, cut - R.ox) and the rest from the other end of the row.
-    asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
-    const int sx = jc.sx;
-    for (int row = tid; row < nrows; row += kThreads) {
-      const int ly = row % R.LY, lz = row / R.LY;
-      const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
-      const int64_t rb = static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(jc.sy) * gz);
-#pragma unroll
-      for (int arr = 0; arr < 2; ++arr) {
-        if (arr == 1 && !eam) break;
-        const int len = arr == 0 ? R.bo : R.br;  // sites of the span
-        const int es = arr == 0 ? 1 : 4;          // bytes per site
-        uint8_t* dst = arr == 0 ? occ_s + R.LX * row : reinterpret_cast<uint8_t*>(rho_s + R.LX * row);
-        const uint8_t* src = arr == 0 ? jc.occ + rb : reinterpret_cast<const uint8_t*>(jc.rho + rb);
-        const int n1 = R.ox < 0 ? -R.ox : min(len, sx - R.ox);  // sites up to the row's end
-        const int a1 = R.ox < 0 ? R.ox + sx : R.ox;              // row position of the first piece
-        bulk_copy(dst, src + static_cast<int64_t>(es) * a1, static_cast<uint32_t>(es * n1), &sm.mbar_st);
-        if (len > n1) bulk_copy(dst + es * n1, src, static_cast<uint32_t>(es * (len - n1)), &sm.mbar_st);
-      }
-    }
+  } else if (!flowpre) {
+    stage_rows(R, jc.occ, jc.rho, jc.sx, jc.sy, jc.sz, eam, occ_s, rho_s, &sm.mbar_st, tid, kThreads);
   }
   AKMC_STAGE_T(2);
   const int cnt = cnt_in;
   if (tid < cnt) {
     const int v = vlist[tid];
-    const int s = __ldcg(&a.vac_site[v]);
+    const int s = flowpre ? sm.fsite[tid] : __ldcg(&a.vac_site[v]);
     const int X = s % jc.sx;
     const int t = s / jc.sx;
     const int y = t % jc.sy;
@@ -773,9 +801,13 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.nord[0] = cnt;
     uint64_t x[4];
     for (int i = 0; i < 4; ++i) {
-      x[i] = __ldcg(&B.xs[i]);
-      sm.xs[i] = x[i];
-      sm.xt[i] = __ldcg(&B.xt[i]);
+      if (flowpre) {
+        x[i] = sm.xs[i];
+      } else {
+        x[i] = __ldcg(&B.xs[i]);
+        sm.xs[i] = x[i];
+        sm.xt[i] = __ldcg(&B.xt[i]);
+      }
     }
     // the first selection's uniform, drawn ahead; the stream moves on only if a selection uses it
     sm.ctl_u[0] = a.mode == kModeRound ? uniform_co(x) : 0.0;
@@ -1144,6 +1176,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
     B.hops = hop0 + nh;
+    sm.hops_out = hop0 + nh;
     if (sm.acc_job != B.job) {
       if (sm.acc_job >= 0 && sm.acc_job_hops)
         atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[sm.acc_job].hops), sm.acc_job_hops);
@@ -1463,7 +1496,7 @@ __device__ __noinline__ int owner_sector(const JobDev& J, int32_t s, int* sec) {
 }
 
 // Puts vacancy v into block o's slots: claim a free slot, write the id, then mark it valid.
-__device__ void flow_give(const RoundArgs& a, int o, int v, int osec) {
+__device__ void flow_give(const RoundArgs& a, int o, int v, int32_t site, int osec) {
   for (int tries = 0; tries < 4 * kFlowSlots; ++tries) {
     const unsigned long long m = *reinterpret_cast<volatile unsigned long long*>(&a.vclaim[o]);
     if (m == ~0ull) break;
@@ -1471,6 +1504,7 @@ __device__ void flow_give(const RoundArgs& a, int o, int v, int osec) {
     const unsigned long long bit = 1ull << slot;
     if (atomicOr(&a.vclaim[o], bit) & bit) continue;  // taken meanwhile
     a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
+    a.vsite[static_cast<int64_t>(o) * kFlowSlots + slot] = site;
     fence_acq_rel();
     atomicOr(&a.vvalid[o], bit);
     atomicOr(&a.vsec[o], 1u << osec);
@@ -1501,7 +1535,7 @@ __device__ __forceinline__ void flow_publish(const RoundArgs& a, int gb, int64_t
 // target (by running rounds, or by a budget moving the target down to r0); false for a block
 // that was at its target already (a stale sweep read).
 __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, int gb, const int8_t (*lag)[27],
-                             int64_t r0, const int32_t (*Pin)[27], int64_t* rn, bool* reached) {
+                             int64_t r0, const int32_t (*Pin)[27], int64_t* rn, bool* reached, int64_t* tgt) {
   *rn = r0;
   *reached = false;
   // one round of loads, all in flight together: the target, the job's constants, the block's
@@ -1516,6 +1550,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
   for (int k = 0; k < 8; ++k) evo[k] = __ldcg(&B.evo[k]);
   // sectors holding a vacancy (the slots' sector mask)
   unsigned occ_sec = __ldcg(&a.vsec[gb]);
+  *tgt = t_old;
   if (r0 >= t_old) return false;
   // a single-block job with a hop budget ends at the end of the first time step at which its
   // hops reached the budget: once they have, its target moves down to the next boundary at or
@@ -1529,6 +1564,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
       B.budget_end = 1;
     }
   }
+  *tgt = target;
   if (r0 >= target) {
     *reached = true;
     return false;
@@ -1560,6 +1596,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
       B.target = r;
       B.budget_end = 1;
       target = r;
+      *tgt = r;
       break;
     }
     const int sec = sector_of_round(r);
@@ -1585,6 +1622,7 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
   }
   *rn = r;
   *reached = r == target;  // the lease holder alone moves the target
+  *tgt = target;
   return stop_full;
 }
 
@@ -1658,13 +1696,15 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
       if (ok && atomicCAS(&a.fstate[gb], w, w | 1ull) == w) {
         fence_acq_rel();
         const JobDev& J = a.jobs[bj];
-        int64_t rn = r;
+        int64_t rn = r, tgt = 0;
         int keep = 0;
         bool reached = false;
-        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &P, &rn, &reached)) {
+        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &P, &rn, &reached, &tgt)) {
           const int i = atomicAdd(&sm0->flow_ncand, 1);
           if (i < kFlowTake) {
             sm0->flow_cand[i] = gb;
+            sm0->flow_cr[i] = rn;
+            sm0->flow_ct[i] = tgt;
             keep = 1;
           }
         }
@@ -1696,6 +1736,8 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
     const int ncand = min(sm0->flow_ncand, kFlowTake);
     for (int c = 0; c < ncand; ++c) {
       const int gb = sm0->flow_cand[c];
+      // the round and target the sweep left (a chained round: the previous link's)
+      int64_t r = sm0->flow_cr[c], target = sm0->flow_ct[c];
       for (int link = 0;; ++link) {
 #ifdef AKMC_PHASE_PROFILE
         long long tw = clock64();
@@ -1705,7 +1747,6 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         // the thread that found this round ready read the neighbours' round counters and then
         // fenced (an acquire), and a CTA barrier followed: every thread's reads come after the
         // rounds it waits for (shared data is read at L2)
-        const int64_t r = static_cast<int64_t>(ld_acquire_u64(&a.fstate[gb]) >> 1);
         const int sec = sector_of_round(r);
         Region R;
         make_region(B, J, sec, R);
@@ -1714,16 +1755,29 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         int32_t* rho_s;
         carve(smem, R.n, sm, occ_s, rho_s);
         if (tid == 0) sm->fnv = 0;
-        __syncthreads();
+        if (R.bulk && tid == kCtl) bulk_expect(&sm->mbar_st, stage_bytes(R, KIND != kPairBond));
+        __syncthreads();  // the previous round's readers are done; the copies' barrier is armed
+        // the region's bulk copies first: the slots, clocks and streams are read while they fly
+        if (R.bulk) stage_rows(R, J.occ, J.rho, J.sx, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
         if (tid < kFlowSlots) {
           const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
           if ((m >> tid) & 1ull) {
             const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + tid]);
-            if (site_in_sector(B, J, sec, __ldcg(&a.vac_site[v]))) {
+            const int32_t st = __ldcg(&a.vsite[static_cast<int64_t>(gb) * kFlowSlots + tid]);
+            if (site_in_sector(B, J, sec, st)) {
               const int i = atomicAdd(&sm->fnv, 1);
               sm->fv[i] = v;
+              sm->fsite[i] = st;
               sm->fslot[i] = tid;
             }
+          }
+        } else if (tid == kCtl) {
+          sm->hops_out = __ldcg(&B.hops);  // run_block replaces it if the round runs
+          sm->pre_evo = __ldcg(&B.evo[sec]);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            sm->xs[i] = __ldcg(&B.xs[i]);
+            sm->xt[i] = __ldcg(&B.xt[i]);
           }
         }
         __syncthreads();
@@ -1734,7 +1788,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           tw = clock64();
         }
 #endif
-        const bool ran = run_block<KIND, W>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt, r);
+        const bool ran = run_block<KIND, W>(a, gb, *sm, occ_s, rho_s, sm->fv, cnt, r, true);
 #ifdef AKMC_PHASE_PROFILE
         if (tid == 0) tw = clock64();
 #endif
@@ -1745,22 +1799,24 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         // vacancies carried into a neighbour's area change owner (only if the round ran:
         // otherwise nothing moved and the vacancy arrays of sm hold another round's data)
         if (ran && tid < cnt) {
-          // a vacancy still inside the block's area keeps its owner; only one that left it
-          // needs the owner lookup
+          // a vacancy still inside the block's area keeps its owner and slot (its site updated);
+          // only one that left it needs the owner lookup
           const int f = sm->fin;
           const int cx = sm->vgx[f][tid] >> 1, cy = sm->vgy[f][tid], cz = sm->vgz[f][tid];
           const bool inside = cx >= B.c0[0] && cx < B.c1[0] && cy >= B.c0[1] && cy < B.c1[1] && cz >= B.c0[2] &&
                               cz < B.c1[2];
+          const int32_t site = sm->vlid[f][tid];
           int osec = 0, o = gb;
           if (inside)
             osec = (cx - B.c0[0] >= (B.c1[0] - B.c0[0]) / 2 ? 1 : 0) | (cy - B.c0[1] >= (B.c1[1] - B.c0[1]) / 2 ? 2 : 0) |
                    (cz - B.c0[2] >= (B.c1[2] - B.c0[2]) / 2 ? 4 : 0);
           else
-            o = owner_sector(J, sm->vlid[f][tid], &osec);
+            o = owner_sector(J, site, &osec);
           if (o == gb) {
+            a.vsite[static_cast<int64_t>(gb) * kFlowSlots + sm->fslot[tid]] = site;
             atomicOr(&a.vsec[gb], 1u << osec);
           } else {
-            flow_give(a, o, sm->vidx[tid], osec);
+            flow_give(a, o, sm->vidx[tid], site, osec);
             const unsigned long long bit = 1ull << sm->fslot[tid];
             atomicAnd(&a.vvalid[gb], ~bit);
             fence_acq_rel();
@@ -1772,22 +1828,25 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
 #ifdef AKMC_FLOW_PROFILE
           const long long q0 = clock64();
 #endif
-          // round r ran (it was below the target when handed over)
-          int64_t rn = r + 1;
-          if ((rn & 7) == 0) B.hops_at[(rn >> 3) & 1] = __ldcg(&B.hops);
-          bool more = false, reached = rn >= __ldcg(&B.target);
+          // round r ran (it was below the target when handed over); the target is the lease
+          // holder's to move, and it is this CTA
+          int64_t rn = r + 1, tgt = target;
+          if ((rn & 7) == 0) B.hops_at[(rn >> 3) & 1] = sm->hops_out;
+          bool more = false, reached = rn >= target;
           const bool in_time =
               a.time_budget_ns <= 0 || globaltimer_ns() - t_begin < static_cast<uint64_t>(a.time_budget_ns);
           if (!reached && J.nblocks == 1 && c + 1 == ncand && in_time) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
             // -- when no other round this CTA took in the sweep is waiting for it
-            more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, nullptr, &rn, &reached);
+            more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, nullptr, &rn, &reached, &tgt);
           }
 #ifdef AKMC_FLOW_PROFILE
           const long long q1 = clock64();
 #endif
           sm->flow_progress = 1;
           sm->flow_more = more;
+          sm->cur_r = rn;
+          sm->cur_t = tgt;
           flow_publish(a, gb, rn, more ? 1 : 0, reached, KIND);
 #ifdef AKMC_FLOW_PROFILE
           atomicAdd(a.counters + 20, static_cast<unsigned long long>(q1 - q0));
@@ -1803,6 +1862,8 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         }
 #endif
         if (!sm0->flow_more) break;
+        r = sm0->cur_r;
+        target = sm0->cur_t;
       }
     }
 #ifdef AKMC_PHASE_PROFILE
@@ -1871,6 +1932,7 @@ __global__ void k_flow_slots(RoundArgs a) {
     return;
   }
   a.vslot[static_cast<int64_t>(o) * kFlowSlots + slot] = v;
+  a.vsite[static_cast<int64_t>(o) * kFlowSlots + slot] = a.vac_site[v];
   atomicOr(&a.vclaim[o], 1ull << slot);
   atomicOr(&a.vvalid[o], 1ull << slot);
   atomicOr(&a.vsec[o], 1u << osec);
