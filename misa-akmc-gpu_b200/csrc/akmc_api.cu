@@ -250,9 +250,26 @@ int region_sites(const HostJob& j, bool bulk) {
   return static_cast<int>(mx);
 }
 
-// Bulk staging needs lattice rows of a multiple of 16 sites: then every row of a region
-// starts at the same offset from a 16-byte boundary, in the occupancy and density arrays alike.
-bool bulk_rows(const HostJob& j) { return (2 * j.cfg.box[0]) % 16 == 0; }
+// Bulk staging works for every job: the device lattice's rows carry a periodic halo and a pitch
+// of a multiple of 16 sites (lattice_pitch), so a region's rows start on 16-byte boundaries.
+bool bulk_rows(const HostJob&) { return true; }
+
+// Plain copies between a job's host lattice (rows of sx entries) and the main part of its device
+// rows (pitch px, after the kHaloL halo entries); a host-to-device copy refreshes the halos.
+template <typename T>
+cudaError_t lattice_upload(T* dev, const T* host, int64_t sx, int64_t nrows, cudaStream_t st) {
+  const int64_t px = lattice_pitch(static_cast<int32_t>(sx));
+  cudaError_t e = cudaMemcpy2DAsync(dev + kHaloL, static_cast<size_t>(px) * sizeof(T), host, static_cast<size_t>(sx) * sizeof(T),
+                                    static_cast<size_t>(sx) * sizeof(T), static_cast<size_t>(nrows), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  return static_cast<cudaError_t>(launch_fill_halo(dev, static_cast<int32_t>(sx), nrows, st));
+}
+template <typename T>
+cudaError_t lattice_download(T* host, const T* dev, int64_t sx, int64_t nrows, cudaStream_t st) {
+  const int64_t px = lattice_pitch(static_cast<int32_t>(sx));
+  return cudaMemcpy2DAsync(host, static_cast<size_t>(sx) * sizeof(T), dev + kHaloL, static_cast<size_t>(px) * sizeof(T),
+                           static_cast<size_t>(sx) * sizeof(T), static_cast<size_t>(nrows), cudaMemcpyDeviceToHost, st);
+}
 
 // Restart snapshot layout: SnapHeader, then one SnapBlock per domain block, then the
 // occupancy bytes.  All fields little-endian, as the host writes them.
@@ -523,13 +540,18 @@ akmc_status upload_pot(akmc_ctx* ctx, size_t i, Potential& hp) {
 // JobDev, its blocks and its slice of the vacancy table (sites in id order), for slot ji.
 akmc_status setup_job(akmc_ctx* ctx, int32_t ji, JobDev& J, BlockDev* hb, int32_t* vsite, int32_t* vjob) {
   HostJob& j = ctx->jobs[static_cast<size_t>(ji)];
-  CK(dalloc(ctx->stream, &j.d_occ, static_cast<size_t>(j.nsites)));
-  CK(cudaMemcpyAsync(j.d_occ, j.occ.data(), static_cast<size_t>(j.nsites), cudaMemcpyHostToDevice, ctx->stream));
-  if (j.has_eam) CK(dalloc(ctx->stream, &j.d_rho, static_cast<size_t>(j.nsites)));
+  const int32_t sx = 2 * static_cast<int32_t>(j.cfg.box[0]);
+  const int64_t nrows = j.cfg.box[1] * j.cfg.box[2];
+  const size_t entries = static_cast<size_t>(lattice_entries(sx, static_cast<int32_t>(j.cfg.box[1]),
+                                                             static_cast<int32_t>(j.cfg.box[2])));
+  CK(dalloc(ctx->stream, &j.d_occ, entries));
+  CK(lattice_upload(j.d_occ, j.occ.data(), sx, nrows, ctx->stream));
+  if (j.has_eam) CK(dalloc(ctx->stream, &j.d_rho, entries));
   std::memset(&J, 0, sizeof(J));
   J.occ = j.d_occ;
   J.rho = j.d_rho;
-  J.bulk = ctx->bulk_ok && (2 * j.cfg.box[0]) % 16 == 0 && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
+  J.px = lattice_pitch(sx);
+  J.bulk = ctx->bulk_ok && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
            (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
   for (int d = 0; d < 3; ++d) {
     J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
@@ -980,8 +1002,9 @@ AKMC_API akmc_status akmc_load_occupancy(akmc_ctx* ctx, int32_t job, const uint8
   HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_sites != j.nsites) return fail(ctx, AKMC_EINVAL, "n_sites does not match the job");
   CK(cudaSetDevice(ctx->cfg.device));
-  CK(cudaMemcpyAsync(j.d_occ, occ, static_cast<size_t>(n_sites), cudaMemcpyHostToDevice, ctx->stream));
-  int e = launch_collect_vacancies(j.d_occ, n_sites, ctx->d_vac_site + j.vac0, ctx->d_vac_job + j.vac0, job,
+  const int32_t sx = 2 * static_cast<int32_t>(j.cfg.box[0]);
+  CK(lattice_upload(j.d_occ, occ, sx, j.cfg.box[1] * j.cfg.box[2], ctx->stream));
+  int e = launch_collect_vacancies(j.d_occ, n_sites, sx, ctx->d_vac_site + j.vac0, ctx->d_vac_job + j.vac0, job,
                                    static_cast<int32_t>(j.nvac), ctx->d_vac_count, ctx->d_status, ctx->stream);
   if (e) return fail(ctx, AKMC_ECUDA, std::string("collect vacancies: ") + cuda_name(e));
   if (j.has_eam) {
@@ -1019,7 +1042,7 @@ AKMC_API akmc_status akmc_save_snapshot(akmc_ctx* ctx, int32_t job, uint8_t* buf
   CK(cudaMemcpyAsync(&J, ctx->d_jobs + job, sizeof(J), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(B.data(), ctx->d_blocks + j.block0, B.size() * sizeof(BlockDev), cudaMemcpyDeviceToHost,
                      ctx->stream));
-  CK(cudaMemcpyAsync(occ, j.d_occ, static_cast<size_t>(j.nsites), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(lattice_download(occ, j.d_occ, 2 * j.cfg.box[0], j.cfg.box[1] * j.cfg.box[2], ctx->stream));
   const akmc_status st = akmc_sync(ctx);  // also the last run's errors
   if (st != AKMC_OK) return st;
   for (int32_t b = 0; b < j.nblocks; ++b) {
@@ -1492,7 +1515,7 @@ AKMC_API akmc_status akmc_get_occupancy(akmc_ctx* ctx, int32_t job, uint8_t* out
     std::memcpy(out, j.occ.data(), static_cast<size_t>(n_sites));
     return AKMC_OK;
   }
-  CK(cudaMemcpyAsync(out, j.d_occ, static_cast<size_t>(n_sites), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(lattice_download(out, j.d_occ, 2 * j.cfg.box[0], j.cfg.box[1] * j.cfg.box[2], ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return AKMC_OK;
 }
@@ -1503,7 +1526,7 @@ AKMC_API akmc_status akmc_get_rho(akmc_ctx* ctx, int32_t job, int32_t* out, int6
   const HostJob& j = ctx->jobs[static_cast<size_t>(job)];
   if (n_sites != j.nsites || !j.has_eam) return AKMC_EINVAL;
   if (!ctx->prepared) return fail(ctx, AKMC_ESTATE, "akmc_prepare first");
-  CK(cudaMemcpyAsync(out, j.d_rho, static_cast<size_t>(n_sites) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(lattice_download(out, j.d_rho, 2 * j.cfg.box[0], j.cfg.box[1] * j.cfg.box[2], ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return AKMC_OK;
 }
@@ -1660,6 +1683,7 @@ AKMC_API akmc_status akmc_job_cluster_stats(akmc_ctx* ctx, int32_t job, int64_t*
   c.occ = j.d_occ;
   c.ns = j.nsites;
   c.sx = 2 * static_cast<int32_t>(j.cfg.box[0]);
+  c.px = lattice_pitch(c.sx);
   c.sy = static_cast<int32_t>(j.cfg.box[1]);
   c.sz = static_cast<int32_t>(j.cfg.box[2]);
   c.bins = hist_len > 0 ? static_cast<int32_t>(hist_len) : 1;

@@ -49,27 +49,34 @@ __device__ __forceinline__ uint32_t cu_bytes(uint32_t w) {
   return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
 }
 
-// Thread t of the grid reads the 16 sites [16 t, 16 t + 16); the warp takes list slots with one
-// atomic.
-__global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int32_t* list, unsigned int* n_list,
-                             int32_t* parent, int32_t* size) {
+// Thread t of the grid reads 16 sites of one row (the lattice's halo layout: rows of pitch px,
+// the row's sites from entry kHaloL on); the warp takes list slots with one atomic.
+__global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int sx, int px, int32_t* list,
+                             unsigned int* n_list, int32_t* parent, int32_t* size) {
   const int lane = threadIdx.x & 31;
-  const int64_t nvec = (ns + 15) / 16;
+  const int vpr = (sx + 15) / 16;  // vectors per row
+  const int64_t nvec = (ns / sx) * vpr;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  const uint4* v = reinterpret_cast<const uint4*>(occ);
   for (int64_t w0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x - lane); w0 < nvec;
        w0 += warps * 32) {
     const int64_t i = w0 + lane;
     uint32_t m[4] = {0, 0, 0, 0};
-    if (i * 16 + 16 <= ns) {
-      const uint4 w = __ldg(v + i);
+    int64_t s0 = 0;
+    if (i < nvec) {
+      const int64_t row = i / vpr;
+      const int k = static_cast<int>(i - row * vpr);
+      s0 = row * sx + 16 * k;
+      const uint4 w = __ldg(reinterpret_cast<const uint4*>(occ + row * px + kHaloL + 16 * k));
       m[0] = cu_bytes(w.x);
       m[1] = cu_bytes(w.y);
       m[2] = cu_bytes(w.z);
       m[3] = cu_bytes(w.w);
-    } else if (i < nvec) {  // the last ns % 16 sites, byte by byte
-      for (int k = 0; i * 16 + k < ns; ++k)
-        if (occ[i * 16 + k] == kCuCode) m[k >> 2] |= 0x80u << (8 * (k & 3));
+      const int valid = sx - 16 * k;  // the row's last vector reaches into its halo
+      if (valid < 16)
+        for (int q = 0; q < 4; ++q) {
+          const int keep = min(max(valid - 4 * q, 0), 4);
+          m[q] &= keep == 4 ? 0xffffffffu : ((1u << (8 * keep)) - 1u);
+        }
     }
     const int cnt = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
     int pre = cnt;  // inclusive prefix over the warp
@@ -85,7 +92,7 @@ __global__ void k_cu_collect(const uint8_t* __restrict__ occ, int64_t ns, int32_
     for (int k = 0; k < 4; ++k) {
       uint32_t z = m[k];
       while (z) {
-        const int64_t s = i * 16 + k * 4 + ((__ffs(static_cast<int>(z)) - 1) >> 3);
+        const int64_t s = s0 + k * 4 + ((__ffs(static_cast<int>(z)) - 1) >> 3);
         z &= z - 1;
         parent[s] = static_cast<int32_t>(s);
         size[s] = 0;
@@ -107,7 +114,7 @@ __device__ __forceinline__ int32_t find_root(int32_t* parent, int32_t x, unsigne
   return x;
 }
 
-__global__ void k_cu_union(const uint8_t* __restrict__ occ, int sx, int sy, int sz, const int32_t* list,
+__global__ void k_cu_union(const uint8_t* __restrict__ occ, int sx, int sy, int sz, int px, const int32_t* list,
                            const unsigned int* n_list, int32_t* parent, unsigned long long* iso,
                            unsigned int* status) {
   const int lane = threadIdx.x & 31;
@@ -120,7 +127,8 @@ __global__ void k_cu_union(const uint8_t* __restrict__ occ, int sx, int sy, int 
     unsigned cu = 0;  // bit b: first neighbour b is Cu
 #pragma unroll
     for (int b = 0; b < 8; ++b)
-      if (s >= 0 && __ldg(occ + nn1_site(s, b, sx, sy, sz)) == kCuCode) cu |= 1u << b;
+      if (s >= 0 && __ldg(occ + lattice_index(static_cast<int32_t>(nn1_site(s, b, sx, sy, sz)), sx, px)) == kCuCode)
+        cu |= 1u << b;
     const int isolated = __reduce_add_sync(kFull, s >= 0 && cu == 0 ? 1 : 0);
     if (lane == 0 && isolated) atomicAdd(iso, static_cast<unsigned long long>(isolated));
 #pragma unroll 1
@@ -187,12 +195,12 @@ int launch_cluster_stats(const ClusterArgs& c, void* stream) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c.iso, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(c.hist, 0, sizeof(unsigned long long) * c.bins, st);
   if (e != cudaSuccess) return static_cast<int>(e);
-  const int64_t nvec = (c.ns + 15) / 16;
+  const int64_t nvec = (c.ns / c.sx) * ((c.sx + 15) / 16);
   int grid = static_cast<int>(std::min<int64_t>((nvec + 255) / 256, 148 * 16));
   if (grid < 1) grid = 1;
-  k_cu_collect<<<grid, 256, 0, st>>>(c.occ, c.ns, c.list, c.n_list, c.parent, c.size);
+  k_cu_collect<<<grid, 256, 0, st>>>(c.occ, c.ns, c.sx, c.px, c.list, c.n_list, c.parent, c.size);
   const int g2 = 148 * 8;
-  k_cu_union<<<g2, 256, 0, st>>>(c.occ, c.sx, c.sy, c.sz, c.list, c.n_list, c.parent, c.iso, c.status);
+  k_cu_union<<<g2, 256, 0, st>>>(c.occ, c.sx, c.sy, c.sz, c.px, c.list, c.n_list, c.parent, c.iso, c.status);
   k_cu_size<<<g2, 256, 0, st>>>(c.list, c.n_list, c.parent, c.size, c.status);
   k_cu_hist<<<g2, 256, sizeof(unsigned long long) * c.bins, st>>>(c.list, c.n_list, c.parent, c.size, c.hist,
                                                                    c.bins);

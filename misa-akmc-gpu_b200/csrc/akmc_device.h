@@ -59,11 +59,41 @@ struct Potential {
 // outside the window are read from global memory (same values, slower).
 constexpr int kFWin = 1024;
 
+// Device lattice layout.  Each x row of a job (sx sites) is stored with a periodic halo:
+// kHaloL sites on its left hold copies of the row's last sites, kHaloR on its right copies of its
+// first ones, in a row of lattice_pitch(sx) entries (a multiple of 16).  Site (x, y, z) sits at
+// kHaloL + x + pitch (y + sy z), and every write of a site writes its halo copies too
+// (lattice_put), so a span of a row from x = -kHaloL to x = sx + kHaloR is contiguous: a sector
+// region's row, rounded out to 16-site boundaries, is one aligned bulk copy whatever the box.
+// Position p of a row (0 <= p < kHaloL + sx + kHaloR) holds site (p - kHaloL) mod sx; the rest
+// of the pitch is padding.
+constexpr int kHaloL = 16, kHaloR = 32;
+AK_HD int32_t lattice_pitch(int32_t sx) { return (kHaloL + sx + kHaloR + 15) & ~15; }
+AK_HD int64_t lattice_entries(int32_t sx, int32_t sy, int32_t sz) {
+  return static_cast<int64_t>(lattice_pitch(sx)) * sy * sz;
+}
+// Entry of site id s = x + sx (y + sy z).
+AK_HD int64_t lattice_index(int32_t s, int32_t sx, int32_t px) {
+  return kHaloL + s % sx + static_cast<int64_t>(px) * (s / sx);
+}
+// Writes site x of a row (row = the row's first entry) and its halo copies: only sites within
+// kHaloR of the row's start or kHaloL of its end have one (rows shorter than the halo, several).
+template <typename T>
+AK_HD void lattice_put(T* row, int32_t sx, int32_t x, T v) {
+  row[kHaloL + x] = v;
+  if (x < kHaloR || x >= sx - kHaloL) {
+    for (int p = kHaloL + x - sx; p >= 0; p -= sx) row[p] = v;
+    for (int p = kHaloL + x + sx; p < kHaloL + sx + kHaloR; p += sx) row[p] = v;
+  }
+}
+
 struct JobDev {
-  uint8_t* occ;
-  int32_t* rho;
+  uint8_t* occ;       // lattice_entries(sx, sy, sz) occupancy codes, halo layout
+  int32_t* rho;       // the same layout, densities
   int32_t n[3];       // cells
   int32_t sx, sy, sz; // sites per dimension (sx = 2 n[0])
+  int32_t px;         // row pitch of the device lattice (lattice_pitch(sx))
+  int32_t pad_px;
   int32_t nb[3];      // domain blocks per dimension
   int32_t block0;     // first global block
   int32_t nblocks;
@@ -163,8 +193,11 @@ int hop_ctas_per_sm(int eval_warps);  // CTAs of the hop kernels the register bu
 int launch_round(const RoundArgs& a, int hop_grid, size_t smem, void* stream, void* ev0, void* ev1);
 // Collects the vacancies of one job's lattice into its slice of the vacancy table and sets
 // kErrVacCount in *status unless exactly cap were found.
-int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
-                             int32_t cap, int32_t* count, unsigned int* status, void* stream);
+int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t sx, int32_t* vac_site, int32_t* vac_job,
+                             int32_t job, int32_t cap, int32_t* count, unsigned int* status, void* stream);
+// Refreshes the halo entries of every row of a lattice (halo layout, rows of sx sites).
+int launch_fill_halo(uint8_t* lat, int32_t sx, int64_t nrows, void* stream);
+int launch_fill_halo(int32_t* lat, int32_t sx, int64_t nrows, void* stream);
 int launch_api(const RoundArgs& a, size_t smem, void* stream);
 int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, const Potential* pot,
                     const Geometry* geo, unsigned int* status, void* stream);
@@ -200,9 +233,10 @@ int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream);
 // Cu cluster statistics of one job's occupancy (akmc_cluster.cu).  list, parent and size hold
 // one int32 per site; iso and hist are cleared by the launch.
 struct ClusterArgs {
-  const uint8_t* occ;
+  const uint8_t* occ;  // halo layout
   int64_t ns;
   int32_t sx, sy, sz, bins;
+  int32_t px, pad;
   int32_t* list;
   unsigned int* n_list;
   int32_t* parent;

@@ -27,6 +27,13 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kStageRows = 4;  // rows of the staged region each warp has in flight
+// Blocks a k_flow thread may visit per sweep, until it takes one.  Measured on the 256^3 lattice
+// and the 512 batched boxes: 2 and 3 cost 1.7% and 4.5% on the 256^3 lattice and gain nothing
+// on the batched boxes.
+#ifndef AKMC_SWEEP_VISITS
+#define AKMC_SWEEP_VISITS 1
+#endif
+constexpr int kSweepVisits = AKMC_SWEEP_VISITS;
 enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };  // energy kinds, one kernel instance each
 // CTA shape: W warps evaluate the 8 jump directions (warp w takes jumps w, w + W, ...), one
 // more warp controls the hop loop.  The hop kernels are built for W = 8 (one jump per warp) and
@@ -105,7 +112,9 @@ __device__ __forceinline__ void make_region(const BlockDev& B, const JobDev& J, 
     const int x0 = R.ox & ~15;  // rounds down, negative origins included
     const int xo = R.ox - x0;
     const int bo = (xo + R.LXt + 15) & ~15;
-    if (bo <= J.sx) {
+    // the span [x0, x0 + bo) lies inside the row and its halo (always, for blocks of >= 8 cells:
+    // x0 >= -16 and x0 + bo <= sx + 19)
+    if (x0 >= -kHaloL && x0 + bo <= J.sx + kHaloR) {
       R.xo = xo;
       R.ox = x0;
       R.LX = (R.LXt + 14 + 15) & ~15;  // one pitch for every alignment: tables stay valid
@@ -168,6 +177,11 @@ struct Smem {
   int64_t flow_cr[kMaxThreads], flow_ct[kMaxThreads];  // round and target of each round handed over
   int64_t cur_r, cur_t;   // the block's round and target for its next chained round
   int64_t hops_out;       // the block's hop count after run_block
+  // run_block's control thread: hops at the start, hops, n_act sum and evaluations of the
+  // block-round, the sector's clock and its threshold
+  int64_t c_hop0, c_nh, c_nact, c_evals;
+  double c_time, c_thr;
+  double c_nu, c_kT;  // the job's attempt frequency and kT (the rates' constants)
   double pre_evo;         // the active sector's clock, read while the region's copies fly
   // device counters summed per CTA and added once when the kernel ends (per-round atomics on
   // the same addresses from every CTA queue up); hops of the current job likewise
@@ -214,12 +228,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
 struct FTab {
   const unsigned char* win;
   int kw0;
-  const double2* g64lo;
-  const double2* g64hi;
-  const float4* g32a;
-  const float* g32b;
+  const Potential* pot;      // the full tables (far cells), read on the rare path only
   unsigned int* status;
-  unsigned long long* prof;  // sub-phase cycles of the evaluation (profiling builds)
+#ifdef AKMC_PHASE_PROFILE
+  unsigned long long* prof;  // sub-phase cycles of the evaluation
+#endif
 };
 
 // Job constants of the running block, held in registers (the job record sits in global
@@ -227,8 +240,7 @@ struct FTab {
 struct JobC {
   uint8_t* occ;
   int32_t* rho;
-  int sx, sy, sz;
-  double nu, kT;
+  int sx, sy, sz, px;
 };
 
 #if defined(AKMC_PHASE_PROFILE) && !defined(AKMC_FLOW_PROFILE) && !defined(AKMC_HOP_PROFILE)
@@ -318,7 +330,7 @@ __device__ __forceinline__ double F64(const FTab& T, int32_t r) {
     const double2 hi = reinterpret_cast<const double2*>(T.win)[kFWin + kk];
     return cubic_d(lo.x, lo.y, hi.x, hi.y, p);
   }
-  return F64_far(T.g64lo, T.g64hi, T.status, r, p);
+  return F64_far(T.pot->F64lo, T.pot->F64hi, T.status, r, p);
 }
 
 // A cell known to lie inside the shared-memory window.
@@ -353,8 +365,8 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
       atomicOr(T.status, kErrRhoRange);
       kc = r < 0 ? 0 : kTabN - 2;
     }
-    a = __ldg(T.g32a + kc);
-    c3 = __ldg(T.g32b + kc);
+    a = __ldg(T.pot->F32a + kc);
+    c3 = __ldg(T.pot->F32b + kc);
   }
   FCell32 c;
   c.hi = a.x; c.lo = a.y; c.c1 = a.z; c.c2 = a.w; c.c3 = c3;
@@ -512,7 +524,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     }
   }
   if (q == 0) {
-    sm.rates[set][k][b] = avail ? arrhenius(jc.nu, jc.kT, Xc, dE) : 0.0;
+    sm.rates[set][k][b] = avail ? arrhenius(sm.c_nu, sm.c_kT, Xc, dE) : 0.0;
     sm.vX[set][k][b] = avail ? Xc : 0;
     if (de_out) de_out[k * 8 + b] = avail ? dE : 0.0;  // akmc_calculate only
   }
@@ -520,30 +532,19 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
 }
 
 // Bulk staging of a region (R.bulk): the bulk-copy unit moves whole rows, R.bo occupancy bytes
-// and R.br densities from the row's 16-site boundary R.ox (unwrapped), into shared rows of pitch
-// R.LX; thread t0 + k nt issues row t0 + k nt.  A span that leaves the row [0, sx) at either end
-// goes in two pieces: sites [R.ox, cut) to shared [0, cut - R.ox) and the rest from the other
-// end of the row.  The barrier is armed for the bytes of every row (stage_bytes).
-__device__ __forceinline__ void stage_rows(const Region& R, const uint8_t* occ, const int32_t* rho, int sx, int sy, int sz,
+// and R.br densities from the row's 16-site boundary R.ox (unwrapped; the row's halo holds the
+// sites past either end), into shared rows of pitch R.LX; thread t0 + k nt issues row
+// t0 + k nt, one copy per array.  The barrier is armed for the bytes of every row (stage_bytes).
+__device__ __forceinline__ void stage_rows(const Region& R, const uint8_t* occ, const int32_t* rho, int px, int sy, int sz,
                                            bool eam, uint8_t* occ_s, int32_t* rho_s, uint64_t* bar, int t0, int nt) {
   asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
   const int nrows = R.LY * R.LZ;
   for (int row = t0; row < nrows; row += nt) {
     const int ly = row % R.LY, lz = row / R.LY;
     const int gy = wrap1(R.oy + ly, sy), gz = wrap1(R.oz + lz, sz);
-    const int64_t rb = static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz);
-#pragma unroll
-    for (int arr = 0; arr < 2; ++arr) {
-      if (arr == 1 && !eam) break;
-      const int len = arr == 0 ? R.bo : R.br;  // sites of the span
-      const int es = arr == 0 ? 1 : 4;          // bytes per site
-      uint8_t* dst = arr == 0 ? occ_s + R.LX * row : reinterpret_cast<uint8_t*>(rho_s + R.LX * row);
-      const uint8_t* src = arr == 0 ? occ + rb : reinterpret_cast<const uint8_t*>(rho + rb);
-      const int n1 = R.ox < 0 ? -R.ox : min(len, sx - R.ox);  // sites up to the row's end
-      const int a1 = R.ox < 0 ? R.ox + sx : R.ox;              // row position of the first piece
-      bulk_copy(dst, src + static_cast<int64_t>(es) * a1, static_cast<uint32_t>(es * n1), bar);
-      if (len > n1) bulk_copy(dst + es * n1, src, static_cast<uint32_t>(es * (len - n1)), bar);
-    }
+    const int64_t first = static_cast<int64_t>(px) * (gy + static_cast<int64_t>(sy) * gz) + kHaloL + R.ox;
+    bulk_copy(occ_s + R.LX * row, occ + first, static_cast<uint32_t>(R.bo), bar);
+    if (eam) bulk_copy(rho_s + R.LX * row, rho + first, static_cast<uint32_t>(4 * R.br), bar);
   }
 }
 // Bytes the bulk staging of region R moves (the barrier's transaction count).
@@ -674,10 +675,14 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   jc.sx = J.sx;
   jc.sy = J.sy;
   jc.sz = J.sz;
-  jc.nu = J.nu;
-  jc.kT = J.kT;
+  jc.px = J.px;
+
   Region R;
   make_region(B, J, sec, R);
+  if (tid == 0) {  // before the barrier below; the evaluations read them
+    sm.c_nu = J.nu;
+    sm.c_kT = J.kT;
+  }
   // F-table window: one bulk copy issued by the control thread, overlapped with the staging
   const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
   const bool need_win = eam && sm.win_pot != win_key;
@@ -711,18 +716,18 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   FTab FT;
   FT.win = sm.fwin;
   FT.kw0 = P.fwin0;
-  FT.g64lo = P.F64lo;
-  FT.g64hi = P.F64hi;
-  FT.g32a = P.F32a;
-  FT.g32b = P.F32b;
+  FT.pot = &P;
   FT.status = a.status;
+#ifdef AKMC_PHASE_PROFILE
   FT.prof = a.counters + 16;
+#endif
   AKMC_STAGE_T(1);
 
   // stage the region: warp w takes rows w, w+9, ...; kStageRows rows of loads are issued
   // before any shared-memory store so they are all in flight (rows hold <= 64 sites)
   if (!R.bulk) {
-    const int gx0 = wrap1(R.ox + lane, jc.sx), gx1 = wrap1(R.ox + lane + 32, jc.sx);
+    // row positions of the region's x span (the halo holds the sites past either end)
+    const int gx0 = kHaloL + R.ox + lane, gx1 = gx0 + 32;
     const bool has0 = lane < R.LX, has1 = lane + 32 < R.LX;
     constexpr int kW = kThreads / 32;
     for (int row0 = warp; row0 < nrows; row0 += kStageRows * kW) {
@@ -734,7 +739,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         if (row < nrows) {
           const int ly = row % R.LY, lz = row / R.LY;
           const int gy = wrap1(R.oy + ly, jc.sy), gz = wrap1(R.oz + lz, jc.sz);
-          const int64_t base = static_cast<int64_t>(jc.sx) * (gy + static_cast<int64_t>(jc.sy) * gz);
+          const int64_t base = static_cast<int64_t>(jc.px) * (gy + static_cast<int64_t>(jc.sy) * gz);
           if (has0) {
             ov[k][0] = __ldcg(jc.occ + base + gx0);
             if (eam) rv[k][0] = __ldcg(jc.rho + base + gx0);
@@ -762,7 +767,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
   } else if (!flowpre) {
-    stage_rows(R, jc.occ, jc.rho, jc.sx, jc.sy, jc.sz, eam, occ_s, rho_s, &sm.mbar_st, tid, kThreads);
+    stage_rows(R, jc.occ, jc.rho, jc.px, jc.sy, jc.sz, eam, occ_s, rho_s, &sm.mbar_st, tid, kThreads);
   }
   AKMC_STAGE_T(2);
   const int cnt = cnt_in;
@@ -876,9 +881,16 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   //    next iteration (indexed by iteration parity).
   // A selection that finds no jump (u * total reached no running sum) advances the clock only and
   // keeps set c.
-  const int64_t hop0 = __ldcg(&B.hops);
-  int64_t nh = 0, nact_sum = 0, evals = cnt;
-  double sector_time = 0.0;
+  // the control thread's running values live in shared memory (sm.c_*): held in registers they
+  // would be live in every thread across the loop
+  if (tid == kCtl) {
+    sm.c_hop0 = __ldcg(&B.hops);
+    sm.c_nh = 0;
+    sm.c_nact = 0;
+    sm.c_evals = cnt;
+    sm.c_time = 0.0;
+    sm.c_thr = thr;
+  }
   int c = 0;   // record set of the current selection
   int it = 0;  // iteration parity: control slots
   // vacancy k of record set `set` lies within D cells of the cell (qx, qy, qz) and in the sector
@@ -964,7 +976,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
             a.api_event->from_site = -1;
             a.api_event->total = total;
           }
-          sector_time = thr;
+          sm.c_time = sm.c_thr;
         }
       }
       break;
@@ -1000,13 +1012,15 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
               rho_s[j] = v;
               const int gx = wrap1(sX + unpack_dx(e), jc.sx), gy = wrap1(sY + unpack_dy(e), jc.sy),
                         gz = wrap1(sZ + unpack_dz(e), jc.sz);
-              jc.rho[gx + jc.sx * (gy + jc.sy * gz)] = v;  // site ids fit in int32 (checked at akmc_add_job)
+              lattice_put(jc.rho + static_cast<int64_t>(jc.px) * (gy + static_cast<int64_t>(jc.sy) * gz), jc.sx, gx, v);
             }
           } else if (i == kRefreshN) {
             occ_s[s + sm.d1[p][bsel]] = kV;
             occ_s[s] = static_cast<uint8_t>(X);
-            jc.occ[to_g] = kV;
-            jc.occ[sm.vlid[c][ksel]] = static_cast<uint8_t>(X);
+            lattice_put(jc.occ + static_cast<int64_t>(jc.px) * (ngy + static_cast<int64_t>(jc.sy) * ngz), jc.sx, ngx,
+                        static_cast<uint8_t>(kV));
+            lattice_put(jc.occ + static_cast<int64_t>(jc.px) * (sY + static_cast<int64_t>(jc.sy) * sZ), jc.sx, sX,
+                        static_cast<uint8_t>(X));
           } else if (i == kRefreshN + 1) {
             // the hopped vacancy leaves its place in the ordered list and re-enters at its new
             // site id if it is still inside the sector
@@ -1088,7 +1102,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         if (a.mode == kModeSelectPerform) {  // the per-hop entry point stops after one selection
           akmc_event* e = a.api_event;
           e->round = 0;
-          e->hop = hop0;
+          e->hop = sm.c_hop0;
           e->from_site = hop ? sm.vlid[c][ksel] : -1;
           e->to_site = hop ? to_g : -1;
           e->block = B.local_id;
@@ -1101,9 +1115,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           e->job = B.job;
           e->reserved = 0;
           if (hop) {
-            nh = 1;
-            evals += nd;
-            nact_sum += nord;
+            sm.c_nh = 1;
+            sm.c_evals += nd;
+            sm.c_nact += nord;
           }
           nstop = 1;
         } else {
@@ -1111,17 +1125,17 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           for (int i = 0; i < 4; ++i) sm.xs[i] = sm.xsn[it][i];
           const double u2 = uniform_oc(sm.xt);  // sublattice.inl:118-120
           const double dt = -port_log(u2) / total;
-          sector_time += dt;
+          sm.c_time += dt;
           if (hop) {
-            ++nh;
-            evals += nd;
-            nact_sum += nord;
+            sm.c_nh += 1;
+            sm.c_evals += nd;
+            sm.c_nact += nord;
             if (a.log_cap > 0) {
               const unsigned long long slot = atomicAdd(a.log_count, 1ull);
               if (slot < static_cast<unsigned long long>(a.log_cap)) {
                 akmc_event* e = a.log + slot;
                 e->round = round_now;
-                e->hop = hop0 + nh - 1;
+                e->hop = sm.c_hop0 + sm.c_nh - 1;
                 e->from_site = sm.vlid[c][ksel];
                 e->to_site = to_g;
                 e->block = B.local_id;
@@ -1138,8 +1152,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
               }
             }
           }
-          if (!(sector_time < thr)) nstop = 1;
-          if (nh >= a.hop_cap) {
+          if (!(sm.c_time < sm.c_thr)) nstop = 1;
+          if (sm.c_nh >= a.hop_cap) {
             atomicOr(a.status, kErrHopCap);
             nstop = 1;
           }
@@ -1168,15 +1182,16 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   if (tid == 0) sm.fin = c;  // every thread holds the same c
   if (a.mode == kModeCalc) return true;
   if (tid == kCtl) {
+    const int64_t nh = sm.c_nh;
     if (a.mode == kModeRound) {
-      B.evo[sec] = __ldcg(&B.evo[sec]) + sector_time;
+      B.evo[sec] = __ldcg(&B.evo[sec]) + sm.c_time;
       for (int i = 0; i < 4; ++i) {
         B.xs[i] = sm.xs[i];
         B.xt[i] = sm.xt[i];
       }
     }
-    B.hops = hop0 + nh;
-    sm.hops_out = hop0 + nh;
+    B.hops = sm.c_hop0 + nh;
+    sm.hops_out = sm.c_hop0 + nh;
     if (sm.acc_job != B.job) {
       if (sm.acc_job >= 0 && sm.acc_job_hops)
         atomicAdd(reinterpret_cast<unsigned long long*>(&a.jobs[sm.acc_job].hops), sm.acc_job_hops);
@@ -1185,9 +1200,9 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
     sm.acc_job_hops += static_cast<unsigned long long>(nh);
     sm.acc[0] += static_cast<unsigned long long>(nh);
-    sm.acc[1] += static_cast<unsigned long long>(evals);
+    sm.acc[1] += static_cast<unsigned long long>(sm.c_evals);
     sm.acc[2] += 1ull;
-    sm.acc[3] += static_cast<unsigned long long>(nact_sum);
+    sm.acc[3] += static_cast<unsigned long long>(sm.c_nact);
     sm.acc[4] += static_cast<unsigned long long>(R.nt);
     sm.acc[5] += static_cast<unsigned long long>(nh * (eam ? 2 + kRefreshN : 2));
   }
@@ -1670,9 +1685,14 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
       st = *reinterpret_cast<volatile unsigned*>(a.status);
     }
 
-    // sweep: thread tid looks after block (cursor + tid) mod nb
-    if (tid < nb) {
-      int gb = cursor + tid;
+    // sweep: thread tid looks after blocks (cursor + tid + k kThreads) mod nb, k < kSweepVisits,
+    // until it takes one: a visit that finds nothing to do ends after one or two round trips,
+    // while the sweep lasts as long as its slowest visit (one that takes a block)
+#pragma unroll 1
+    for (int vis = 0; vis < kSweepVisits; ++vis) {
+      const int off = tid + vis * kThreads;
+      if (off >= nb) break;
+      int gb = cursor + off;
       if (gb >= nb) gb -= nb;
       BlockDev& B = a.blocks[gb];
       // one round of loads decides whether to look closer: the block's word, target, job, and its
@@ -1710,6 +1730,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         }
         if (rn > r) sm0->flow_progress = 1;
         flow_publish(a, gb, rn, keep, reached, KIND);
+        break;
       }
     }
     if (tid == 0) {
@@ -1758,7 +1779,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         if (R.bulk && tid == kCtl) bulk_expect(&sm->mbar_st, stage_bytes(R, KIND != kPairBond));
         __syncthreads();  // the previous round's readers are done; the copies' barrier is armed
         // the region's bulk copies first: the slots, clocks and streams are read while they fly
-        if (R.bulk) stage_rows(R, J.occ, J.rho, J.sx, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
+        if (R.bulk) stage_rows(R, J.occ, J.rho, J.px, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
         if (tid < kFlowSlots) {
           const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
           if ((m >> tid) & 1ull) {
@@ -1870,7 +1891,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
     if (tid == 0) t_hop += clock64() - t0;
 #endif
     if (!sm0->flow_progress) __nanosleep(256);
-    cursor += kThreads;
+    cursor += kSweepVisits * kThreads;
     if (cursor >= nb) cursor %= nb;
   }
   cta_flush<W>(a, smem);
@@ -2085,7 +2106,7 @@ __device__ void rho_table(int32_t* fqc, const Potential* pot) {
 }
 
 // One tile of the density build (tix-th tile of the lattice); CTA-collective, 256 threads.
-__device__ void rho_tile(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, int64_t tix,
+__device__ void rho_tile(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t sz, int32_t px, int64_t tix,
                          uint8_t* tile, const int32_t* fqc) {
   const int tid = threadIdx.x;
   const int nx = (sx + kRhoTX - 1) / kRhoTX, ny = (sy + kRhoTY - 1) / kRhoTY;
@@ -2107,7 +2128,7 @@ __device__ void rho_tile(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t s
       gy -= gy >= sy ? sy : 0;
       gz -= gz >= sz ? sz : 0;
     }
-    tile[i] = __ldg(occ + gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz));
+    tile[i] = __ldg(occ + kHaloL + gx + static_cast<int64_t>(px) * (gy + static_cast<int64_t>(sy) * gz));
   }
   __syncthreads();
   // each warp takes sites of one x parity (both parities' sums are unrolled code): warp w
@@ -2120,7 +2141,7 @@ __device__ void rho_tile(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t s
     if (gx >= sx || gy >= sy || gz >= sz) continue;
     const uint8_t* t = tile + (lx + kRhoHX) + kRhoLX * ((ly + kRhoHY) + kRhoLY * (lz + kRhoHZ));
     const int32_t acc = p ? rho_terms<1, 0>(t, fqc) : rho_terms<0, 0>(t, fqc);
-    rho[gx + static_cast<int64_t>(sx) * (gy + static_cast<int64_t>(sy) * gz)] = acc;
+    lattice_put(rho + static_cast<int64_t>(px) * (gy + static_cast<int64_t>(sy) * gz), sx, gx, acc);
   }
 }
 
@@ -2130,12 +2151,12 @@ __host__ __device__ __forceinline__ int64_t rho_tiles(int32_t sx, int32_t sy, in
 }
 
 __global__ void __launch_bounds__(256) k_init_rho(const uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy,
-                                                  int32_t sz, const Potential* pot) {
+                                                  int32_t sz, int32_t px, const Potential* pot) {
   __shared__ uint8_t tile[kRhoLX * kRhoLY * kRhoLZ];
   __shared__ int32_t fqc[16 * 8];
   rho_table(fqc, pot);
   const int64_t ntiles = rho_tiles(sx, sy, sz);
-  for (int64_t tix = blockIdx.x; tix < ntiles; tix += gridDim.x) rho_tile(occ, rho, sx, sy, sz, tix, tile, fqc);
+  for (int64_t tix = blockIdx.x; tix < ntiles; tix += gridDim.x) rho_tile(occ, rho, sx, sy, sz, px, tix, tile, fqc);
 }
 
 // The density build of every EAM job of a context in one launch: global tile t belongs to the
@@ -2158,7 +2179,7 @@ __global__ void __launch_bounds__(256) k_init_rho_jobs(RoundArgs a, const int64_
       rho_table(fqc, a.pots + J.pot);
       pot = J.pot;
     }
-    rho_tile(J.occ, J.rho, J.sx, J.sy, J.sz, t - tile0[lo], tile, fqc);
+    rho_tile(J.occ, J.rho, J.sx, J.sy, J.sz, J.px, t - tile0[lo], tile, fqc);
   }
 }
 
@@ -2166,10 +2187,11 @@ __global__ void __launch_bounds__(256) k_init_rho_jobs(RoundArgs a, const int64_
 // occupancy and appends the vacancies to the job's slice of the vacancy table.
 __global__ void k_scatter_collect(RoundArgs a, const uint8_t* stage, const SiteChunk* chunks, int32_t* counts) {
   const SiteChunk c = chunks[blockIdx.x];
-  uint8_t* occ = a.jobs[c.job].occ;
+  const JobDev& J = a.jobs[c.job];
   for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
     const uint8_t o = stage[c.stage0 + i];
-    occ[c.site0 + i] = o;
+    const int32_t s = static_cast<int32_t>(c.site0 + i);
+    lattice_put(J.occ + static_cast<int64_t>(J.px) * (s / J.sx), J.sx, s % J.sx, o);
     if (o == kV) {
       const int k = atomicAdd(counts + c.job, 1);
       if (k < c.nvac) {
@@ -2188,20 +2210,39 @@ __global__ void k_check_counts(const int32_t* counts, const int32_t* want, int32
 // Whole-context lattice read-back: the reverse copy into the staging buffer.
 __global__ void k_gather(RoundArgs a, uint8_t* stage, const SiteChunk* chunks) {
   const SiteChunk c = chunks[blockIdx.x];
-  const uint8_t* occ = a.jobs[c.job].occ;
-  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) stage[c.stage0 + i] = occ[c.site0 + i];
+  const JobDev& J = a.jobs[c.job];
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x)
+    stage[c.stage0 + i] = J.occ[lattice_index(static_cast<int32_t>(c.site0 + i), J.sx, J.px)];
 }
 
-__global__ void k_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
-                                    int32_t cap, int32_t* count) {
+__global__ void k_collect_vacancies(const uint8_t* occ, int64_t n, int32_t sx, int32_t px, int32_t* vac_site,
+                                    int32_t* vac_job, int32_t job, int32_t cap, int32_t* count) {
   for (int64_t s = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; s < n;
        s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (occ[s] != kV) continue;
+    if (occ[lattice_index(static_cast<int32_t>(s), sx, px)] != kV) continue;
     const int k = atomicAdd(count, 1);
     if (k < cap) {
       vac_site[k] = static_cast<int32_t>(s);
       vac_job[k] = job;
     }
+  }
+}
+
+// The halo entries of every row of a lattice whose main entries were written by a plain copy:
+// row r, entry p outside [kHaloL, kHaloL + sx) takes site (p - kHaloL) mod sx of the row.
+template <typename T>
+__global__ void k_fill_halo(T* lat, int32_t sx, int32_t px, int64_t nrows) {
+  const int nh = kHaloL + kHaloR;
+  const int64_t n = nrows * nh;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = i / nh;
+    const int k = static_cast<int>(i - row * nh);
+    const int p = k < kHaloL ? k : sx + k;  // [0, kHaloL) then [kHaloL + sx, kHaloL + sx + kHaloR)
+    int x = (p - kHaloL) % sx;
+    if (x < 0) x += sx;
+    T* r = lat + row * px;
+    r[p] = r[kHaloL + x];
   }
 }
 
@@ -2300,7 +2341,7 @@ int launch_init_rho(uint8_t* occ, int32_t* rho, int32_t sx, int32_t sy, int32_t 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t blocks = std::min<int64_t>(rho_tiles(sx, sy, sz), 148 * 16);
   (void)geo;
-  k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, pot);
+  k_init_rho<<<static_cast<int>(blocks), 256, 0, st>>>(occ, rho, sx, sy, sz, lattice_pitch(sx), pot);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -2330,16 +2371,27 @@ int launch_gather_jobs(const RoundArgs& a, const JobsLoad& L, void* stream) {
   return static_cast<int>(cudaGetLastError());
 }
 
-int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t* vac_site, int32_t* vac_job, int32_t job,
-                             int32_t cap, int32_t* count, unsigned int* status, void* stream) {
+int launch_collect_vacancies(const uint8_t* occ, int64_t n, int32_t sx, int32_t* vac_site, int32_t* vac_job,
+                             int32_t job, int32_t cap, int32_t* count, unsigned int* status, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int64_t blocks = (n + 255) / 256;
   if (blocks > 148 * 64) blocks = 148 * 64;
   cudaMemsetAsync(count, 0, sizeof(int32_t), st);
-  k_collect_vacancies<<<static_cast<int>(blocks), 256, 0, st>>>(occ, n, vac_site, vac_job, job, cap, count);
+  k_collect_vacancies<<<static_cast<int>(blocks), 256, 0, st>>>(occ, n, sx, lattice_pitch(sx), vac_site, vac_job, job,
+                                                                cap, count);
   k_check_vacancy_count<<<1, 1, 0, st>>>(count, cap, status);
   return static_cast<int>(cudaGetLastError());
 }
+
+template <typename T>
+int fill_halo(T* lat, int32_t sx, int64_t nrows, void* stream) {
+  const int64_t n = nrows * (kHaloL + kHaloR);
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 64));
+  if (n > 0) k_fill_halo<T><<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(lat, sx, lattice_pitch(sx), nrows);
+  return static_cast<int>(cudaGetLastError());
+}
+int launch_fill_halo(uint8_t* lat, int32_t sx, int64_t nrows, void* stream) { return fill_halo(lat, sx, nrows, stream); }
+int launch_fill_halo(int32_t* lat, int32_t sx, int64_t nrows, void* stream) { return fill_halo(lat, sx, nrows, stream); }
 
 int launch_device_math(const double* x, int64_t n, double* e, double* l, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
