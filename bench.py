@@ -347,8 +347,12 @@ class Runner:
         n = max(1, launches)
         return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic,
-                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a 16-round capture, "
-                                   "cold L2, scaled to the launch's rounds; stored in %s" % TRAFFIC_FILE)
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one full 1024-round "
+                                   "launch of this command (1 pass, warm L2), per round, scaled to the launch's "
+                                   "rounds; stored in %s" % TRAFFIC_FILE
+                                   if sched == "flow" else
+                                   "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 16-round capture "
+                                   "with a cold L2; stored in %s" % TRAFFIC_FILE)
                 if traffic is not None else None,
                 "peak_kind": peak_kind, "kernel": "k_flow" if sched == "flow" else "k_hop",
                 "bytes_per_launch": bytes_alg / n, "avg_launch_us": 1e3 * hop_ms / n, "launches": launches,
