@@ -1184,7 +1184,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   if (tid == kCtl) {
     const int64_t nh = sm.c_nh;
     if (a.mode == kModeRound) {
-      B.evo[sec] = __ldcg(&B.evo[sec]) + sm.c_time;
+      // (k_flow read the clock while the region's copies flew: no second round trip)
+      B.evo[sec] = (flowpre ? sm.pre_evo : __ldcg(&B.evo[sec])) + sm.c_time;
       for (int i = 0; i < 4; ++i) {
         B.xs[i] = sm.xs[i];
         B.xt[i] = sm.xt[i];
@@ -1363,6 +1364,9 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 // Release/acquire fence at GPU scope (lighter than the sequentially consistent __threadfence).
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -1529,13 +1533,18 @@ __device__ void flow_give(const RoundArgs& a, int o, int v, int32_t site, int os
 }
 
 // Publishes the block's completed rounds (rn) and keeps (keep = 1) or frees the lease, with
-// one store after a fence.  The fence is cumulative: writes of other threads of the CTA that a
-// barrier ordered before this call are released too.  `reached`: this lease holder moved the
+// one release store.  Release is cumulative: writes of other threads of the CTA that a barrier
+// ordered before this call are released too.  (-DAKMC_PUBLISH_FENCE: a fence and a relaxed
+// store instead, the form measured before.)  `reached`: this lease holder moved the
 // block onto its target (each block is counted once).
 __device__ __forceinline__ void flow_publish(const RoundArgs& a, int gb, int64_t rn, int keep, bool reached,
                                              int kind) {
+#ifdef AKMC_PUBLISH_FENCE
   fence_acq_rel();
   st_relaxed_u64(&a.fstate[gb], (static_cast<unsigned long long>(rn) << 1) | static_cast<unsigned long long>(keep));
+#else
+  st_release_u64(&a.fstate[gb], (static_cast<unsigned long long>(rn) << 1) | static_cast<unsigned long long>(keep));
+#endif
   if (reached) atomicAdd(&a.flow_done[kind], 1);
 }
 
