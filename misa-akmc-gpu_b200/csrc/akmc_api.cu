@@ -1,4 +1,6 @@
 // akmc_api.cu -- the C ABI of include/akmc.h over the kernels of akmc_kernels.cu.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +34,7 @@ struct HostJob {
   std::vector<int32_t> split[3];
   uint8_t* d_occ = nullptr;
   int32_t* d_rho = nullptr;
+  CUtensorMap tmap[2];    // occupancy and density maps of the device lattice (JobDev::tma)
 };
 
 struct DevPot {
@@ -45,6 +48,39 @@ struct DevPot {
 };
 
 const char* cuda_name(int e) { return cudaGetErrorString(static_cast<cudaError_t>(e)); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
+// library); null when the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_encode() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The tensor map of a job's device lattice array (halo layout, element size es): 3D tensor of
+// (pitch, sy, sz) entries, box = the job's widest staged region.  False if it cannot be encoded
+// (the job then stages by row copies).
+bool encode_lattice_map(CUtensorMap* m, void* base, int es, int32_t sx, int32_t sy, int32_t sz, const int32_t box[3]) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_encode();
+  if (!enc || !base) return false;
+  for (int d = 0; d < 3; ++d)
+    if (box[d] < 1 || box[d] > 256) return false;
+  if ((box[0] * es) % 16) return false;
+  const cuuint64_t px = static_cast<cuuint64_t>(lattice_pitch(sx));
+  const cuuint64_t dim[3] = {px, static_cast<cuuint64_t>(sy), static_cast<cuuint64_t>(sz)};
+  const cuuint64_t stride[2] = {px * es, px * es * dim[1]};
+  const cuuint32_t bdim[3] = {static_cast<cuuint32_t>(box[0]), static_cast<cuuint32_t>(box[1]), static_cast<cuuint32_t>(box[2])};
+  const cuuint32_t estride[3] = {1, 1, 1};
+  return enc(m, es == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_INT32, 3, base, dim, stride, bdim,
+             estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -96,6 +132,7 @@ struct akmc_ctx {
   int32_t* d_vsite = nullptr;
   int32_t* d_vcount = nullptr;
   int32_t* d_nbr = nullptr;
+  unsigned char* d_tmaps = nullptr;  // per job slot: two 128-byte tensor maps
   unsigned int* d_vsec = nullptr;
   int32_t* d_flow = nullptr;  // flow_need[3], flow_done[3]
   // cluster statistics scratch: list, parent, size (one int32 per site of the largest job
@@ -182,6 +219,8 @@ void free_device(akmc_ctx* ctx) {
   ctx->d_vslot = ctx->d_vcount = ctx->d_nbr = ctx->d_flow = nullptr;
   ctx->d_vsec = nullptr;
   ctx->d_vsite = nullptr;
+  dfree(ctx->stream, ctx->d_tmaps);
+  ctx->d_tmaps = nullptr;
   dfree(ctx->stream, ctx->d_cl);
   dfree(ctx->stream, ctx->d_cl_misc);
   ctx->d_cl = nullptr;
@@ -553,6 +592,20 @@ akmc_status setup_job(akmc_ctx* ctx, int32_t ji, JobDev& J, BlockDev* hb, int32_
   J.px = lattice_pitch(sx);
   J.bulk = ctx->bulk_ok && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
            (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
+  // the tensor copies' box: the job's widest region, x rounded out as the bulk form rounds it
+  // (the sizes region_sites multiplies)
+  for (int d = 0; d < 3; ++d) {
+    int wmax = 0;
+    for (size_t k = 0; k + 1 < j.split[d].size(); ++k) {
+      const int w = j.split[d][k + 1] - j.split[d][k];
+      wmax = std::max(wmax, w - w / 2);
+    }
+    J.tbox[d] = d == 0 ? (2 * (wmax + 4) + 14 + 15) & ~15 : wmax + 4;
+  }
+  std::memset(j.tmap, 0, sizeof(j.tmap));
+  const int32_t sy = static_cast<int32_t>(j.cfg.box[1]), sz = static_cast<int32_t>(j.cfg.box[2]);
+  J.tma = J.bulk && encode_lattice_map(&j.tmap[0], j.d_occ, 1, sx, sy, sz, J.tbox) &&
+          (!j.has_eam || encode_lattice_map(&j.tmap[1], j.d_rho, 4, sx, sy, sz, J.tbox));
   for (int d = 0; d < 3; ++d) {
     J.n[d] = static_cast<int32_t>(j.cfg.box[d]);
     J.nb[d] = static_cast<int32_t>(j.split[d].size() - 1);
@@ -813,6 +866,14 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   CK(dalloc(ctx->stream, &ctx->d_vcount, ncap));
   CK(dalloc(ctx->stream, &ctx->d_nbr, ncap * kNbrStride));
   CK(dalloc(ctx->stream, &ctx->d_vsec, ncap));
+  {
+    // every job slot's two tensor maps (filled for the jobs added so far; admitted jobs later)
+    std::vector<unsigned char> tm(static_cast<size_t>(ctx->cap_jobs) * 256, 0);
+    for (size_t ji = 0; ji < ctx->jobs.size(); ++ji) std::memcpy(tm.data() + ji * 256, ctx->jobs[ji].tmap, 256);
+    CK(dalloc(ctx->stream, &ctx->d_tmaps, tm.size()));
+    CK(cudaMemcpyAsync(ctx->d_tmaps, tm.data(), tm.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // tm leaves scope
+  }
   CK(dalloc(ctx->stream, &ctx->d_flow, 6));
   CK(dalloc(ctx->stream, &ctx->d_log_count, 1));
   CK(dalloc(ctx->stream, &ctx->d_api_total, 1));
@@ -881,6 +942,7 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
   a.vcount = ctx->d_vcount;
   a.nbr = ctx->d_nbr;
   a.vsec = ctx->d_vsec;
+  a.tmaps = ctx->d_tmaps;
   a.flow_need = ctx->d_flow;
   a.flow_done = ctx->d_flow + 3;
   a.flow_take = ctx->cfg.flow_take;
@@ -943,6 +1005,7 @@ AKMC_API akmc_status akmc_admit_job(akmc_ctx* ctx, const akmc_job_config* cfg, c
   std::vector<int32_t> vsite(static_cast<size_t>(h.nvac)), vjob(static_cast<size_t>(h.nvac));
   st = setup_job(ctx, slot, J, hb.data(), vsite.data(), vjob.data());
   if (st != AKMC_OK) return st;
+  CK(cudaMemcpyAsync(ctx->d_tmaps + static_cast<size_t>(slot) * 256, h.tmap, 256, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_jobs + slot, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_blocks + h.block0, hb.data(), hb.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
                      ctx->stream));

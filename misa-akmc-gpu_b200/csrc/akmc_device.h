@@ -93,7 +93,11 @@ struct JobDev {
   int32_t n[3];       // cells
   int32_t sx, sy, sz; // sites per dimension (sx = 2 n[0])
   int32_t px;         // row pitch of the device lattice (lattice_pitch(sx))
-  int32_t pad_px;
+  int32_t tma;        // 1: every region has the box tbox as its shared-memory pitch, and a region
+                      // that does not wrap in y or z is staged by one tensor copy per array through
+                      // the job's tensor maps (RoundArgs::tmaps)
+  int32_t tbox[3];    // the box: the job's widest region, x rounded out as the bulk form rounds it
+  int32_t pad_tbox;
   int32_t nb[3];      // domain blocks per dimension
   int32_t block0;     // first global block
   int32_t nblocks;
@@ -165,6 +169,7 @@ struct RoundArgs {
   int32_t* vsite;               // per block: their sites (kept with the ids by whoever moves them)
   int32_t* vcount;              // per block: fill counter while the slots are rebuilt
   unsigned int* vsec;           // per block: bit s set while a vacancy of its area lies in sector s
+  const void* tmaps;            // per job slot: two 128-byte tensor maps (occupancy, densities)
   int32_t* nbr;                 // per block, kNbrStride words: the 27 neighbour blocks (offset
                                 // o = (dz+1)*9 + (dy+1)*3 + dx+1) and a flags word (k_flow_prep)
   int32_t* flow_need;           // per energy kind: blocks with rounds to run in this launch

@@ -74,7 +74,9 @@ struct Region {
   int slo[3], w[3];
   int ox, oy, oz;  // origin in sites (x doubled); may be negative (periodic wrap)
   int LX, LY, LZ, n;  // row pitch in sites and rows of the shared layout, its sites
-  int LXt, xo, nt;    // region row width, its first site within the pitch, region sites
+  int LXt, xo, nt;    // region row width, its first site within the pitch, sites staged
+  int ey, ez;         // rows of the region in y and z (LY, LZ: the pitch, the job's box with tma)
+  int tma;            // staged by one tensor copy per array
   int hx;             // cells before the sector in x within the pitch (the 2-cell halo, plus xo / 2)
   int bulk;           // rows staged by bulk copies: bo occupancy bytes and br densities each
   int bo, br;
@@ -123,9 +125,20 @@ __device__ __forceinline__ void make_region(const BlockDev& B, const JobDev& J, 
       R.bulk = 1;
     }
   }
+  R.ey = R.LY;
+  R.ez = R.LZ;
+  R.tma = 0;
+  if (R.bulk && J.tma) {
+    // every region of the job takes the box as its pitch (the shell tables stay valid across
+    // them); one that does not wrap in y or z is one box of the lattice
+    R.LX = J.tbox[0];
+    R.LY = J.tbox[1];
+    R.LZ = J.tbox[2];
+    R.tma = R.oy >= 0 && R.oy + R.ey <= J.sy && R.oz >= 0 && R.oz + R.ez <= J.sz;
+  }
   R.hx = R.slo[0] - R.ox / 2;
   R.n = R.LX * R.LY * R.LZ;
-  R.nt = R.LXt * R.LY * R.LZ;
+  R.nt = R.tma ? R.n : R.LXt * R.ey * R.ez;
 }
 
 // Shared-memory working set of one CTA (followed by the staged region).
@@ -264,7 +277,7 @@ __device__ __forceinline__ int local_delta(int32_t w, const Region& R) {
 
 // Region layout after Smem: int32 densities, then occupancy bytes (16-byte aligned).
 __device__ __forceinline__ uint8_t* occ_of(int32_t* rho_s, int nreg) {
-  return reinterpret_cast<uint8_t*>(rho_s) + ((static_cast<size_t>(nreg) * 4 + 15) & ~static_cast<size_t>(15));
+  return reinterpret_cast<uint8_t*>(rho_s) + ((static_cast<size_t>(nreg) * 4 + 127) & ~static_cast<size_t>(127));
 }
 
 template <int W>
@@ -538,18 +551,42 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
 __device__ __forceinline__ void stage_rows(const Region& R, const uint8_t* occ, const int32_t* rho, int px, int sy, int sz,
                                            bool eam, uint8_t* occ_s, int32_t* rho_s, uint64_t* bar, int t0, int nt) {
   asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
-  const int nrows = R.LY * R.LZ;
+  const int nrows = R.ey * R.ez;
   for (int row = t0; row < nrows; row += nt) {
-    const int ly = row % R.LY, lz = row / R.LY;
+    const int ly = row % R.ey, lz = row / R.ey;
     const int gy = wrap1(R.oy + ly, sy), gz = wrap1(R.oz + lz, sz);
     const int64_t first = static_cast<int64_t>(px) * (gy + static_cast<int64_t>(sy) * gz) + kHaloL + R.ox;
-    bulk_copy(occ_s + R.LX * row, occ + first, static_cast<uint32_t>(R.bo), bar);
-    if (eam) bulk_copy(rho_s + R.LX * row, rho + first, static_cast<uint32_t>(4 * R.br), bar);
+    const int l = R.LX * (ly + R.LY * lz);  // the shared row (pitch LX, LY)
+    bulk_copy(occ_s + l, occ + first, static_cast<uint32_t>(R.bo), bar);
+    if (eam) bulk_copy(rho_s + l, rho + first, static_cast<uint32_t>(4 * R.br), bar);
   }
 }
 // Bytes the bulk staging of region R moves (the barrier's transaction count).
 __device__ __forceinline__ uint32_t stage_bytes(const Region& R, bool eam) {
-  return static_cast<uint32_t>(R.LY * R.LZ) * static_cast<uint32_t>(R.bo + (eam ? 4 * R.br : 0));
+  if (R.tma) return static_cast<uint32_t>(R.n) * (eam ? 5u : 1u);
+  return static_cast<uint32_t>(R.ey * R.ez) * static_cast<uint32_t>(R.bo + (eam ? 4 * R.br : 0));
+}
+// Tensor staging of a region (R.tma): one 3D tile copy per array of the job's box from entry
+// (kHaloL + R.ox, R.oy, R.oz) of the lattice (x a multiple of 16 entries: 16-byte aligned in both
+// arrays), into shared memory laid out with the box as pitch.  Parts of the box past the region
+// are staged too and never read; parts past the array are filled with zeros.  One thread issues
+// both copies.
+__device__ __forceinline__ void stage_tensor(const Region& R, const void* tmaps, int job, bool eam, uint8_t* occ_s,
+                                             int32_t* rho_s, uint64_t* bar) {
+  asm volatile("fence.proxy.async;" ::: "memory");  // generic accesses before, copies after
+  const unsigned char* m = static_cast<const unsigned char*>(tmaps) + static_cast<size_t>(job) * 256;
+  const int x = kHaloL + R.ox, y = R.oy, z = R.oz;
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_u32(occ_s)),
+      "l"(m), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+  if (eam)
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(rho_s)),
+        "l"(m + 128), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // Phase profile (builds with -DAKMC_PHASE_PROFILE): thread 0 accumulates the cycles
@@ -767,7 +804,11 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       }
     }
   } else if (!flowpre) {
-    stage_rows(R, jc.occ, jc.rho, jc.px, jc.sy, jc.sz, eam, occ_s, rho_s, &sm.mbar_st, tid, kThreads);
+    if (R.tma) {
+      if (tid == kCtl) stage_tensor(R, a.tmaps, B.job, eam, occ_s, rho_s, &sm.mbar_st);
+    } else {
+      stage_rows(R, jc.occ, jc.rho, jc.px, jc.sy, jc.sz, eam, occ_s, rho_s, &sm.mbar_st, tid, kThreads);
+    }
   }
   AKMC_STAGE_T(2);
   const int cnt = cnt_in;
@@ -1212,9 +1253,12 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   return true;
 }
 
+// The region's arrays after Smem, each starting on a 128-byte boundary of the shared window
+// (tensor copies want it; hop_smem_bytes leaves room for the padding).
 __device__ __forceinline__ void carve(uint8_t* smem, int nreg, Smem*& sm, uint8_t*& occ_s, int32_t*& rho_s) {
   sm = reinterpret_cast<Smem*>(smem);
-  uint8_t* p = smem + ((sizeof(Smem) + 15) & ~static_cast<size_t>(15));
+  uint8_t* p = smem + sizeof(Smem);
+  p += (128u - (smem_u32(p) & 127u)) & 127u;
   rho_s = reinterpret_cast<int32_t*>(p);
   occ_s = occ_of(rho_s, nreg);
 }
@@ -1367,9 +1411,11 @@ __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gp
 __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+#ifdef AKMC_PUBLISH_FENCE
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+#endif
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
@@ -1788,7 +1834,11 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         if (R.bulk && tid == kCtl) bulk_expect(&sm->mbar_st, stage_bytes(R, KIND != kPairBond));
         __syncthreads();  // the previous round's readers are done; the copies' barrier is armed
         // the region's bulk copies first: the slots, clocks and streams are read while they fly
-        if (R.bulk) stage_rows(R, J.occ, J.rho, J.px, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
+        if (R.tma) {
+          if (tid == kCtl) stage_tensor(R, a.tmaps, B.job, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st);
+        } else if (R.bulk) {
+          stage_rows(R, J.occ, J.rho, J.px, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
+        }
         if (tid < kFlowSlots) {
           const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
           if ((m >> tid) & 1ull) {
@@ -2265,7 +2315,7 @@ __global__ void k_device_math(const double* x, int64_t n, double* e, double* l) 
 }  // namespace
 
 size_t hop_smem_bytes(int max_region_sites) {
-  return ((sizeof(Smem) + 15) & ~static_cast<size_t>(15)) + ((static_cast<size_t>(max_region_sites) * 4 + 15) & ~static_cast<size_t>(15)) +
+  return sizeof(Smem) + 128 + ((static_cast<size_t>(max_region_sites) * 4 + 127) & ~static_cast<size_t>(127)) +
          static_cast<size_t>(max_region_sites) + 16;
 }
 

@@ -1,5 +1,7 @@
 """The bulk-copy staging geometry and the device lattice's halo layout, checked on the CPU for
-every block and sector of the box and block layouts the host accepts.
+every block and sector of the box and block layouts the host accepts.  (A region that does not
+wrap in y or z is staged instead by one tensor copy per array of the job's box; the box check
+below restates that sizing.)
 
 The device stores each x row of a job's lattice (sx sites) with a periodic halo
 (lattice_pitch, lattice_put in csrc/akmc_device.h): kHaloL = 16 entries on the left hold copies
@@ -141,6 +143,23 @@ def test_every_bulk_copy_is_aligned_and_in_bounds(n, nb):
         assert R["n"] % 2 == 0
         # the mbarrier's transaction count
         assert R["LY"] * R["LZ"] * (bo + 4 * br) < (1 << 20)
+
+
+@pytest.mark.parametrize("n,nb", LAYOUTS)
+def test_tensor_box_holds_every_region(n, nb):
+    # the job's tensor box (setup_job: the widest region, x rounded as the bulk form rounds it)
+    # is every region's shared-memory pitch: each region's bulk row span and its rows fit it, the
+    # box's x extent is a multiple of 16 entries, and its volume is the host's shared-memory sizing
+    sp = splits(n, nb)
+    wmax = max((sp[k + 1] - sp[k]) - (sp[k + 1] - sp[k]) // 2 for k in range(nb))
+    box = ((2 * (wmax + 4) + 14 + 15) & ~15, wmax + 4, wmax + 4)
+    assert box[0] % 16 == 0 and all(1 <= b <= 256 for b in box)
+    assert box[0] * box[1] * box[2] == region_sites([sp] * 3)
+    for _, _, R in regions(n, nb):
+        assert R["LX"] <= box[0] and R["bo"] <= box[0] and R["br"] <= box[0]
+        assert R["LY"] <= box[1] and R["LZ"] <= box[2]
+        # a region staged by the tensor copy starts on a 16-entry boundary of its row
+        assert (HALO_L + R["ox"]) % 16 == 0
 
 
 def test_256_cubed_regions_on_the_box_faces_in_x_use_the_halo():
