@@ -40,6 +40,8 @@ AK_HD bool is_atom(uint8_t c) { return c == kFe || c == kCu || c == kNi || c == 
 AK_HD int species_index(uint8_t c) {
   return c == kFe ? 0 : c == kCu ? 1 : c == kNi ? 2 : c == kMn ? 3 : -1;
 }
+// The same for a code known to be an atom (1, 2, 4, 8 -> 0..3), without the compare chain.
+AK_HD int atom_index(uint8_t c) { return (c >> 1) - (c >> 3); }
 // V, Fe, Cu, Ni, Mn -> 0..4 (pair-bond table index)
 AK_HD int bond_index(uint8_t c) { return c == kV ? 0 : species_index(c) + 1; }
 

@@ -164,8 +164,7 @@ struct Smem {
   int32_t ord[2][kMaxV];        // the active vacancies in z-y-x order (ascending site id)
   int32_t nord[2];
   uint8_t vX[2][kMaxV][8];      // code of jump b's target atom (0: the target is a vacancy)
-  double rates[2][kMaxV][8];
-  double presel[kMaxThreads / 32][8];  // per warp: the running sums of the selection's total
+  alignas(16) double rates[2][kMaxV][8];
   // F-table window, two planes: FP64 (c0, c1) x kFWin then (c2, c3) x kFWin;
   // FP32 (hi, lo, c1, c2) x kFWin then c3 x kFWin
   alignas(16) unsigned char fwin[kFWin * 32];
@@ -394,14 +393,15 @@ __device__ __forceinline__ FCell32 cell32(const FTab& T, int32_t r) {
 //  EAM:       lane q sums sites i = q, q+32, q+64 of the jump's list; the 32 partials
 //             merge by a xor butterfly (16, 8, 4, 2, 1), then the moving atom's own
 //             embedding change is added.
+// l is the vacancy's local site (its record's vloc), d1b[p] jump b's 1nn offset for x parity p.
 template <int KIND>
-__device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int32_t* rho_s, int k, int b,
-                             const FTab& FT, const JobC& jc, const int32_t (&jr)[2][3], double* de_out) {
+__device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int32_t* rho_s, int k, int l, int b,
+                             const int32_t (&d1b)[2], const FTab& FT, const JobC& jc, const int32_t (&jr)[2][3],
+                             double* de_out) {
   const int lane = threadIdx.x & 31;
   const int q = lane;
-  const int l = sm.vloc[set][k];
   const int p = l & 1;
-  const int tl = l + sm.d1[p][b];
+  const int tl = l + (p ? d1b[1] : d1b[0]);
   const uint8_t Xc = occ_s[tl];
   const bool avail = is_atom(Xc);
   double dE = 0.0;
@@ -436,7 +436,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     dE = after - pair;
   } else if (KIND == kEam64) {
     double acc = 0.0, EX = 0.0;
-    const int X = species_index(Xc);
+    const int X = atom_index(Xc);  // read only when avail
     if (avail) {
       // gather: this lane's sites (q, q+32, q+64 of the jump's list; lanes 12..31 have two),
       // their occupancy, densities and shell codes, and the moving atom's own two densities
@@ -476,7 +476,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
       // site term (F(r+d) - F(r)) + (phi_s - phi_t), summed in list order
 #pragma unroll
       for (int u = 0; u < 3; ++u)
-        if (in[u] && o[u] != kV) acc += t[u] + sm.dphi64[(X * 4 + species_index(o[u])) * 64 + h[u]];
+        if (in[u] && o[u] != kV) acc += t[u] + sm.dphi64[(X * 4 + atom_index(o[u])) * 64 + h[u]];
     }
 #pragma unroll
     EVAL_T(0);
@@ -488,7 +488,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     Comp32 acc;
     acc.s = 0.f;
     acc.c = 0.f;
-    const int X = species_index(Xc);
+    const int X = atom_index(Xc);  // read only when avail
     if (avail) {
       uint8_t o[3];
       int32_t r0[3], r1[3];
@@ -519,7 +519,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
       }
 #pragma unroll
       for (int u = 0; u < 3; ++u)
-        if (in[u] && o[u] != kV) kahan_add(acc, t[u] + sm.dphi32[(X * 4 + species_index(o[u])) * 64 + h[u]]);
+        if (in[u] && o[u] != kV) kahan_add(acc, t[u] + sm.dphi32[(X * 4 + atom_index(o[u])) * 64 + h[u]]);
     }
 #pragma unroll
     for (int m = 16; m >= 1; m >>= 1) {
@@ -897,15 +897,24 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       jr[jj][0][u] = in ? sm.jl[0][b][i] : 0;
       jr[jj][1][u] = in ? sm.jl[1][b][i] : 0;
     }
+  // and its jumps' 1nn offsets, both x parities
+  int32_t d1r[kJumpsPerWarp][2];
+#pragma unroll
+  for (int jj = 0; jj < kJumpsPerWarp; ++jj) {
+    const int b = evaluator ? warp + kEvalWarps * jj : 0;
+    d1r[jj][0] = sm.d1[0][b];
+    d1r[jj][1] = sm.d1[1][b];
+  }
   double* const de_out = a.mode == kModeCalc ? a.api_de : nullptr;
   const int D = eam ? 4 : 3;  // a hop changes the rates of vacancies within D cells of its origin
 
   // first evaluation: every vacancy of the sector, into record set 0
   if (evaluator) {
     for (int k = 0; k < cnt; ++k) {
+      const int l = sm.vloc[0][k];
 #pragma unroll
       for (int jj = 0; jj < kJumpsPerWarp; ++jj)
-        eval_vacancy<KIND>(sm, 0, occ_s, rho_s, k, warp + kEvalWarps * jj, FT, jc, jr[jj], de_out);
+        eval_vacancy<KIND>(sm, 0, occ_s, rho_s, k, l, warp + kEvalWarps * jj, d1r[jj], FT, jc, jr[jj], de_out);
     }
   }
   __syncthreads();
@@ -943,27 +952,39 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   long long thp = clock64();
 #endif
   while (true) {
+    // the active count and the first active vacancy, read with the loop's stop word
+    const int nord = sm.nord[c];
+    const int k0 = sm.ord[c][0];
     if (sm.ctl_stop[it]) break;
     const int n = c ^ 1;
-    const int nord = sm.nord[c];
+    // With one active vacancy (nearly every sector at these dilutions) that vacancy is the one
+    // that hops: its record is read while lane 0 selects (k0 is any value when nord != 1).
+    const int kq = nord == 1 ? k0 : 0;
+    int s = sm.vloc[c][kq];
+    int vx2 = sm.vcx[c][kq], qy = sm.vcy[c][kq], qz = sm.vcz[c][kq];
+    int sX = sm.vgx[c][kq], sY = sm.vgy[c][kq], sZ = sm.vgz[c][kq];
     // [1] selection: lane 0 of every warp forms the ordered total (ABVIModel::calcRates,
     // kmc.cpp:68-115), then finds the first of the same running sums above u * total
     // (ABVIModel::select, kmc.cpp:242-309).  Jumps onto a vacancy hold 0.0, which leaves a
-    // positive sum unchanged.  With one active vacancy (nearly every sector at these
-    // dilutions) the running sums of the total's pass are kept and compared afterwards,
+    // positive sum unchanged.  With one active vacancy the running sums of the total's pass stay
+    // in registers (its 8 rates read in four 16-byte loads) and are compared afterwards,
     // independently of one another, instead of being formed a second time.
     int isel = -1, stop = 0;
     double total = 0.0, u = 0.0;
     if (lane == 0) {
-      constexpr int kPreSel = 1;
-      double* pre = sm.presel[warp];
-      if (nord <= kPreSel) {
-        const double* r = sm.rates[c][sm.ord[c][0]];
-#pragma unroll
-        for (int bb = 0; bb < 8; ++bb) {
-          if (nord) total += r[bb];
-          pre[bb] = total;
-        }
+      double pv[8];
+      if (nord == 1) {
+        const double2* r2 = reinterpret_cast<const double2*>(sm.rates[c][kq]);
+        const double2 a0 = r2[0], a1 = r2[1], a2 = r2[2], a3 = r2[3];
+        pv[0] = total + a0.x;
+        pv[1] = pv[0] + a0.y;
+        pv[2] = pv[1] + a1.x;
+        pv[3] = pv[2] + a1.y;
+        pv[4] = pv[3] + a2.x;
+        pv[5] = pv[4] + a2.y;
+        pv[6] = pv[5] + a3.x;
+        pv[7] = pv[6] + a3.y;
+        total = pv[7];
       } else {
         for (int i = 0; i < nord; ++i) {
           const double* r = sm.rates[c][sm.ord[c][i]];
@@ -978,13 +999,10 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       } else {
         u = a.mode == kModeSelectPerform ? a.api_u : sm.ctl_u[it];
         const double expected = u * total;  // ModelAdapter::selectAndPerform
-        if (nord <= kPreSel) {
-          double pv[8 * kPreSel];
+        if (nord == 1) {
 #pragma unroll
-          for (int q = 0; q < 8 * kPreSel; ++q) pv[q] = pre[q];
-#pragma unroll
-          for (int q = 8 * kPreSel - 1; q >= 0; --q)
-            if (q < 8 * nord && pv[q] > expected) isel = q;
+          for (int q = 7; q >= 0; --q)
+            if (pv[q] > expected) isel = q;
         } else {
           double acc = 0.0;
           for (int i = 0; i < nord && isel < 0; ++i) {
@@ -1024,16 +1042,26 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     }
     // the selected jump: vacancy ksel of set c, direction bsel, atom X
     const bool hop = isel >= 0;
-    const int ksel = hop ? sm.ord[c][isel >> 3] : 0, bsel = hop ? (isel & 7) : 0;
-    const int s = sm.vloc[c][ksel];
+    const int bsel = hop ? (isel & 7) : 0;
+    int ksel = kq;
+    if (nord != 1) {  // several active vacancies: the selected one's record
+      ksel = hop ? sm.ord[c][isel >> 3] : 0;
+      s = sm.vloc[c][ksel];
+      vx2 = sm.vcx[c][ksel];
+      qy = sm.vcy[c][ksel];
+      qz = sm.vcz[c][ksel];
+      sX = sm.vgx[c][ksel];
+      sY = sm.vgy[c][ksel];
+      sZ = sm.vgz[c][ksel];
+    }
     const int p = s & 1;
     const int X = hop ? sm.vX[c][ksel][bsel] : 0;
     const int32_t wg = sm.w1[p][bsel];
-    const int qx = sm.vcx[c][ksel] >> 1, qy = sm.vcy[c][ksel], qz = sm.vcz[c][ksel];
-    const int nlx = sm.vcx[c][ksel] + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
+    const int snew = s + sm.d1[p][bsel];  // the vacancy's local site after the hop
+    const int qx = vx2 >> 1;
+    const int nlx = vx2 + unpack_dx(wg), nly = qy + unpack_dy(wg), nlz = qz + unpack_dz(wg);
     const bool nact = (nlx >> 1) >= R.hx && (nlx >> 1) < R.hx + R.w[0] && nly >= 2 && nly < 2 + R.w[1] &&
                       nlz >= 2 && nlz < 2 + R.w[2];
-    const int sX = sm.vgx[c][ksel], sY = sm.vgy[c][ksel], sZ = sm.vgz[c][ksel];
     const int ngx = wrap1(sX + unpack_dx(wg), jc.sx), ngy = wrap1(sY + unpack_dy(wg), jc.sy),
               ngz = wrap1(sZ + unpack_dz(wg), jc.sz);
     const int32_t to_g = ngx + jc.sx * (ngy + jc.sy * ngz);
@@ -1042,21 +1070,38 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
       if (hop) {
         // [2] perform (ABVIModel::perform, kmc.cpp:358-396) on the staged region, written
         // through, and set n: items 0..77 the density deltas, 78 the occupancy swap, 79 the
-        // ordered list, then one record and 8 rates per vacancy
+        // ordered list, then one record and 8 rates per vacancy.  With 8 evaluator warps no warp
+        // holds two kinds of item (a warp runs its kinds one after another): warps 0-2 the
+        // deltas, warp 3 the swap, warp 4 the list, warps 5-7 the records and rates.
         const int nitems = kRefreshN + 2 + 9 * cnt;
-        for (int i = tid; i < nitems; i += kCtl) {
+        int i0 = tid, lim = nitems, step = kCtl;
+        if (kEvalWarps == 8) {
+          static_assert(kRefreshN <= 96, "three warps of density deltas");
+          if (tid < 96) {
+            lim = kRefreshN;
+          } else if (tid == 96 || tid == 128) {
+            i0 = tid == 96 ? kRefreshN : kRefreshN + 1;
+            lim = i0 + 1;
+          } else if (tid >= 160) {
+            i0 = kRefreshN + 2 + (tid - 160);
+            step = 96;
+          } else {
+            lim = 0;
+          }
+        }
+        for (int i = i0; i < lim; i += step) {
           if (i < kRefreshN) {
             if (eam) {
               const int32_t e = sm.rl[p][bsel][i];
               const int j = s + local_delta(e, R);
-              const int32_t v = rho_s[j] + sm.dfq[species_index(static_cast<uint8_t>(X)) * 64 + rshells(e)];
+              const int32_t v = rho_s[j] + sm.dfq[atom_index(static_cast<uint8_t>(X)) * 64 + rshells(e)];
               rho_s[j] = v;
               const int gx = wrap1(sX + unpack_dx(e), jc.sx), gy = wrap1(sY + unpack_dy(e), jc.sy),
                         gz = wrap1(sZ + unpack_dz(e), jc.sz);
               lattice_put(jc.rho + static_cast<int64_t>(jc.px) * (gy + static_cast<int64_t>(jc.sy) * gz), jc.sx, gx, v);
             }
           } else if (i == kRefreshN) {
-            occ_s[s + sm.d1[p][bsel]] = kV;
+            occ_s[snew] = kV;
             occ_s[s] = static_cast<uint8_t>(X);
             lattice_put(jc.occ + static_cast<int64_t>(jc.px) * (ngy + static_cast<int64_t>(jc.sy) * ngz), jc.sx, ngx,
                         static_cast<uint8_t>(kV));
@@ -1082,7 +1127,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
           } else if (i < kRefreshN + 2 + cnt) {
             const int k = i - kRefreshN - 2;
             if (k == ksel) {
-              sm.vloc[n][k] = s + sm.d1[p][bsel];
+              sm.vloc[n][k] = snew;
               sm.vlid[n][k] = to_g;
               sm.vcx[n][k] = static_cast<int16_t>(nlx);
               sm.vcy[n][k] = static_cast<int16_t>(nly);
@@ -1114,22 +1159,26 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
         HOP_P(2);
         HOP_T(1);
         // [3] + [4] the vacancies within D cells of the hop's origin, evaluated into set n
+        // (the hopped vacancy alone: dirty while it stays inside the sector, at its new site)
         for (int base = 0; base < cnt; base += 32) {
           const int k = base + lane;
-          unsigned m = __ballot_sync(kFull, k < cnt && dirty(n, k, qx, qy, qz));
+          unsigned m = cnt == 1 ? (nact ? 1u : 0u) : __ballot_sync(kFull, k < cnt && dirty(n, k, qx, qy, qz));
           while (m) {
             const int kk = base + __ffs(m) - 1;
             m &= m - 1;
+            const int l = cnt == 1 ? snew : sm.vloc[n][kk];
 #pragma unroll
             for (int jj = 0; jj < kJumpsPerWarp; ++jj)
-              eval_vacancy<KIND>(sm, n, occ_s, rho_s, kk, warp + kEvalWarps * jj, FT, jc, jr[jj], nullptr);
+              eval_vacancy<KIND>(sm, n, occ_s, rho_s, kk, l, warp + kEvalWarps * jj, d1r[jj], FT, jc, jr[jj], nullptr);
           }
         }
         HOP_T(2);
       }
     } else {  // control warp: the hop's clock and event, the next iteration's decision and uniform
       int nd = 0;
-      if (hop) {
+      if (hop && cnt == 1) {
+        nd = nact ? 1 : 0;
+      } else if (hop) {
         // the dirty count, from set c with the hopped vacancy at its new cell
         for (int base = 0; base < cnt; base += 32) {
           const int k = base + lane;
