@@ -91,6 +91,10 @@ struct akmc_ctx {
   std::string err;
   std::vector<HostJob> jobs;
   std::vector<DevPot> pots;
+  // x and y extents of every job's tensor box: the widest of the context's jobs (and of the
+  // blocks an admitted job may have), so that every region shares one row and plane pitch and
+  // the shell tables built for it hold from one job to the next
+  int32_t ubox[2] = {0, 0};
   bool prepared = false;
   int32_t nblocks = 0, nvac = 0;
   // device state
@@ -287,6 +291,19 @@ int region_sites(const HostJob& j, bool bulk) {
     mx *= ext;
   }
   return static_cast<int>(mx);
+}
+
+// The job's own tensor box: its widest region, x rounded out as the bulk form rounds it (the
+// sizes region_sites multiplies).
+void job_box(const HostJob& j, int32_t box[3]) {
+  for (int d = 0; d < 3; ++d) {
+    int wmax = 0;
+    for (size_t k = 0; k + 1 < j.split[d].size(); ++k) {
+      const int w = j.split[d][k + 1] - j.split[d][k];
+      wmax = std::max(wmax, w - w / 2);
+    }
+    box[d] = d == 0 ? (2 * (wmax + 4) + 14 + 15) & ~15 : wmax + 4;
+  }
 }
 
 // Bulk staging works for every job: the device lattice's rows carry a periodic halo and a pitch
@@ -592,16 +609,11 @@ akmc_status setup_job(akmc_ctx* ctx, int32_t ji, JobDev& J, BlockDev* hb, int32_
   J.px = lattice_pitch(sx);
   J.bulk = ctx->bulk_ok && (reinterpret_cast<uintptr_t>(j.d_occ) & 15) == 0 &&
            (reinterpret_cast<uintptr_t>(j.d_rho) & 15) == 0;
-  // the tensor copies' box: the job's widest region, x rounded out as the bulk form rounds it
-  // (the sizes region_sites multiplies)
-  for (int d = 0; d < 3; ++d) {
-    int wmax = 0;
-    for (size_t k = 0; k + 1 < j.split[d].size(); ++k) {
-      const int w = j.split[d][k + 1] - j.split[d][k];
-      wmax = std::max(wmax, w - w / 2);
-    }
-    J.tbox[d] = d == 0 ? (2 * (wmax + 4) + 14 + 15) & ~15 : wmax + 4;
-  }
+  // the tensor copies' box: the job's widest region in z, the context's widest in x and y (the
+  // pitch every region of the context shares)
+  job_box(j, J.tbox);
+  J.tbox[0] = std::max(J.tbox[0], ctx->ubox[0]);
+  J.tbox[1] = std::max(J.tbox[1], ctx->ubox[1]);
   std::memset(j.tmap, 0, sizeof(j.tmap));
   const int32_t sy = static_cast<int32_t>(j.cfg.box[1]), sz = static_cast<int32_t>(j.cfg.box[2]);
   J.tma = J.bulk && encode_lattice_map(&j.tmap[0], j.d_occ, 1, sx, sy, sz, J.tbox) &&
@@ -787,6 +799,25 @@ AKMC_API akmc_status akmc_prepare(akmc_ctx* ctx) {
     max_region = std::max(max_region, region_sites_edge(ctx->max_edge, false));
     max_region_bulk = std::max(max_region_bulk, region_sites_edge(ctx->max_edge, true));
   }
+  // the shared x and y pitch of the tensor boxes, and the largest box with it
+  ctx->ubox[0] = ctx->ubox[1] = 0;
+  for (auto& j : ctx->jobs) {
+    int32_t b[3];
+    job_box(j, b);
+    ctx->ubox[0] = std::max(ctx->ubox[0], b[0]);
+    ctx->ubox[1] = std::max(ctx->ubox[1], b[1]);
+  }
+  const int he = room ? ctx->max_edge - ctx->max_edge / 2 + 4 : 0;
+  if (room) {
+    ctx->ubox[0] = std::max(ctx->ubox[0], (2 * he + 14 + 15) & ~15);
+    ctx->ubox[1] = std::max(ctx->ubox[1], he);
+  }
+  for (auto& j : ctx->jobs) {
+    int32_t b[3];
+    job_box(j, b);
+    max_region_bulk = std::max(max_region_bulk, ctx->ubox[0] * ctx->ubox[1] * b[2]);
+  }
+  if (room) max_region_bulk = std::max(max_region_bulk, ctx->ubox[0] * ctx->ubox[1] * he);
   ctx->cap_jobs = std::max<int32_t>(static_cast<int32_t>(ctx->jobs.size()), room ? ctx->cfg.max_jobs : 0);
   ctx->cap_blocks = std::max<int32_t>(nb, room ? static_cast<int32_t>(std::min<int64_t>(ctx->cfg.max_blocks, INT32_MAX)) : 0);
   ctx->cap_vac = std::max<int32_t>(nv, room ? static_cast<int32_t>(std::min<int64_t>(ctx->cfg.max_vacancies, INT32_MAX)) : 0);
