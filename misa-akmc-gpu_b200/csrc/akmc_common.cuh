@@ -165,6 +165,30 @@ AK_HD double arrhenius(double nu, double kT, uint8_t moving, double dE) {
   return nu * port_exp(-Ea / kT);
 }
 
+// a / b rounded to nearest from y = RN(1 / b), by Markstein's correction (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): when y is the correctly rounded reciprocal and q lies within one ulp of
+// a / b, the remainder r = a - b q is exact under a fused multiply-add and RN(q + r y) is the
+// correctly rounded quotient.  q0 = RN(a y) may lie up to 1.5 ulp away, so a first correction
+// brings it within one ulp (its error becomes about half an ulp) and a second one gives RN(a / b),
+// the same bits as an IEEE division.  Valid away from overflow and underflow of q and r: the
+// rates' exponent arguments are a few eV over kT in (0, 1) eV.  Five dependent operations in
+// place of a division on the latency chain of every rate.
+AK_HD double div_rn_recip(double a, double b, double y) {
+  const double q0 = a * y;
+  const double r0 = fma_d(-q0, b, a);
+  const double q1 = fma_d(r0, y, q0);
+  const double r1 = fma_d(-q1, b, a);
+  return fma_d(r1, y, q1);
+}
+
+// arrhenius() with the exponent argument -Ea / kT formed by div_rn_recip (rkT = RN(1 / kT)):
+// the same bits.
+AK_HD double arrhenius_rk(double nu, double kT, double rkT, uint8_t moving, double dE) {
+  const double Ea = e0_of(moving) + dE / 2;
+  return nu * port_exp(div_rn_recip(-Ea, kT, rkT));
+}
+
 // ---------------------------------------------------------------------------
 // xoshiro256** (Blackman & Vigna 2018); streams seeded through splitmix64.
 // Stream (seed, tag, index): tag 1 alloy types, 2 vacancies, 3 event selection,

@@ -188,12 +188,15 @@ struct Smem {
   int32_t fsite[kFlowSlots];                        // their sites
   int64_t flow_cr[kMaxThreads], flow_ct[kMaxThreads];  // round and target of each round handed over
   int64_t cur_r, cur_t;   // the block's round and target for its next chained round
+  int32_t bc0[3], bc1[3];  // the running block's area and its job's block count, kept for the
+  int32_t bnb;             // post-round updates (a reload after the round's stores is an L2 trip)
   int64_t hops_out;       // the block's hop count after run_block
   // run_block's control thread: hops at the start, hops, n_act sum and evaluations of the
   // block-round, the sector's clock and its threshold
   int64_t c_hop0, c_nh, c_nact, c_evals;
   double c_time, c_thr;
   double c_nu, c_kT;  // the job's attempt frequency and kT (the rates' constants)
+  double c_rkT;       // RN(1 / kT): the rates' exponent arguments without a division
   double pre_evo;         // the active sector's clock, read while the region's copies fly
   // device counters summed per CTA and added once when the kernel ends (per-round atomics on
   // the same addresses from every CTA queue up); hops of the current job likewise
@@ -537,7 +540,7 @@ __device__ void eval_vacancy(Smem& sm, int set, const uint8_t* occ_s, const int3
     }
   }
   if (q == 0) {
-    sm.rates[set][k][b] = avail ? arrhenius(sm.c_nu, sm.c_kT, Xc, dE) : 0.0;
+    sm.rates[set][k][b] = avail ? arrhenius_rk(sm.c_nu, sm.c_kT, sm.c_rkT, Xc, dE) : 0.0;
     sm.vX[set][k][b] = avail ? Xc : 0;
     if (de_out) de_out[k * 8 + b] = avail ? dE : 0.0;  // akmc_calculate only
   }
@@ -719,6 +722,7 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
   if (tid == 0) {  // before the barrier below; the evaluations read them
     sm.c_nu = J.nu;
     sm.c_kT = J.kT;
+    sm.c_rkT = 1.0 / J.kT;
   }
   // F-table window: one bulk copy issued by the control thread, overlapped with the staging
   const int win_key = J.pot * 2 + (KIND == kEam32 ? 1 : 0);
@@ -1879,7 +1883,15 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         uint8_t* occ_s;
         int32_t* rho_s;
         carve(smem, R.n, sm, occ_s, rho_s);
-        if (tid == 0) sm->fnv = 0;
+        if (tid == 0) {
+          sm->fnv = 0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            sm->bc0[d] = B.c0[d];
+            sm->bc1[d] = B.c1[d];
+          }
+          sm->bnb = J.nblocks;
+        }
         if (R.bulk && tid == kCtl) bulk_expect(&sm->mbar_st, stage_bytes(R, KIND != kPairBond));
         __syncthreads();  // the previous round's readers are done; the copies' barrier is armed
         // the region's bulk copies first: the slots, clocks and streams are read while they fly
@@ -1932,13 +1944,14 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           // only one that left it needs the owner lookup
           const int f = sm->fin;
           const int cx = sm->vgx[f][tid] >> 1, cy = sm->vgy[f][tid], cz = sm->vgz[f][tid];
-          const bool inside = cx >= B.c0[0] && cx < B.c1[0] && cy >= B.c0[1] && cy < B.c1[1] && cz >= B.c0[2] &&
-                              cz < B.c1[2];
+          const int* c0 = sm->bc0;
+          const int* c1 = sm->bc1;
+          const bool inside = cx >= c0[0] && cx < c1[0] && cy >= c0[1] && cy < c1[1] && cz >= c0[2] && cz < c1[2];
           const int32_t site = sm->vlid[f][tid];
           int osec = 0, o = gb;
           if (inside)
-            osec = (cx - B.c0[0] >= (B.c1[0] - B.c0[0]) / 2 ? 1 : 0) | (cy - B.c0[1] >= (B.c1[1] - B.c0[1]) / 2 ? 2 : 0) |
-                   (cz - B.c0[2] >= (B.c1[2] - B.c0[2]) / 2 ? 4 : 0);
+            osec = (cx - c0[0] >= (c1[0] - c0[0]) / 2 ? 1 : 0) | (cy - c0[1] >= (c1[1] - c0[1]) / 2 ? 2 : 0) |
+                   (cz - c0[2] >= (c1[2] - c0[2]) / 2 ? 4 : 0);
           else
             o = owner_sector(J, site, &osec);
           if (o == gb) {
@@ -1964,7 +1977,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           bool more = false, reached = rn >= target;
           const bool in_time =
               a.time_budget_ns <= 0 || globaltimer_ns() - t_begin < static_cast<uint64_t>(a.time_budget_ns);
-          if (!reached && J.nblocks == 1 && c + 1 == ncand && in_time) {
+          if (!reached && sm->bnb == 1 && c + 1 == ncand && in_time) {
             // a single-block job: its next rounds wait for nothing, so keep the lease and run on
             // -- when no other round this CTA took in the sweep is waiting for it
             more = flow_advance(a, B, J, gb, sm0->flow_lag, r + 1, nullptr, &rn, &reached, &tgt);
