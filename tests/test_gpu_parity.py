@@ -63,8 +63,11 @@ def check_job(eng, o, j, dev_events):
 
 def test_device_exp_log_bit_exact(ak):
     rng = np.random.default_rng(7)
+    inf = float("inf")
     x = np.concatenate([rng.uniform(-60, 0, 4000), rng.uniform(1e-300, 1, 4000), rng.uniform(-700, 700, 2000),
-                        [0.0, 1.0, 0.5, 2.0 ** -1074, 709.0, -745.0]])
+                        rng.uniform(-746, -708, 2000), rng.uniform(-750, 715, 2000),
+                        [0.0, 1.0, 0.5, 2.0 ** -1074, 709.0, -745.0, float("nan"), inf, -inf, 709.782712893384,
+                         709.79, 710.0, 1e300, -745.1332191019412, -745.2, -1e300]])
     with ak.Engine() as eng:
         e, l = eng.device_math(x)
     want_e = np.array([po.port_exp(v) for v in x])
