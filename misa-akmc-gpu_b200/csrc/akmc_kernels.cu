@@ -34,6 +34,10 @@ constexpr int kStageRows = 4;  // rows of the staged region each warp has in fli
 #define AKMC_SWEEP_VISITS 1
 #endif
 constexpr int kSweepVisits = AKMC_SWEEP_VISITS;
+// Nanoseconds a k_flow CTA sleeps after a sweep that moved no block on (0: none).
+#ifndef AKMC_SWEEP_SLEEP_NS
+#define AKMC_SWEEP_SLEEP_NS 256
+#endif
 enum : int { kPairBond = 0, kEam64 = 1, kEam32 = 2 };  // energy kinds, one kernel instance each
 // CTA shape: W warps evaluate the 8 jump directions (warp w takes jumps w, w + W, ...), one
 // more warp controls the hop loop.  The hop kernels are built for W = 8 (one jump per warp) and
@@ -2011,7 +2015,7 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
 #ifdef AKMC_PHASE_PROFILE
     if (tid == 0) t_hop += clock64() - t0;
 #endif
-    if (!sm0->flow_progress) __nanosleep(256);
+    if (AKMC_SWEEP_SLEEP_NS > 0 && !sm0->flow_progress) __nanosleep(AKMC_SWEEP_SLEEP_NS);
     cursor += kSweepVisits * kThreads;
     if (cursor >= nb) cursor %= nb;
   }
