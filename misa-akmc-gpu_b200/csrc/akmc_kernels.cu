@@ -165,6 +165,9 @@ struct Smem {
   int16_t vcx[2][kMaxV], vcy[2][kMaxV], vcz[2][kMaxV];  // local coordinates (x in doubled sites)
   int32_t vgx[2][kMaxV], vgy[2][kMaxV], vgz[2][kMaxV];  // global coordinates
   uint8_t vact[2][kMaxV];       // vacancy still inside the active sector
+  // the same record packed for the selection, which every warp reads: (local site, local x, y,
+  // z) and (global x, y, z, site id), two 16-byte loads instead of seven
+  alignas(16) int4 vpk[2][kMaxV][2];
   int32_t ord[2][kMaxV];        // the active vacancies in z-y-x order (ascending site id)
   int32_t nord[2];
   uint8_t vX[2][kMaxV][8];      // code of jump b's target atom (0: the target is a vacancy)
@@ -838,6 +841,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     sm.vgy[0][tid] = y;
     sm.vgz[0][tid] = z;
     sm.vact[0][tid] = 1;
+    sm.vpk[0][tid][0] = make_int4(lx + R.LX * (ly + R.LY * lz), lx, ly, lz);
+    sm.vpk[0][tid][1] = make_int4(X, y, z, s);
   }
   __syncthreads();
   AKMC_STAGE_T(3);
@@ -968,9 +973,10 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     // With one active vacancy (nearly every sector at these dilutions) that vacancy is the one
     // that hops: its record is read while lane 0 selects (k0 is any value when nord != 1).
     const int kq = nord == 1 ? k0 : 0;
-    int s = sm.vloc[c][kq];
-    int vx2 = sm.vcx[c][kq], qy = sm.vcy[c][kq], qz = sm.vcz[c][kq];
-    int sX = sm.vgx[c][kq], sY = sm.vgy[c][kq], sZ = sm.vgz[c][kq];
+    const int4 pa = sm.vpk[c][kq][0], pb = sm.vpk[c][kq][1];
+    int s = pa.x;
+    int vx2 = pa.y, qy = pa.z, qz = pa.w;
+    int sX = pb.x, sY = pb.y, sZ = pb.z;
     // [1] selection: lane 0 of every warp forms the ordered total (ABVIModel::calcRates,
     // kmc.cpp:68-115), then finds the first of the same running sums above u * total
     // (ABVIModel::select, kmc.cpp:242-309).  Jumps onto a vacancy hold 0.0, which leaves a
@@ -1054,13 +1060,14 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
     int ksel = kq;
     if (nord != 1) {  // several active vacancies: the selected one's record
       ksel = hop ? sm.ord[c][isel >> 3] : 0;
-      s = sm.vloc[c][ksel];
-      vx2 = sm.vcx[c][ksel];
-      qy = sm.vcy[c][ksel];
-      qz = sm.vcz[c][ksel];
-      sX = sm.vgx[c][ksel];
-      sY = sm.vgy[c][ksel];
-      sZ = sm.vgz[c][ksel];
+      const int4 qa = sm.vpk[c][ksel][0], qb = sm.vpk[c][ksel][1];
+      s = qa.x;
+      vx2 = qa.y;
+      qy = qa.z;
+      qz = qa.w;
+      sX = qb.x;
+      sY = qb.y;
+      sZ = qb.z;
     }
     const int p = s & 1;
     const int X = hop ? sm.vX[c][ksel][bsel] : 0;
@@ -1144,6 +1151,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
               sm.vgy[n][k] = ngy;
               sm.vgz[n][k] = ngz;
               sm.vact[n][k] = nact ? 1 : 0;
+              sm.vpk[n][k][0] = make_int4(snew, nlx, nly, nlz);
+              sm.vpk[n][k][1] = make_int4(ngx, ngy, ngz, to_g);
             } else {
               sm.vloc[n][k] = sm.vloc[c][k];
               sm.vlid[n][k] = sm.vlid[c][k];
@@ -1154,6 +1163,8 @@ __device__ bool run_block(const RoundArgs& a, int gb, Smem& sm, uint8_t* occ_s, 
               sm.vgy[n][k] = sm.vgy[c][k];
               sm.vgz[n][k] = sm.vgz[c][k];
               sm.vact[n][k] = sm.vact[c][k];
+              sm.vpk[n][k][0] = sm.vpk[c][k][0];
+              sm.vpk[n][k][1] = sm.vpk[c][k][1];
             }
           } else {
             // rates of vacancy q / 8, jump q % 8 carried over; the dirty ones are overwritten below
