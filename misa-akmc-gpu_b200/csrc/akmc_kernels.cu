@@ -194,6 +194,7 @@ struct Smem {
   int32_t fv[kFlowSlots], fslot[kFlowSlots], fnv;  // the sector's vacancies and their slots
   int32_t fsite[kFlowSlots];                        // their sites
   int64_t flow_cr[kMaxThreads], flow_ct[kMaxThreads];  // round and target of each round handed over
+  unsigned long long flow_cvv[kMaxThreads];             // its block's vacancy-slot valid bits
   int64_t cur_r, cur_t;   // the block's round and target for its next chained round
   int32_t bc0[3], bc1[3];  // the running block's area and its job's block count, kept for the
   int32_t bnb;             // post-round updates (a reload after the round's stores is an L2 trip)
@@ -1673,7 +1674,8 @@ __device__ __forceinline__ void flow_publish(const RoundArgs& a, int gb, int64_t
 // target (by running rounds, or by a budget moving the target down to r0); false for a block
 // that was at its target already (a stale sweep read).
 __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, int gb, const int8_t (*lag)[27],
-                             int64_t r0, const int32_t (*Pin)[27], int64_t* rn, bool* reached, int64_t* tgt) {
+                             int64_t r0, const int32_t (*Pin)[27], int64_t* rn, bool* reached, int64_t* tgt,
+                             unsigned long long* vv = nullptr) {
   *rn = r0;
   *reached = false;
   // one round of loads, all in flight together: the target, the job's constants, the block's
@@ -1688,6 +1690,11 @@ __device__ bool flow_advance(const RoundArgs& a, BlockDev& B, const JobDev& J, i
   for (int k = 0; k < 8; ++k) evo[k] = __ldcg(&B.evo[k]);
   // sectors holding a vacancy (the slots' sector mask)
   unsigned occ_sec = __ldcg(&a.vsec[gb]);
+  // and, for the round this call may hand over, the valid bits of the block's vacancy slots, read
+  // last and with acquire: the slots' ids and sites (written before a give sets its bit) are read
+  // after it, by the CTA's threads past a barrier.  Every vacancy that can lie in the round's
+  // sector came with a round this lease's snapshot covers; only the lease holder clears bits.
+  if (vv) *vv = ld_acquire_u64(&a.vvalid[gb]);
   *tgt = t_old;
   if (r0 >= t_old) return false;
   // a single-block job with a hop budget ends at the end of the first time step at which its
@@ -1842,10 +1849,12 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
         int64_t rn = r, tgt = 0;
         int keep = 0;
         bool reached = false;
-        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &P, &rn, &reached, &tgt)) {
+        unsigned long long vv = 0;
+        if (flow_advance(a, B, J, gb, sm0->flow_lag, r, &P, &rn, &reached, &tgt, &vv)) {
           const int i = atomicAdd(&sm0->flow_ncand, 1);
           if (i < kFlowTake) {
             sm0->flow_cand[i] = gb;
+            sm0->flow_cvv[i] = vv;
             sm0->flow_cr[i] = rn;
             sm0->flow_ct[i] = tgt;
             keep = 1;
@@ -1916,7 +1925,8 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
           stage_rows(R, J.occ, J.rho, J.px, J.sy, J.sz, KIND != kPairBond, occ_s, rho_s, &sm->mbar_st, tid, kThreads);
         }
         if (tid < kFlowSlots) {
-          const unsigned long long m = ld_acquire_u64(&a.vvalid[gb]);
+          // the sweep read the valid bits when it handed the round over; a chained round reads them
+          const unsigned long long m = link == 0 ? sm0->flow_cvv[c] : ld_acquire_u64(&a.vvalid[gb]);
           if ((m >> tid) & 1ull) {
             const int v = __ldcg(&a.vslot[static_cast<int64_t>(gb) * kFlowSlots + tid]);
             const int32_t st = __ldcg(&a.vsite[static_cast<int64_t>(gb) * kFlowSlots + tid]);
@@ -1927,14 +1937,14 @@ __global__ void __launch_bounds__(Shape<W>::kThreads, Shape<W>::kCtasPerSm) k_fl
               sm->fslot[i] = tid;
             }
           }
-        } else if (tid == kCtl) {
-          sm->hops_out = __ldcg(&B.hops);  // run_block replaces it if the round runs
-          sm->pre_evo = __ldcg(&B.evo[sec]);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            sm->xs[i] = __ldcg(&B.xs[i]);
-            sm->xt[i] = __ldcg(&B.xt[i]);
-          }
+        } else if (tid < kFlowSlots + 10) {
+          // the block's hops, the sector's clock and the two streams, one value per thread, while
+          // the control thread issues the copies
+          const int q = tid - kFlowSlots;
+          if (q == 0) sm->hops_out = __ldcg(&B.hops);  // run_block replaces it if the round runs
+          else if (q == 1) sm->pre_evo = __ldcg(&B.evo[sec]);
+          else if (q < 6) sm->xs[q - 2] = __ldcg(&B.xs[q - 2]);
+          else sm->xt[q - 6] = __ldcg(&B.xt[q - 6]);
         }
         __syncthreads();
         const int cnt = sm->fnv;
